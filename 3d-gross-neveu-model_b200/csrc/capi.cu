@@ -1,0 +1,375 @@
+// capi.cu -- the extern "C" functions of include/gn_b200.h.  Each host-buffer
+// function copies its inputs into the context's device I/O area, runs the
+// engine and copies the outputs back before returning.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "../../include/gn_b200.h"
+#include "engine.h"
+#include "errors.h"
+
+struct gn_context {
+  std::unique_ptr<gn::Engine> eng;
+  double *io = nullptr;     // 24 V doubles of device staging for the host-buffer API
+  void *flush = nullptr;    // 512 MB, allocated on the first gn_flush_l2
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int status, const char *msg) {
+  g_last_error = msg;
+  return status;
+}
+
+template <typename F>
+int guarded(gn_context *ctx, F &&f) {
+  if (ctx == nullptr || !ctx->eng) return fail(GN_ERR_ARG, "null context");
+  try {
+    cudaSetDevice(ctx->eng->device());
+    return f(*ctx->eng);
+  } catch (const gn::GnError &e) {
+    return fail(e.status, e.what());
+  } catch (const std::exception &e) {
+    return fail(GN_ERR_CUDA, e.what());
+  }
+}
+
+void up(gn::Engine &E, double *dst, const double *src, size_t n) {
+  E.check(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyHostToDevice, E.stream()), "upload");
+}
+void down(gn::Engine &E, double *dst, const double *src, size_t n) {
+  E.check(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToHost, E.stream()), "download");
+}
+void sync(gn::Engine &E) { E.check(cudaStreamSynchronize(E.stream()), "synchronize"); }
+
+void fill_info(const gn::SolveInfo &s, gn_cg_info *o) {
+  o->status = s.status;
+  o->counted = s.status == gn::kCgConverged;
+  o->iterations = s.iters;
+  o->residual = std::sqrt(s.r2);
+  o->b_norm = std::sqrt(s.b2);
+  o->inner_iterations = s.inner;
+  o->reliable_updates = s.reliable;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *gn_last_error(void) { return g_last_error.c_str(); }
+
+int gn_create(gn_context **out, int L, int device) {
+  if (out == nullptr) return fail(GN_ERR_ARG, "null output pointer");
+  *out = nullptr;
+  try {
+    auto ctx = std::make_unique<gn_context>();
+    ctx->eng = std::make_unique<gn::Engine>(L, device);
+    const size_t V = size_t(ctx->eng->V());
+    ctx->eng->check(cudaMalloc(&ctx->io, 24 * V * sizeof(double)), "cudaMalloc io");
+    *out = ctx.release();
+    return GN_OK;
+  } catch (const gn::GnError &e) {
+    return fail(e.status, e.what());
+  } catch (const std::exception &e) {
+    return fail(GN_ERR_CUDA, e.what());
+  }
+}
+
+void gn_destroy(gn_context *ctx) {
+  if (ctx == nullptr) return;
+  if (ctx->eng) {
+    cudaSetDevice(ctx->eng->device());
+    cudaStreamSynchronize(ctx->eng->stream());
+  }
+  if (ctx->io) cudaFree(ctx->io);
+  if (ctx->flush) cudaFree(ctx->flush);
+  delete ctx;
+}
+
+long long gn_volume(const gn_context *ctx) { return (ctx && ctx->eng) ? (long long)ctx->eng->V() : 0; }
+
+void gn_request_abort(gn_context *ctx, int on) {
+  if (ctx && ctx->eng) *(volatile int *)ctx->eng->abort_flag_host() = on;
+}
+
+int gn_sigma_mass(gn_context *ctx, const double *sigma, double *sigmamass) {
+  if (!sigma || !sigmamass) return fail(GN_ERR_ARG, "null pointer");
+  return guarded(ctx, [&](gn::Engine &E) {
+    const size_t V = size_t(E.V());
+    double *d_s = ctx->io, *d_sm = ctx->io + V;
+    up(E, d_s, sigma, V);
+    E.sigma_mass(d_s, nullptr, 0.0, nullptr, d_sm);
+    down(E, sigmamass, d_sm, V);
+    sync(E);
+    return GN_OK;
+  });
+}
+
+int gn_dirac(gn_context *ctx, const double *sigmamass, const double *in, double *out, int ncomp, int op) {
+  if (!sigmamass || !in || !out) return fail(GN_ERR_ARG, "null pointer");
+  if (ncomp < 1 || ncomp > 2 || op < 0 || op > 2) return fail(GN_ERR_ARG, "bad ncomp or op");
+  return guarded(ctx, [&](gn::Engine &E) {
+    const size_t V = size_t(E.V()), n = size_t(ncomp) * V;
+    double *d_sm = ctx->io, *d_in = ctx->io + V, *d_out = ctx->io + 3 * V;
+    up(E, d_sm, sigmamass, V);
+    up(E, d_in, in, n);
+    if (op == GN_OP_SUB_M) up(E, d_out, out, n);
+    E.dirac(d_sm, d_in, d_out, ncomp, op);
+    down(E, out, d_out, n);
+    sync(E);
+    return GN_OK;
+  });
+}
+
+int gn_cg(gn_context *ctx, const double *sigmamass, const double *b, double *x, int nrhs, int ncomp, double tol,
+          int variant, int relative, long long max_iter, int precision, gn_cg_info *info) {
+  if (!sigmamass || !b || !x) return fail(GN_ERR_ARG, "null pointer");
+  if (nrhs < 1 || nrhs > gn::kMaxRhs || ncomp < 1 || ncomp > 2) return fail(GN_ERR_ARG, "bad nrhs or ncomp");
+  if (variant < 0 || variant > 1 || precision < 0 || precision > 1) return fail(GN_ERR_ARG, "bad variant/precision");
+  return guarded(ctx, [&](gn::Engine &E) {
+    const size_t V = size_t(E.V()), n = size_t(nrhs) * ncomp * V;
+    double *d_sm = ctx->io, *d_b = ctx->io + V, *d_x = ctx->io + V + n;
+    up(E, d_sm, sigmamass, V);
+    up(E, d_b, b, n);
+    up(E, d_x, x, n);
+    const double *bs[gn::kMaxRhs];
+    double *xs[gn::kMaxRhs];
+    for (int k = 0; k < nrhs; k++) {
+      bs[k] = d_b + size_t(k) * ncomp * V;
+      xs[k] = d_x + size_t(k) * ncomp * V;
+    }
+    gn::SolveInfo si[gn::kMaxRhs];
+    const int st = E.solve(d_sm, bs, xs, nrhs, ncomp, tol, variant, relative, max_iter, precision, si);
+    down(E, x, d_x, n);
+    sync(E);
+    if (info)
+      for (int k = 0; k < nrhs; k++) fill_info(si[k], &info[k]);
+    return st;
+  });
+}
+
+int gn_sigma_force(gn_context *ctx, double beta_s, const double *sigma, const double *sigmamass, const double *phi,
+                   double *X, double *Y, double tol, double *force, int precision, gn_cg_info *info) {
+  if (!sigma || !sigmamass || !phi || !X || !Y || !force) return fail(GN_ERR_ARG, "null pointer");
+  return guarded(ctx, [&](gn::Engine &E) {
+    const size_t V = size_t(E.V());
+    double *d_s = ctx->io, *d_sm = d_s + V, *d_phi = d_sm + V, *d_X = d_phi + 2 * V, *d_Y = d_X + 2 * V,
+           *d_F = d_Y + 2 * V;
+    up(E, d_s, sigma, V);
+    up(E, d_sm, sigmamass, V);
+    up(E, d_phi, phi, 2 * V);
+    up(E, d_X, X, 2 * V);
+    const double *bs[2] = {d_phi, d_phi + V};
+    double *xs[2] = {d_X, d_X + V};
+    gn::SolveInfo si[2];
+    const int st = E.solve(d_sm, bs, xs, 2, 1, tol, 0, 0, 0, precision, si);
+    if (st == GN_OK) {
+      E.dirac(d_sm, d_X, d_Y, 2, GN_OP_MT);
+      E.force(d_X, d_Y, d_s, beta_s, d_F, nullptr, 0.0);
+      down(E, Y, d_Y, 2 * V);
+      down(E, force, d_F, V);
+    }
+    down(E, X, d_X, 2 * V);
+    sync(E);
+    if (st != GN_OK) memset(force, 0, V * sizeof(double));  // SetForceSigmaToZero ran first
+    if (info)
+      for (int k = 0; k < 2; k++) fill_info(si[k], &info[k]);
+    return st;
+  });
+}
+
+int gn_energy(gn_context *ctx, double beta_s, const double *sigma, const double *P, const double *phi,
+              const double *X, double *H) {
+  if (!sigma || !P || !phi || !X || !H) return fail(GN_ERR_ARG, "null pointer");
+  return guarded(ctx, [&](gn::Engine &E) {
+    const size_t V = size_t(E.V());
+    double *d_s = ctx->io, *d_P = d_s + V, *d_phi = d_P + V, *d_X = d_phi + 2 * V;
+    up(E, d_s, sigma, V);
+    up(E, d_P, P, V);
+    up(E, d_phi, phi, 2 * V);
+    up(E, d_X, X, 2 * V);
+    double e[3];
+    E.energy_terms(d_P, d_phi, d_X, d_s, e);
+    *H = (e[0] + e[1]) + (4 * beta_s / 4.0) * e[2];
+    return GN_OK;
+  });
+}
+
+int gn_evolve_sigma(gn_context *ctx, double *sigma, double *sigmamass, const double *P, double eps) {
+  if (!sigma || !sigmamass || !P) return fail(GN_ERR_ARG, "null pointer");
+  return guarded(ctx, [&](gn::Engine &E) {
+    const size_t V = size_t(E.V());
+    double *d_s = ctx->io, *d_P = d_s + V, *d_out = d_P + V, *d_sm = d_out + V;
+    up(E, d_s, sigma, V);
+    up(E, d_P, P, V);
+    E.sigma_mass(d_s, d_P, eps, d_out, d_sm);
+    down(E, sigma, d_out, V);
+    down(E, sigmamass, d_sm, V);
+    sync(E);
+    return GN_OK;
+  });
+}
+
+int gn_evolve_momenta(gn_context *ctx, double *P, const double *F, double eps) {
+  if (!P || !F) return fail(GN_ERR_ARG, "null pointer");
+  return guarded(ctx, [&](gn::Engine &E) {
+    const size_t V = size_t(E.V());
+    double *d_P = ctx->io, *d_F = d_P + V;
+    up(E, d_P, P, V);
+    up(E, d_F, F, V);
+    E.momenta(d_P, d_F, eps);
+    down(E, P, d_P, V);
+    sync(E);
+    return GN_OK;
+  });
+}
+
+int gn_condensate(gn_context *ctx, const double *sigmamass, double tol, double *target, double *D,
+                  double (*uniform)(void), double *out, double *cg_iterations, long long *cg_calls, int precision) {
+  if (!sigmamass || !target || !D || !uniform || !out) return fail(GN_ERR_ARG, "null pointer");
+  return guarded(ctx, [&](gn::Engine &E) {
+    const size_t V = size_t(E.V());
+    double *d_sm = ctx->io, *d_t = d_sm + V, *d_D = d_t + 2 * V;
+    up(E, d_sm, sigmamass, V);
+    up(E, d_t, target, 2 * V);
+    double it = 0.0;
+    long long calls = 0;
+    const int st = E.condensate(d_sm, tol, d_t, d_D, uniform, out, &it, &calls, precision);
+    down(E, target, d_t, 2 * V);
+    down(E, D, d_D, 2 * V);
+    sync(E);
+    if (cg_iterations) *cg_iterations = it;
+    if (cg_calls) *cg_calls = calls;
+    return st;
+  });
+}
+
+int gn_load_sigma(gn_context *ctx, const double *sigma) {
+  if (!sigma) return fail(GN_ERR_ARG, "null pointer");
+  return guarded(ctx, [&](gn::Engine &E) {
+    up(E, E.sigma(), sigma, size_t(E.V()));
+    E.sigma_mass(E.sigma(), nullptr, 0.0, nullptr, E.sm());
+    sync(E);
+    return GN_OK;
+  });
+}
+
+int gn_store_sigma(gn_context *ctx, double *sigma, double *sigmamass) {
+  return guarded(ctx, [&](gn::Engine &E) {
+    if (sigma) down(E, sigma, E.sigma(), size_t(E.V()));
+    if (sigmamass) down(E, sigmamass, E.sm(), size_t(E.V()));
+    sync(E);
+    return GN_OK;
+  });
+}
+
+static double *field_ptr(gn::Engine &E, int field, size_t &n) {
+  const size_t V = size_t(E.V());
+  switch (field) {
+    case GN_F_P: n = V; return E.P();
+    case GN_F_F: n = V; return E.F();
+    case GN_F_CHI: n = 2 * V; return E.chi();
+    case GN_F_PHI: n = 2 * V; return E.phi();
+    case GN_F_X: n = 2 * V; return E.X();
+    case GN_F_Y: n = 2 * V; return E.Y();
+    default: throw gn::GnError(GN_ERR_ARG, "unknown field");
+  }
+}
+
+int gn_read_state(gn_context *ctx, int field, double *outp) {
+  if (!outp) return fail(GN_ERR_ARG, "null pointer");
+  return guarded(ctx, [&](gn::Engine &E) {
+    size_t n = 0;
+    double *p = field_ptr(E, field, n);
+    down(E, outp, p, n);
+    sync(E);
+    return GN_OK;
+  });
+}
+
+int gn_write_state(gn_context *ctx, int field, const double *in) {
+  if (!in) return fail(GN_ERR_ARG, "null pointer");
+  return guarded(ctx, [&](gn::Engine &E) {
+    size_t n = 0;
+    double *p = field_ptr(E, field, n);
+    up(E, p, in, n);
+    sync(E);
+    return GN_OK;
+  });
+}
+
+int gn_trajectory(gn_context *ctx, const gn_hmc_params *params, double (*gauss)(void), double (*uniform)(void),
+                  gn_traj_result *res) {
+  if (!params || !res) return fail(GN_ERR_ARG, "null pointer");
+  return guarded(ctx, [&](gn::Engine &E) { return E.trajectory(*params, gauss, uniform, nullptr, nullptr, res); });
+}
+
+void *gn_stream(gn_context *ctx) { return (ctx && ctx->eng) ? (void *)ctx->eng->stream() : nullptr; }
+
+double *gn_field_ptr(gn_context *ctx, int field) {
+  if (!ctx || !ctx->eng) return nullptr;
+  gn::Engine &E = *ctx->eng;
+  if (field == GN_F_SIGMA) return E.sigma();
+  if (field == GN_F_SM) return E.sm();
+  try {
+    size_t n = 0;
+    return field_ptr(E, field, n);
+  } catch (const gn::GnError &e) {
+    fail(e.status, e.what());
+    return nullptr;
+  }
+}
+
+int gn_dirac_device(gn_context *ctx, const double *sigmamass, const double *in, double *out, int ncomp, int op) {
+  if (!sigmamass || !in || !out) return fail(GN_ERR_ARG, "null pointer");
+  if (ncomp < 1 || ncomp > 2 || op < 0 || op > 2) return fail(GN_ERR_ARG, "bad ncomp or op");
+  return guarded(ctx, [&](gn::Engine &E) {
+    E.dirac(sigmamass, in, out, ncomp, op);
+    return GN_OK;
+  });
+}
+
+int gn_cg_device(gn_context *ctx, const double *sigmamass, const double *b, double *x, int nrhs, int ncomp, double tol,
+                 int variant, int relative, long long max_iter, int precision, gn_cg_info *info) {
+  if (!sigmamass || !b || !x) return fail(GN_ERR_ARG, "null pointer");
+  if (nrhs < 1 || nrhs > gn::kMaxRhs || ncomp < 1 || ncomp > 2) return fail(GN_ERR_ARG, "bad nrhs or ncomp");
+  if (variant < 0 || variant > 1 || precision < 0 || precision > 1) return fail(GN_ERR_ARG, "bad variant/precision");
+  return guarded(ctx, [&](gn::Engine &E) {
+    const size_t V = size_t(E.V());
+    const double *bs[gn::kMaxRhs];
+    double *xs[gn::kMaxRhs];
+    for (int k = 0; k < nrhs; k++) {
+      bs[k] = b + size_t(k) * ncomp * V;
+      xs[k] = x + size_t(k) * ncomp * V;
+    }
+    gn::SolveInfo si[gn::kMaxRhs];
+    const int st = E.solve(sigmamass, bs, xs, nrhs, ncomp, tol, variant, relative, max_iter, precision, si);
+    if (info)
+      for (int k = 0; k < nrhs; k++) fill_info(si[k], &info[k]);
+    return st;
+  });
+}
+
+int gn_trajectory_device(gn_context *ctx, const gn_hmc_params *params, const double *P, const double *chi,
+                         double (*uniform)(void), gn_traj_result *res) {
+  if (!params || !res || !P || !chi) return fail(GN_ERR_ARG, "null pointer");
+  return guarded(ctx, [&](gn::Engine &E) { return E.trajectory(*params, nullptr, uniform, P, chi, res); });
+}
+
+long long gn_launch_count(gn_context *ctx) { return (ctx && ctx->eng) ? ctx->eng->launches : 0; }
+
+int gn_flush_l2(gn_context *ctx) {
+  return guarded(ctx, [&](gn::Engine &E) {
+    const size_t bytes = size_t(512) << 20;
+    if (!ctx->flush) E.check(cudaMalloc(&ctx->flush, bytes), "cudaMalloc flush");
+    E.check(cudaMemsetAsync(ctx->flush, ctx->eng->V() & 0xff, bytes, E.stream()), "flush");
+    return GN_OK;
+  });
+}
+
+}  // extern "C"

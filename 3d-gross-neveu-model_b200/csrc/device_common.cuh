@@ -1,0 +1,176 @@
+// device_common.cuh -- building blocks shared by every kernel: the staggered
+// stencils, deterministic block reductions and a bounded grid barrier.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "geometry.cuh"
+
+namespace gn {
+
+// ------------------------------------------------------------------ stencils
+// The Dirac operator of dirac.c:46-82 on one site, real arithmetic (the
+// reference's fields are complex with a zero imaginary part on this path;
+// a genuinely complex field is handled as two real planes):
+//   (M psi)(x)   = sm(x) psi(x) + sum_mu 1/2 [eta_pp(x,mu) psi(x+mu) - eta_mm(x,mu) psi(x-mu)]
+//   (M^T psi)(x) = sm(x) psi(x) - sum_mu 1/2 [eta_pp(x,mu) psi(x+mu) - eta_mm(x,mu) psi(x-mu)]
+// M^T is the gather form of the scatter in dirac.c:88-123 (eta_mm(x+mu, mu) =
+// eta_pp(x, mu) under antiperiodic time).  The order of the additions of M
+// (and of out - M psi) is the reference's: mass term first, then mu = 0, 1, 2
+// with the forward term before the backward one.  With FMA contraction off
+// (the FP64 translation units are built with --fmad=false) M is therefore bit
+// identical to DiracFermion; M^T adds the same seven terms in another order.
+template <typename T>
+struct Nb {
+  T c, up[3], dn[3];
+};
+
+template <typename T, typename Load>
+__device__ __forceinline__ Nb<T> gather7(const Site &s, uint32_t i, Load ld) {
+  Nb<T> n;
+  n.c = ld(i);
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    n.up[d] = ld(s.nb_up[d]);
+    n.dn[d] = ld(s.nb_dn[d]);
+  }
+  return n;
+}
+
+template <typename T>
+__device__ __forceinline__ T apply_M(const Site &s, T sm, const Nb<T> &n) {
+  T t = sm * n.c;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    t = t + (T(0.5) * T(s.eta_up[d])) * n.up[d];
+    t = t - (T(0.5) * T(s.eta_dn[d])) * n.dn[d];
+  }
+  return t;
+}
+
+template <typename T>
+__device__ __forceinline__ T apply_Mt(const Site &s, T sm, const Nb<T> &n) {
+  T t = sm * n.c;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    t = t - (T(0.5) * T(s.eta_up[d])) * n.up[d];
+    t = t + (T(0.5) * T(s.eta_dn[d])) * n.dn[d];
+  }
+  return t;
+}
+
+// out - M psi in the order of SubtractDiracFermion (dirac.c:213-247)
+template <typename T>
+__device__ __forceinline__ T apply_sub_M(const Site &s, T out, T sm, const Nb<T> &n) {
+  T t = out - sm * n.c;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    t = t - (T(0.5) * T(s.eta_up[d])) * n.up[d];
+    t = t + (T(0.5) * T(s.eta_dn[d])) * n.dn[d];
+  }
+  return t;
+}
+
+// ------------------------------------------------------------------ reductions
+// Deterministic: fixed shuffle pattern, fixed warp order.  Every call with the
+// same inputs returns the same bits.
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Sums N values over the block; thread 0 gets the totals in v.
+// smem needs 32*N doubles.
+template <int N>
+__device__ __forceinline__ void block_sum(double (&v)[N], double *smem) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int j = 0; j < N; j++) v[j] = warp_sum(v[j]);
+  __syncthreads();
+  if (lane == 0) {
+#pragma unroll
+    for (int j = 0; j < N; j++) smem[j * 32 + w] = v[j];
+  }
+  __syncthreads();
+  if (w == 0) {
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      double a = lane < nw ? smem[j * 32 + lane] : 0.0;
+      v[j] = warp_sum(a);
+    }
+  }
+  __syncthreads();
+}
+
+// Error-free two-sum (Knuth), for compensated energy sums.
+__device__ __forceinline__ void two_sum(double a, double b, double &s, double &e) {
+  s = a + b;
+  double bb = s - a;
+  e = (a - (s - bb)) + (b - bb);
+}
+
+// ------------------------------------------------------------------ grid barrier
+// A generation barrier for cooperative launches (all blocks co-resident).  Every
+// wait is bounded: after kSpinLimit polls (about a second) the waiting block sets
+// *err and returns false, so a kernel can never hang the device.
+struct GridBar {
+  unsigned count;
+  unsigned gen;
+};
+
+constexpr unsigned kSpinLimit = 1u << 24;
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned atom_add_acq_rel(unsigned *p, unsigned v) {
+  unsigned old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+__device__ __forceinline__ void st_relaxed(unsigned *p, unsigned v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ int ld_err(const int *p) {
+  int v;
+  asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Returns false if this block gave up waiting or another block reported an error.
+__device__ __forceinline__ bool grid_barrier(GridBar *bar, unsigned &gen_local, int *err) {
+  __syncthreads();
+  __shared__ int s_ok;
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    __threadfence();
+    const unsigned g = gen_local;
+    const unsigned arrived = atom_add_acq_rel(&bar->count, 1u);
+    if (arrived == gridDim.x * gridDim.y * gridDim.z - 1u) {
+      st_relaxed(&bar->count, 0u);
+      __threadfence();
+      atom_add_acq_rel(&bar->gen, 1u);
+    } else {
+      unsigned spins = 0;
+      while (ld_acquire(&bar->gen) == g) {
+        if (++spins > kSpinLimit) {
+          atomicExch(err, 1);
+          ok = 0;
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+    if (ld_err(err) != 0) ok = 0;
+    s_ok = ok;
+  }
+  gen_local++;
+  __syncthreads();
+  return s_ok != 0;
+}
+
+}  // namespace gn

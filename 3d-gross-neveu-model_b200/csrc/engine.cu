@@ -1,0 +1,486 @@
+// engine.cu -- device engine of the sigma-HMC fermion path (FP64 kernels).
+// Built with --fmad=false: the FP64 kernels follow the reference's rounding
+// (mul then add) wherever the reference's result is reproducible bit for bit.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+
+#include "engine.h"
+#include "errors.h"
+#include "ops_kernels.cuh"
+
+namespace gn {
+
+constexpr int kNumWorkVecs = 4;  // r, p0, p1, t per right-hand side
+
+void Engine::check(cudaError_t e, const char *what) {
+  if (e != cudaSuccess) {
+    char buf[256];
+    snprintf(buf, sizeof buf, "%s: %s", what, cudaGetErrorString(e));
+    throw GnError(GN_ERR_CUDA, buf);
+  }
+}
+
+void *Engine::alloc(size_t bytes) {
+  void *p = nullptr;
+  check(cudaMalloc(&p, bytes), "cudaMalloc");
+  allocs_.push_back(p);
+  check(cudaMemsetAsync(p, 0, bytes, stream_), "cudaMemsetAsync");
+  return p;
+}
+
+Engine::Engine(int L, int device) : L_(L), device_(device) {
+  if (L < 4 || L > 256 || (L & 1)) throw GnError(GN_ERR_ARG, "L must be even and in [4, 256]");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+    throw GnError(GN_ERR_NO_DEVICE, "no such CUDA device");
+  check(cudaSetDevice(device), "cudaSetDevice");
+  cudaDeviceProp prop;
+  check(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+  if (prop.major != 10) throw GnError(GN_ERR_NO_DEVICE, "this library is built for sm_100a (B200) only");
+  if (!prop.cooperativeLaunch) throw GnError(GN_ERR_NO_DEVICE, "device lacks cooperative launch");
+  num_sms_ = prop.multiProcessorCount;
+  check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  g_ = make_geom(L);
+  V_ = g_.V;
+  const size_t V = size_t(V_);
+  const size_t d = sizeof(double);
+  sigma_[0] = (double *)alloc(V * d);
+  sigma_[1] = (double *)alloc(V * d);
+  sm_ = (double *)alloc(V * d);
+  P_ = (double *)alloc(V * d);
+  F_ = (double *)alloc(V * d);
+  chi_ = (double *)alloc(2 * V * d);
+  phi_ = (double *)alloc(2 * V * d);
+  X_ = (double *)alloc(2 * V * d);
+  Y_ = (double *)alloc(2 * V * d);
+  for (int i = 0; i < 4; i++) scratch_[i] = (double *)alloc(2 * V * d);
+  signs_ = (signed char *)alloc(V);
+  table_ = (double *)alloc(2 * 256 * d);
+  cg_work_ = (double *)alloc(size_t(kMaxRhs) * kNumWorkVecs * 2 * V * d);
+  max_blocks_ = num_sms_ * 8;
+  partials_ = (double *)alloc(size_t(32) * max_blocks_ * d);
+  bar_ = (GridBar *)alloc(sizeof(GridBar));
+  err_ = (int *)alloc(sizeof(int));
+  state_ = (CgState *)alloc(sizeof(CgState) * kMaxRhs);
+  check(cudaHostAlloc((void **)&h_partials_, size_t(32) * max_blocks_ * d, cudaHostAllocDefault), "cudaHostAlloc");
+  check(cudaHostAlloc((void **)&h_state_, sizeof(CgState) * kMaxRhs, cudaHostAllocDefault), "cudaHostAlloc");
+  check(cudaHostAlloc((void **)&h_abort_, sizeof(int), cudaHostAllocMapped), "cudaHostAlloc");
+  *h_abort_ = 0;
+  check(cudaHostGetDevicePointer((void **)&d_abort_, h_abort_, 0), "cudaHostGetDevicePointer");
+  check(cudaHostAlloc((void **)&h_stage_, 4 * V * d, cudaHostAllocDefault), "cudaHostAlloc");
+  mixed_init();
+  check(cudaStreamSynchronize(stream_), "init");
+}
+
+Engine::~Engine() {
+  cudaSetDevice(device_);
+  if (stream_) cudaStreamSynchronize(stream_);
+  for (void *p : allocs_) cudaFree(p);
+  if (h_partials_) cudaFreeHost(h_partials_);
+  if (h_state_) cudaFreeHost(h_state_);
+  if (h_abort_) cudaFreeHost(h_abort_);
+  if (h_stage_) cudaFreeHost(h_stage_);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+static int op_blocks(int64_t V, int num_sms) {
+  int64_t b = (V + kOpThreads - 1) / kOpThreads;
+  int64_t cap = int64_t(num_sms) * (2048 / kOpThreads);
+  return int(b < cap ? b : cap);
+}
+
+void Engine::sigma_mass(const double *sigma, const double *P, double eps, double *sigma_out, double *sm) {
+  sigma_mass_kernel<double><<<op_blocks(V_, num_sms_), kOpThreads, 0, stream_>>>(g_, sigma, P, eps, sigma_out, sm);
+  check(cudaGetLastError(), "sigma_mass_kernel");
+  launches++;
+}
+
+void Engine::dirac(const double *sm, const double *in, double *out, int ncomp, int op) {
+  const int nb = op_blocks(V_, num_sms_);
+  if (op == GN_OP_M) dirac_kernel<double, 0><<<nb, kOpThreads, 0, stream_>>>(g_, sm, in, out, ncomp);
+  else if (op == GN_OP_MT) dirac_kernel<double, 1><<<nb, kOpThreads, 0, stream_>>>(g_, sm, in, out, ncomp);
+  else dirac_kernel<double, 2><<<nb, kOpThreads, 0, stream_>>>(g_, sm, in, out, ncomp);
+  check(cudaGetLastError(), "dirac_kernel");
+  launches++;
+}
+
+void Engine::momenta(double *P, const double *F, double eps) {
+  momenta_kernel<double><<<op_blocks(V_, num_sms_), kOpThreads, 0, stream_>>>(uint32_t(V_), P, F, eps);
+  check(cudaGetLastError(), "momenta_kernel");
+  launches++;
+}
+
+void Engine::force(const double *X, const double *Y, const double *sigma, double beta_s, double *F, double *P,
+                   double pcoef) {
+  const double gcoef = (4 * beta_s / 2.0);  // (NFLAV * beta_scalar / 2.0), moleculardynamics.c:580
+  force_kernel<double><<<op_blocks(V_, num_sms_), kOpThreads, 0, stream_>>>(g_, X, Y, sigma, gcoef, F, P, pcoef);
+  check(cudaGetLastError(), "force_kernel");
+  launches++;
+}
+
+double sum_partials(const double *part, int nb, int q) {
+  // Neumaier over the block (hi, lo) pairs
+  double s = 0.0, c = 0.0;
+  for (int b = 0; b < nb; b++) {
+    for (int h = 0; h < 2; h++) {
+      const double v = part[(size_t(q) * nb + b) * 2 + h];
+      const double t = s + v;
+      if (std::fabs(s) >= std::fabs(v)) c += (s - t) + v;
+      else c += (v - t) + s;
+      s = t;
+    }
+  }
+  return s + c;
+}
+
+void Engine::energy_terms(const double *P, const double *phi, const double *X, const double *sigma, double out[3]) {
+  const int nb = op_blocks(V_, num_sms_);
+  energy_kernel<double><<<nb, kOpThreads, 0, stream_>>>(uint32_t(V_), P, phi, X, sigma, partials_);
+  check(cudaGetLastError(), "energy_kernel");
+  launches++;
+  check(cudaMemcpyAsync(h_partials_, partials_, sizeof(double) * 6 * nb, cudaMemcpyDeviceToHost, stream_), "copy");
+  check(cudaStreamSynchronize(stream_), "energy sync");
+  for (int q = 0; q < 3; q++) out[q] = sum_partials(h_partials_, nb, q);
+}
+
+void Engine::cond_dots(const double *v, const double *D, double out[3]) {
+  const int nb = op_blocks(V_, num_sms_);
+  cond_dot_kernel<<<nb, kOpThreads, 0, stream_>>>(uint32_t(V_), v, D, partials_);
+  check(cudaGetLastError(), "cond_dot_kernel");
+  launches++;
+  check(cudaMemcpyAsync(h_partials_, partials_, sizeof(double) * 6 * nb, cudaMemcpyDeviceToHost, stream_), "copy");
+  check(cudaStreamSynchronize(stream_), "dots sync");
+  for (int q = 0; q < 3; q++) out[q] = sum_partials(h_partials_, nb, q);
+}
+
+void Engine::cond_fill(int mode, const signed char *signs, const double *table, const double *sm, double *v) {
+  cond_fill_kernel<<<op_blocks(V_, num_sms_), kOpThreads, 0, stream_>>>(g_, mode, signs, table, sm, v);
+  check(cudaGetLastError(), "cond_fill_kernel");
+  launches++;
+}
+
+int Engine::cg_blocks(int ncomp, bool mixed) {
+  int &cached = cg_blocks_cache_[mixed ? 1 : 0][ncomp - 1];
+  if (cached) return cached;
+  int per_sm = 0;
+  const void *fn = mixed ? mixed_kernel_ptr(ncomp)
+                         : (ncomp == 1 ? (const void *)cg_kernel<double, 1> : (const void *)cg_kernel<double, 2>);
+  check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kCgThreads, 0), "occupancy");
+  if (per_sm < 1) throw GnError(GN_ERR_CUDA, "CG kernel cannot be resident");
+  int64_t want = (V_ + kCgThreads - 1) / kCgThreads;
+  int64_t cap = int64_t(per_sm) * num_sms_;
+  if (cap > max_blocks_) cap = max_blocks_;
+  cached = int(want < cap ? want : cap);
+  return cached;
+}
+
+int Engine::solve(const double *sm, const double *const *b, double *const *x, int nrhs, int ncomp, double tol,
+                  int variant, int rel, long long max_iter, int precision, SolveInfo *info) {
+  if (nrhs < 1 || nrhs > kMaxRhs || ncomp < 1 || ncomp > 2) throw GnError(GN_ERR_ARG, "bad nrhs / ncomp");
+  if (max_iter <= 0) max_iter = V_ + 1;  // MAX_CONJUGATE_GRADIENT_ITERATION, macro.h:134
+  if (precision == GN_PREC_MIXED) return solve_mixed(sm, b, x, nrhs, ncomp, tol, variant, rel, max_iter, info);
+  const size_t V = size_t(V_);
+  CgArgs<double> a;
+  memset(&a, 0, sizeof a);
+  a.g = g_;
+  a.sm = sm;
+  for (int k = 0; k < nrhs; k++) {
+    double *w = cg_work_ + size_t(k) * kNumWorkVecs * 2 * V;
+    a.b[k] = b[k];
+    a.x[k] = x[k];
+    a.r[k] = w;
+    a.p0[k] = w + 2 * V;
+    a.p1[k] = w + 4 * V;
+    a.t[k] = w + 6 * V;
+  }
+  a.nrhs = nrhs;
+  a.variant = variant;
+  a.rel = rel;
+  a.tol = tol;
+  a.max_iter = max_iter;
+  a.partials = partials_;
+  a.bar = bar_;
+  a.err = err_;
+  a.abort_flag = d_abort_;
+  a.state = state_;
+  check(cudaMemsetAsync(bar_, 0, sizeof(unsigned), stream_), "memset");
+  check(cudaMemsetAsync(err_, 0, sizeof(int), stream_), "memset");
+  const int nb = cg_blocks(ncomp, false);
+  void *args[] = {(void *)&a};
+  const void *fn = ncomp == 1 ? (const void *)cg_kernel<double, 1> : (const void *)cg_kernel<double, 2>;
+  check(cudaLaunchCooperativeKernel(fn, dim3(nb), dim3(kCgThreads), args, 0, stream_), "cg_kernel launch");
+  launches++;
+  return finish_solve(nrhs, info);
+}
+
+int Engine::finish_solve(int nrhs, SolveInfo *info) {
+  int h_err = 0;
+  check(cudaMemcpyAsync(h_state_, state_, sizeof(CgState) * nrhs, cudaMemcpyDeviceToHost, stream_), "copy");
+  check(cudaMemcpyAsync(&h_err, err_, sizeof(int), cudaMemcpyDeviceToHost, stream_), "copy");
+  check(cudaStreamSynchronize(stream_), "cg sync");
+  if (h_err == 1) throw GnError(GN_ERR_TIMEOUT, "CG grid barrier timed out");
+  if (h_err == 2) throw GnError(GN_ERR_ABORTED, "CG aborted on request");
+  bool all = true;
+  for (int k = 0; k < nrhs; k++) {
+    info[k].status = h_state_[k].status;
+    info[k].iters = h_state_[k].iters;
+    info[k].r2 = h_state_[k].r2;
+    info[k].b2 = h_state_[k].b2;
+    info[k].inner = h_state_[k].iters;
+    info[k].reliable = h_state_[k].reliable;
+    if (info[k].status != kCgConverged && info[k].status != kCgConvergedStart) all = false;
+  }
+  return all ? GN_OK : GN_NOT_CONVERGED;
+}
+
+// ------------------------------------------------------------------ trajectory
+// Integrator schedules (moleculardynamics.c:859-1005, :1018-1221, :1234-1434)
+// as op lists: F force (medium / high tolerance), P momentum step, Q sigma
+// step, S X0-imposed solve at high tolerance.
+enum { OP_F_MED = 1, OP_F_HIGH, OP_P, OP_Q, OP_S_HIGH };
+struct Op {
+  int op;
+  double c;
+};
+
+static std::vector<Op> schedule(int integrator, double eps, int step) {
+  std::vector<Op> v;
+  const double lam = 0.1931833275037836;  // MAGIC_LAMBDA, macro.h:169
+  auto push = [&](int o, double c) { v.push_back({o, c}); };
+  if (integrator == GN_LFMN2VF) {
+    push(OP_F_MED, 0); push(OP_P, lam * eps); push(OP_Q, eps / 2.0);
+    push(OP_F_MED, 0); push(OP_P, (1.0 - (2.0 * lam)) * eps); push(OP_Q, eps / 2.0);
+    for (int s = 1; s < step - 1; s++) {
+      push(OP_F_MED, 0); push(OP_P, 2.0 * lam * eps); push(OP_Q, eps / 2.0);
+      push(OP_F_MED, 0); push(OP_P, (1.0 - (2.0 * lam)) * eps); push(OP_Q, eps / 2.0);
+    }
+    push(OP_F_MED, 0); push(OP_P, 2.0 * lam * eps); push(OP_Q, eps / 2.0);
+    push(OP_F_MED, 0); push(OP_P, (1.0 - (2.0 * lam)) * eps); push(OP_Q, eps / 2.0);
+    push(OP_F_HIGH, 0); push(OP_P, lam * eps);
+  } else if (integrator == GN_LF2) {
+    push(OP_F_MED, 0); push(OP_P, eps / 2.0);
+    for (int s = 0; s < step - 1; s++) { push(OP_Q, eps); push(OP_F_MED, 0); push(OP_P, eps); }
+    push(OP_Q, eps); push(OP_F_HIGH, 0); push(OP_P, eps / 2.0);
+  } else {
+    push(OP_Q, lam * eps); push(OP_F_MED, 0); push(OP_P, eps / 2.0);
+    push(OP_Q, (1.0 - (2.0 * lam)) * eps); push(OP_F_MED, 0); push(OP_P, eps / 2.0);
+    for (int s = 1; s < step - 1; s++) {
+      push(OP_Q, 2.0 * lam * eps); push(OP_F_MED, 0); push(OP_P, eps / 2.0);
+      push(OP_Q, (1.0 - (2.0 * lam)) * eps); push(OP_F_MED, 0); push(OP_P, eps / 2.0);
+    }
+    push(OP_Q, 2.0 * lam * eps); push(OP_F_MED, 0); push(OP_P, eps / 2.0);
+    push(OP_Q, (1 - (2.0 * lam)) * eps); push(OP_F_MED, 0); push(OP_P, eps / 2.0);
+    push(OP_Q, lam * eps); push(OP_S_HIGH, 0);
+  }
+  return v;
+}
+
+// kit->iterations / kit->CG_call bookkeeping of a flavour loop that stops at
+// the first failure (moleculardynamics.c:593-597).
+static void count_flavours(const SolveInfo *info, int n, double &iters, long long &calls, long long &inner,
+                           long long &rel) {
+  for (int k = 0; k < n; k++) {
+    if (info[k].status == kCgConverged) {
+      iters += double(info[k].iters);
+      calls++;
+    }
+    inner += info[k].inner;
+    rel += info[k].reliable;
+    if (info[k].status != kCgConverged && info[k].status != kCgConvergedStart) break;
+  }
+}
+
+int Engine::trajectory(const gn_hmc_params &hp, double (*gauss)(void), double (*uniform)(void), const double *pre_P,
+                       const double *pre_chi, gn_traj_result *res) {
+  if (hp.steps < 2) throw GnError(GN_ERR_ARG, "steps must be >= 2 (info.c:66)");
+  if (hp.integrator < 0 || hp.integrator > 2) throw GnError(GN_ERR_ARG, "unknown integrator");
+  const size_t V = size_t(V_);
+  memset(res, 0, sizeof *res);
+  // draws: P, chi_0, chi_1 (moleculardynamics.c:1240-1247), uploaded in one copy
+  if (gauss != nullptr) {
+    double *h = h_stage_;
+    for (size_t i = 0; i < 3 * V; i++) h[i] = gauss();
+    check(cudaMemcpyAsync(P_, h, V * sizeof(double), cudaMemcpyHostToDevice, stream_), "upload P");
+    check(cudaMemcpyAsync(chi_, h + V, 2 * V * sizeof(double), cudaMemcpyHostToDevice, stream_), "upload chi");
+  } else {
+    if (pre_P) check(cudaMemcpyAsync(P_, pre_P, V * sizeof(double), cudaMemcpyDeviceToDevice, stream_), "copy P");
+    if (pre_chi)
+      check(cudaMemcpyAsync(chi_, pre_chi, 2 * V * sizeof(double), cudaMemcpyDeviceToDevice, stream_), "copy chi");
+  }
+  dirac(sm_, chi_, phi_, 2, GN_OP_M);  // phi_f = M chi_f (both flavours as planes)
+  double *sigma_copy = scratch_[3];
+  check(cudaMemcpyAsync(sigma_copy, sigma(), V * sizeof(double), cudaMemcpyDeviceToDevice, stream_), "copy sigma");
+  auto restore = [&]() {
+    check(cudaMemcpyAsync(sigma(), sigma_copy, V * sizeof(double), cudaMemcpyDeviceToDevice, stream_), "restore");
+    sigma_mass(sigma(), nullptr, 0.0, nullptr, sm_);
+  };
+  const double *phis[2] = {phi_, phi_ + V};
+  double *Xs[2] = {X_, X_ + V};
+  SolveInfo info[2];
+  double iters = 0.0;
+  long long calls = 0, inner = 0, rel = 0;
+  auto finish = [&](int ok) {
+    res->ok = ok;
+    res->cg_iterations = iters;
+    res->cg_calls = calls;
+    res->inner_iterations = inner;
+    res->reliable_updates = rel;
+  };
+  int st = solve(sm_, phis, Xs, 2, 1, hp.tol_high, 1, hp.relative, 0, hp.precision, info);
+  count_flavours(info, 2, iters, calls, inner, rel);
+  if (st != GN_OK) {
+    restore();
+    check(cudaStreamSynchronize(stream_), "restore");
+    finish(0);
+    return GN_NOT_CONVERGED;
+  }
+  const double ccoef = (4 * hp.beta_s / 4.0);  // (NFLAV * beta_scalar / 4.0), moleculardynamics.c:316
+  double e[3];
+  energy_terms(P_, phi_, X_, sigma(), e);
+  const double h0 = (e[0] + e[1]) + ccoef * e[2];
+  const std::vector<Op> ops = schedule(hp.integrator, hp.eps, hp.steps);
+  for (size_t k = 0; k < ops.size(); k++) {
+    const Op &o = ops[k];
+    if (o.op == OP_F_MED || o.op == OP_F_HIGH) {
+      const double tol = o.op == OP_F_MED ? hp.tol_medium : hp.tol_high;
+      st = solve(sm_, phis, Xs, 2, 1, tol, 0, hp.relative, 0, hp.precision, info);
+      count_flavours(info, 2, iters, calls, inner, rel);
+      if (st != GN_OK) {
+        restore();
+        check(cudaStreamSynchronize(stream_), "restore");
+        finish(0);
+        return GN_NOT_CONVERGED;
+      }
+      dirac(sm_, X_, Y_, 2, GN_OP_MT);
+      if (k + 1 < ops.size() && ops[k + 1].op == OP_P) {
+        force(X_, Y_, sigma(), hp.beta_s, F_, P_, ops[k + 1].c);
+        k++;
+      } else {
+        force(X_, Y_, sigma(), hp.beta_s, F_, nullptr, 0.0);
+      }
+    } else if (o.op == OP_P) {
+      momenta(P_, F_, o.c);
+    } else if (o.op == OP_Q) {
+      sigma_mass(sigma(), P_, o.c, sigma_alt(), sm_);
+      swap_sigma();
+      distance += o.c;
+      res->distance += o.c;
+    } else {
+      st = solve(sm_, phis, Xs, 2, 1, hp.tol_high, 1, hp.relative, 0, hp.precision, info);
+      count_flavours(info, 2, iters, calls, inner, rel);
+      if (st != GN_OK) {
+        restore();
+        check(cudaStreamSynchronize(stream_), "restore");
+        finish(0);
+        return GN_NOT_CONVERGED;
+      }
+    }
+  }
+  energy_terms(P_, phi_, X_, sigma(), e);
+  const double h1 = (e[0] + e[1]) + ccoef * e[2];
+  res->H0 = h0;
+  res->H1 = h1;
+  res->dH = h1 - h0;
+  // Metropolis on the host with the reference's uniform (moleculardynamics.c:1385)
+  const int acc = uniform != nullptr ? (uniform() <= std::exp(-(h1 - h0))) : 1;
+  res->accepted = acc;
+  if (!acc) restore();
+  check(cudaStreamSynchronize(stream_), "trajectory");
+  finish(1);
+  return GN_OK;
+}
+
+// ------------------------------------------------------------------ condensate
+int Engine::condensate(const double *sm, double tol, double *target, double *D, double (*uniform)(void),
+                       double out[11], double *iterations, long long *calls, int precision) {
+  const size_t V = size_t(V_);
+  double *vec = scratch_[0];
+  double *z = scratch_[1];
+  signed char *h_signs = reinterpret_cast<signed char *>(h_stage_);
+  SolveInfo info[1];
+  int all_ok = 1;
+  auto solve1 = [&](const double *b) {
+    const double *bs[1] = {b};
+    double *xs[1] = {target};
+    const int st = solve(sm, bs, xs, 1, 2, tol, 0, 0, 0, precision, info);
+    if (info[0].status == kCgConverged) {
+      *iterations += double(info[0].iters);
+      (*calls)++;
+    }
+    if (st != GN_OK) all_ok = 0;
+  };
+  auto z2 = [&]() {  // Z2NoiseFullRandomVec, condensate.c:52-60: one uniform per site
+    check(cudaStreamSynchronize(stream_), "z2 sync");
+    for (size_t x = 0; x < V; x++) h_signs[x] = (uniform() <= 0.5) ? 1 : -1;
+    check(cudaMemcpyAsync(signs_, h_signs, V, cudaMemcpyHostToDevice, stream_), "upload signs");
+    cond_fill(0, signs_, nullptr, nullptr, vec);
+  };
+  double q[3];
+  for (int k = 0; k < 11; k++) out[k] = 0.0;
+  double temp[4];
+  for (int p = 0; p < 4; p++) {
+    z2();
+    solve1(vec);
+    dirac(sm, target, D, 2, GN_OP_MT);
+    cond_dots(vec, D, q);
+    temp[p] = q[0];
+  }
+  const double tr0 = temp[0], tr1 = temp[1], tr2 = temp[2], tr3 = temp[3];
+  out[0] = (tr0 + tr1 + tr2 + tr3) / 4.0;
+  out[1] = std::fabs(out[0]);
+  out[2] = ((tr0 * tr1) + (tr0 * tr2) + (tr0 * tr3) + (tr1 * tr2) + (tr1 * tr3) + (tr2 * tr3)) / 6.0;
+  out[3] = (tr0 * tr1 * tr2 * tr3);
+  // mu2, chi: the 1/V vector (condensate.c:167-181)
+  cond_fill(1, nullptr, nullptr, nullptr, vec);
+  solve1(vec);
+  dirac(sm, target, D, 2, GN_OP_MT);
+  cond_dots(vec, D, q);
+  out[4] = q[1];
+  out[5] = out[4] * out[4];
+  out[6] = double(int(V)) * out[4];
+  out[7] = std::fabs(out[6]);
+  // chi_p: e^{i pi/L x2} / V (condensate.c:84-89, :185-197); the table is
+  // formed on the host with the same expression as the reference.
+  {
+    double *h_tab = h_stage_ + V;  // past the sign bytes
+    const double pi = 3.141592653589793238462643383279502884197169399375105820974944;
+    for (int t = 0; t < L_; t++) {
+      const double th = (pi / L_) * t;
+      // cexp(I * (pi/L) * t) / V: real part cos, imaginary part sin
+      h_tab[2 * t] = std::cos(th) / double(int(V));
+      h_tab[2 * t + 1] = std::sin(th) / double(int(V));
+    }
+    check(cudaMemcpyAsync(table_, h_tab, sizeof(double) * 2 * L_, cudaMemcpyHostToDevice, stream_), "table");
+    cond_fill(2, nullptr, table_, nullptr, vec);
+    solve1(vec);
+    dirac(sm, target, D, 2, GN_OP_MT);
+    cond_dots(vec, D, q);
+    out[8] = q[2] * double(int(V));
+  }
+  // <chibar1 chi2> without sigma (condensate.c:201-212)
+  z2();
+  check(cudaMemcpyAsync(z, vec, 2 * V * sizeof(double), cudaMemcpyDeviceToDevice, stream_), "copy z");
+  solve1(vec);
+  dirac(sm, target, D, 2, GN_OP_MT);
+  solve1(D);
+  dirac(sm, target, D, 2, GN_OP_MT);
+  cond_dots(z, D, q);
+  out[9] = q[0];
+  // with sigma-mass insertions (condensate.c:216-230)
+  z2();
+  check(cudaMemcpyAsync(z, vec, 2 * V * sizeof(double), cudaMemcpyDeviceToDevice, stream_), "copy z");
+  cond_fill(3, nullptr, nullptr, sm, vec);
+  solve1(vec);
+  dirac(sm, target, D, 2, GN_OP_MT);
+  cond_fill(3, nullptr, nullptr, sm, D);
+  solve1(D);
+  dirac(sm, target, D, 2, GN_OP_MT);
+  cond_dots(z, D, q);
+  out[10] = q[0];
+  check(cudaStreamSynchronize(stream_), "condensate");
+  return all_ok ? GN_OK : GN_NOT_CONVERGED;
+}
+
+}  // namespace gn

@@ -1,0 +1,134 @@
+// engine.h -- internal C++ interface of the device engine behind the C-ABI.
+// One Engine per lattice (L) and device; it owns every device buffer of that
+// lattice and one CUDA stream.  All fields live in the reference's fermion
+// order (see geometry.cuh) as real planes of V = L^3 values.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/gn_b200.h"
+#include "cg_kernel.cuh"
+#include "geometry.cuh"
+
+namespace gn {
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+};
+
+// Result of one solve, per right-hand side.
+struct SolveInfo {
+  int status;       // CgStatus
+  long long iters;  // iterations the reference would count (0 if not counted)
+  double r2;        // final |r|^2 of the stopping test
+  double b2;
+  long long inner;  // mixed precision: low-precision iterations
+  long long reliable;  // mixed precision: reliable updates
+};
+
+class Engine {
+ public:
+  Engine(int L, int device);
+  ~Engine();
+
+  int L() const { return L_; }
+  int64_t V() const { return V_; }
+  const Geom &geom() const { return g_; }
+  cudaStream_t stream() const { return stream_; }
+  int device() const { return device_; }
+
+  // ---- device-pointer operations (asynchronous on stream(), FP64)
+  void sigma_mass(const double *sigma, const double *P, double eps, double *sigma_out, double *sm);
+  void dirac(const double *sm, const double *in, double *out, int ncomp, int op);
+  void momenta(double *P, const double *F, double eps);
+  void force(const double *X, const double *Y, const double *sigma, double beta_s, double *F, double *P, double pcoef);
+  // H terms (sum P^2/2, sum 1/2 phi X, sum sigma^2), compensated; synchronises.
+  void energy_terms(const double *P, const double *phi, const double *X, const double *sigma, double out[3]);
+  // sum Re(conj v D)/V, sum Re(conj v D), sum Im(conj v D); synchronises.
+  void cond_dots(const double *v, const double *D, double out[3]);
+  void cond_fill(int mode, const signed char *signs, const double *table, const double *sm, double *v);
+
+  // CG on M M^T for nrhs right-hand sides of ncomp planes each (b[k], x[k] are
+  // device pointers of ncomp*V).  precision: GN_PREC_FP64 or GN_PREC_MIXED.
+  // Synchronises and fills info[k].
+  int solve(const double *sm, const double *const *b, double *const *x, int nrhs, int ncomp, double tol, int variant,
+            int rel, long long max_iter, int precision, SolveInfo *info);
+
+  // ---- resident sigma-HMC state
+  double *sigma() { return sigma_[cur_]; }
+  double *sigma_alt() { return sigma_[cur_ ^ 1]; }
+  void swap_sigma() { cur_ ^= 1; }
+  double *sm() { return sm_; }
+  double *P() { return P_; }
+  double *F() { return F_; }
+  double *chi() { return chi_; }
+  double *phi() { return phi_; }
+  double *X() { return X_; }
+  double *Y() { return Y_; }
+  double *scratch(int i) { return scratch_[i]; }  // 4 scratch planes pairs of 2V
+  signed char *signs() { return signs_; }
+  double *table() { return table_; }
+  double distance = 0.0;  // lat->distance_sigma of the resident state
+  long long launches = 0; // kernels launched by this engine (for launch accounting)
+
+  // One trajectory on the resident state; see gn_trajectory in gn_b200.h.
+  int trajectory(const gn_hmc_params &hp, double (*gauss)(void), double (*uniform)(void), const double *pre_P,
+                 const double *pre_chi, gn_traj_result *res);
+
+  // Full condensate measurement (condensate.c:114-244) on device pointers.
+  int condensate(const double *sm, double tol, double *target, double *D, double (*uniform)(void), double out[11],
+                 double *iterations, long long *calls, int precision);
+
+  // host staging (pinned), at least 4*V doubles
+  double *host_stage() { return h_stage_; }
+  int *abort_flag_host() { return h_abort_; }
+
+  void check(cudaError_t e, const char *what);
+
+ private:
+  int finish_solve(int nrhs, SolveInfo *info);
+  void mixed_init();
+  const void *mixed_kernel_ptr(int ncomp);
+  int solve_mixed(const double *sm, const double *const *b, double *const *x, int nrhs, int ncomp, double tol,
+                  int variant, int rel, long long max_iter, SolveInfo *info);
+  void *alloc(size_t bytes);
+  int cg_blocks(int ncomp, bool mixed);
+
+  int L_, device_;
+  int64_t V_;
+  Geom g_;
+  cudaStream_t stream_ = nullptr;
+  int num_sms_ = 0;
+  std::vector<void *> allocs_;
+  double *sigma_[2] = {nullptr, nullptr};
+  int cur_ = 0;
+  double *sm_ = nullptr, *P_ = nullptr, *F_ = nullptr;
+  double *chi_ = nullptr, *phi_ = nullptr, *X_ = nullptr, *Y_ = nullptr;
+  double *scratch_[4] = {nullptr, nullptr, nullptr, nullptr};
+  signed char *signs_ = nullptr;
+  double *table_ = nullptr;
+  // solver workspace
+  double *cg_work_ = nullptr;  // kMaxRhs * 4 vectors * 2 planes * V
+  float *mx_work_ = nullptr;   // mixed precision: kMaxRhs * 6 vectors * 2 planes * V
+  float *sm32_ = nullptr;
+  double *partials_ = nullptr;
+  double *h_partials_ = nullptr;
+  GridBar *bar_ = nullptr;
+  int *err_ = nullptr;
+  CgState *state_ = nullptr;
+  CgState *h_state_ = nullptr;
+  int *h_abort_ = nullptr;
+  int *d_abort_ = nullptr;
+  double *h_stage_ = nullptr;
+  int max_blocks_ = 0;
+  int cg_blocks_cache_[2][2] = {{0, 0}, {0, 0}};
+};
+
+// Host-side compensated sum of (hi, lo) block partials.
+double sum_partials(const double *part, int nb, int q);
+
+}  // namespace gn

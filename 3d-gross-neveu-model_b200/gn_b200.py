@@ -1,0 +1,333 @@
+"""Python front-end of the B200 fermion path (ctypes over include/gn_b200.h).
+
+The product is the CUDA library lib/libgn_b200.so; this module only marshals
+numpy arrays.  There is no CPU fallback: if the library cannot be loaded or no
+sm_100 device is present, every call raises.
+
+Fields are float64 arrays in the reference's fermion order (lexicographic
+(x0*L + x1)*L + x2 with x2 = time fastest, even sites first).  Complex fields
+(numpy complex128) are passed as two real planes.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "lib" / "libgn_b200.so"
+
+GN_OK, GN_NOT_CONVERGED = 0, 1
+GN_OP_M, GN_OP_MT, GN_OP_SUB_M = 0, 1, 2
+GN_PREC_FP64, GN_PREC_MIXED = 0, 1
+GN_LFMN2VF, GN_LF2, GN_LFMN2 = 0, 1, 2
+GN_F_P, GN_F_F, GN_F_CHI, GN_F_PHI, GN_F_X, GN_F_Y, GN_F_SIGMA, GN_F_SM = range(8)
+STATUS_NAMES = {0: "GN_OK", 1: "GN_NOT_CONVERGED", -1: "GN_ERR_ARG", -2: "GN_ERR_CUDA", -3: "GN_ERR_TIMEOUT",
+                -4: "GN_ERR_ABORTED", -5: "GN_ERR_NO_DEVICE"}
+DRAW_FN = C.CFUNCTYPE(C.c_double)
+
+
+class GnError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class CgInfo(C.Structure):
+    _fields_ = [("status", C.c_int), ("counted", C.c_int), ("iterations", C.c_longlong), ("residual", C.c_double),
+                ("b_norm", C.c_double), ("inner_iterations", C.c_longlong), ("reliable_updates", C.c_longlong)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class HmcParams(C.Structure):
+    _fields_ = [("beta_s", C.c_double), ("eps", C.c_double), ("steps", C.c_int), ("integrator", C.c_int),
+                ("tol_medium", C.c_double), ("tol_high", C.c_double), ("relative", C.c_int), ("precision", C.c_int)]
+
+
+class TrajResult(C.Structure):
+    _fields_ = [("ok", C.c_int), ("accepted", C.c_int), ("dH", C.c_double), ("H0", C.c_double), ("H1", C.c_double),
+                ("cg_iterations", C.c_double), ("cg_calls", C.c_longlong), ("distance", C.c_double),
+                ("inner_iterations", C.c_longlong), ("reliable_updates", C.c_longlong)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_dp = C.POINTER(C.c_double)
+_lib = None
+
+
+def load_library(build_if_missing: bool = True) -> C.CDLL:
+    """Load lib/libgn_b200.so (compiling it with nvcc first if it is absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists() and build_if_missing:
+        import importlib.util
+        spec = importlib.util.spec_from_file_location("gn_build", PKG / "build.py")
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        mod.build()
+    lib = C.CDLL(str(LIB_PATH))
+    v = C.c_void_p
+    sig = {
+        "gn_create": ([C.POINTER(v), C.c_int, C.c_int], C.c_int),
+        "gn_destroy": ([v], None),
+        "gn_last_error": ([], C.c_char_p),
+        "gn_volume": ([v], C.c_longlong),
+        "gn_request_abort": ([v, C.c_int], None),
+        "gn_sigma_mass": ([v, _dp, _dp], C.c_int),
+        "gn_dirac": ([v, _dp, _dp, _dp, C.c_int, C.c_int], C.c_int),
+        "gn_cg": ([v, _dp, _dp, _dp, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_longlong, C.c_int,
+                   C.POINTER(CgInfo)], C.c_int),
+        "gn_sigma_force": ([v, C.c_double, _dp, _dp, _dp, _dp, _dp, C.c_double, _dp, C.c_int, C.POINTER(CgInfo)],
+                           C.c_int),
+        "gn_energy": ([v, C.c_double, _dp, _dp, _dp, _dp, _dp], C.c_int),
+        "gn_evolve_sigma": ([v, _dp, _dp, _dp, C.c_double], C.c_int),
+        "gn_evolve_momenta": ([v, _dp, _dp, C.c_double], C.c_int),
+        "gn_condensate": ([v, _dp, C.c_double, _dp, _dp, C.c_void_p, _dp, _dp, C.POINTER(C.c_longlong), C.c_int],
+                          C.c_int),
+        "gn_load_sigma": ([v, _dp], C.c_int),
+        "gn_store_sigma": ([v, _dp, _dp], C.c_int),
+        "gn_read_state": ([v, C.c_int, _dp], C.c_int),
+        "gn_write_state": ([v, C.c_int, _dp], C.c_int),
+        "gn_trajectory": ([v, C.POINTER(HmcParams), C.c_void_p, C.c_void_p, C.POINTER(TrajResult)], C.c_int),
+        "gn_stream": ([v], C.c_void_p),
+        "gn_field_ptr": ([v, C.c_int], C.c_void_p),
+        "gn_dirac_device": ([v, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int], C.c_int),
+        "gn_cg_device": ([v, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int,
+                          C.c_longlong, C.c_int, C.POINTER(CgInfo)], C.c_int),
+        "gn_trajectory_device": ([v, C.POINTER(HmcParams), C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.POINTER(TrajResult)], C.c_int),
+        "gn_launch_count": ([v], C.c_longlong),
+        "gn_flush_l2": ([v], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def _p(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _planes(a) -> tuple[np.ndarray, int]:
+    """complex -> (re, im) planes; real -> itself."""
+    if np.iscomplexobj(a):
+        return np.ascontiguousarray(np.concatenate([a.real, a.imag]), np.float64), 2
+    return np.ascontiguousarray(a, np.float64), 1
+
+
+def _unplanes(a: np.ndarray, nc: int, V: int):
+    return a[:V] + 1j * a[V:] if nc == 2 else a
+
+
+def fn_address(f) -> int | None:
+    """Address of a C function for the random-number hooks: accepts an int, a
+    ctypes function pointer or a Python callable (wrapped; keep a reference)."""
+    if f is None:
+        return None
+    if isinstance(f, int):
+        return f
+    if isinstance(f, C._CFuncPtr):
+        return C.cast(f, C.c_void_p).value
+    cb = DRAW_FN(f)
+    _keepalive.append(cb)
+    return C.cast(cb, C.c_void_p).value
+
+
+_keepalive: list = []
+
+
+class Lattice:
+    """A device-resident L^3 lattice (one gn_context)."""
+
+    def __init__(self, L: int, device: int = 0):
+        self.lib = load_library()
+        self.ctx = C.c_void_p()
+        self._check(self.lib.gn_create(C.byref(self.ctx), L, device))
+        self.L = L
+        self.V = L ** 3
+
+    def close(self):
+        if self.ctx:
+            self.lib.gn_destroy(self.ctx)
+            self.ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, st: int, allow=(GN_OK,)):
+        if st not in allow:
+            raise GnError(st, self.lib.gn_last_error().decode())
+        return st
+
+    # ---- operators
+    def sigma_mass(self, sigma):
+        s = np.ascontiguousarray(sigma, np.float64)
+        sm = np.empty(self.V)
+        self._check(self.lib.gn_sigma_mass(self.ctx, _p(s), _p(sm)))
+        return sm
+
+    def dirac(self, sm, psi, op=GN_OP_M, out=None):
+        inp, nc = _planes(psi)
+        if op == GN_OP_SUB_M:
+            o, _ = _planes(out)
+            o = o.copy()
+        else:
+            o = np.zeros_like(inp)
+        self._check(self.lib.gn_dirac(self.ctx, _p(np.ascontiguousarray(sm, np.float64)), _p(inp), _p(o), nc, op))
+        return _unplanes(o, nc, self.V)
+
+    def cg(self, sm, b, x0=None, tol=1e-9, variant=0, relative=False, max_iter=0, precision=GN_PREC_FP64):
+        """Solve (M M^T) x = b.  b: (V,) or (nrhs, V), real or complex.  Returns (x, infos, status)."""
+        b = np.asarray(b)
+        single = b.ndim == 1
+        bb = b[None] if single else b
+        nrhs = bb.shape[0]
+        cplx = np.iscomplexobj(bb) or (x0 is not None and np.iscomplexobj(x0))
+        nc = 2 if cplx else 1
+        if cplx:
+            bb = bb.astype(np.complex128)
+            bp = np.concatenate([np.concatenate([r.real, r.imag]) for r in bb])
+        else:
+            bp = bb.astype(np.float64).reshape(-1)
+        if x0 is None:
+            xp = np.zeros_like(bp)
+        else:
+            xx = np.asarray(x0)
+            xx = xx[None] if xx.ndim == 1 else xx
+            xp = (np.concatenate([np.concatenate([r.real, r.imag]) for r in xx.astype(np.complex128)]) if cplx
+                  else xx.astype(np.float64).reshape(-1))
+        bp = np.ascontiguousarray(bp)
+        xp = np.ascontiguousarray(xp, np.float64).copy()
+        infos = (CgInfo * nrhs)()
+        st = self._check(self.lib.gn_cg(self.ctx, _p(np.ascontiguousarray(sm, np.float64)), _p(bp), _p(xp), nrhs,
+                                        nc, tol, variant, int(relative), max_iter, precision, infos),
+                         allow=(GN_OK, GN_NOT_CONVERGED))
+        V = self.V
+        xs = [_unplanes(xp[k * nc * V:(k + 1) * nc * V], nc, V) for k in range(nrhs)]
+        x = xs[0] if single else np.stack(xs)
+        return x, [i.as_dict() for i in infos], st
+
+    def sigma_force(self, beta_s, sigma, sm, phi, X, tol, precision=GN_PREC_FP64):
+        phi = np.ascontiguousarray(phi, np.float64).reshape(-1)
+        Xp = np.array(X, np.float64).reshape(-1)
+        Y = np.zeros(2 * self.V)
+        F = np.zeros(self.V)
+        infos = (CgInfo * 2)()
+        st = self._check(self.lib.gn_sigma_force(self.ctx, beta_s, _p(np.ascontiguousarray(sigma, np.float64)),
+                                                 _p(np.ascontiguousarray(sm, np.float64)), _p(phi), _p(Xp), _p(Y),
+                                                 tol, _p(F), precision, infos), allow=(GN_OK, GN_NOT_CONVERGED))
+        return F, Xp.reshape(2, -1), Y.reshape(2, -1), [i.as_dict() for i in infos], st
+
+    def energy(self, beta_s, sigma, P, phi, X):
+        H = C.c_double()
+        self._check(self.lib.gn_energy(self.ctx, beta_s, _p(np.ascontiguousarray(sigma, np.float64)),
+                                       _p(np.ascontiguousarray(P, np.float64)),
+                                       _p(np.ascontiguousarray(phi, np.float64).reshape(-1)),
+                                       _p(np.ascontiguousarray(X, np.float64).reshape(-1)), C.byref(H)))
+        return H.value
+
+    def evolve_sigma(self, sigma, P, eps):
+        s = np.array(sigma, np.float64)
+        sm = np.empty(self.V)
+        self._check(self.lib.gn_evolve_sigma(self.ctx, _p(s), _p(sm), _p(np.ascontiguousarray(P, np.float64)), eps))
+        return s, sm
+
+    def evolve_momenta(self, P, F, eps):
+        p = np.array(P, np.float64)
+        self._check(self.lib.gn_evolve_momenta(self.ctx, _p(p), _p(np.ascontiguousarray(F, np.float64)), eps))
+        return p
+
+    def condensate(self, sm, tol, target, uniform, precision=GN_PREC_FP64):
+        t = np.concatenate([np.real(target), np.imag(target)]).astype(np.float64)
+        D = np.zeros(2 * self.V)
+        out = np.zeros(11)
+        it = C.c_double()
+        calls = C.c_longlong()
+        st = self._check(self.lib.gn_condensate(self.ctx, _p(np.ascontiguousarray(sm, np.float64)), tol, _p(t), _p(D),
+                                                fn_address(uniform), _p(out), C.byref(it), C.byref(calls), precision),
+                         allow=(GN_OK, GN_NOT_CONVERGED))
+        V = self.V
+        return out, t[:V] + 1j * t[V:], D[:V] + 1j * D[V:], it.value, calls.value, st
+
+    # ---- resident state
+    def load_sigma(self, sigma):
+        self._check(self.lib.gn_load_sigma(self.ctx, _p(np.ascontiguousarray(sigma, np.float64))))
+
+    def store_sigma(self):
+        s = np.empty(self.V)
+        sm = np.empty(self.V)
+        self._check(self.lib.gn_store_sigma(self.ctx, _p(s), _p(sm)))
+        return s, sm
+
+    def read_state(self, field):
+        n = self.V if field in (GN_F_P, GN_F_F) else 2 * self.V
+        a = np.empty(n)
+        self._check(self.lib.gn_read_state(self.ctx, field, _p(a)))
+        return a if n == self.V else a.reshape(2, self.V)
+
+    def write_state(self, field, a):
+        self._check(self.lib.gn_write_state(self.ctx, field, _p(np.ascontiguousarray(a, np.float64).reshape(-1))))
+
+    def trajectory(self, beta_s, eps, steps, gauss=None, uniform=None, integrator=GN_LFMN2VF, tol_medium=1e-3,
+                   tol_high=1e-9, relative=False, precision=GN_PREC_FP64):
+        hp = HmcParams(beta_s, eps, steps, integrator, tol_medium, tol_high, int(relative), precision)
+        res = TrajResult()
+        self._check(self.lib.gn_trajectory(self.ctx, C.byref(hp), fn_address(gauss), fn_address(uniform),
+                                           C.byref(res)), allow=(GN_OK, GN_NOT_CONVERGED))
+        return res.as_dict()
+
+    def request_abort(self, on=True):
+        self.lib.gn_request_abort(self.ctx, int(on))
+
+    # ---- device-resident entry points (pointers are ints)
+    @property
+    def stream(self) -> int:
+        return self.lib.gn_stream(self.ctx)
+
+    def field_ptr(self, field) -> int:
+        return self.lib.gn_field_ptr(self.ctx, field)
+
+    def dirac_device(self, sm_ptr, in_ptr, out_ptr, ncomp=1, op=GN_OP_M):
+        self._check(self.lib.gn_dirac_device(self.ctx, sm_ptr, in_ptr, out_ptr, ncomp, op))
+
+    def cg_device(self, sm_ptr, b_ptr, x_ptr, nrhs, ncomp=1, tol=1e-9, variant=1, relative=False, max_iter=0,
+                  precision=GN_PREC_FP64):
+        infos = (CgInfo * nrhs)()
+        st = self._check(self.lib.gn_cg_device(self.ctx, sm_ptr, b_ptr, x_ptr, nrhs, ncomp, tol, variant,
+                                               int(relative), max_iter, precision, infos),
+                         allow=(GN_OK, GN_NOT_CONVERGED))
+        return [i.as_dict() for i in infos], st
+
+    def trajectory_device(self, P_ptr, chi_ptr, beta_s, eps, steps, uniform=None, integrator=GN_LFMN2VF,
+                          tol_medium=1e-3, tol_high=1e-9, relative=False, precision=GN_PREC_FP64):
+        hp = HmcParams(beta_s, eps, steps, integrator, tol_medium, tol_high, int(relative), precision)
+        res = TrajResult()
+        self._check(self.lib.gn_trajectory_device(self.ctx, C.byref(hp), P_ptr, chi_ptr, fn_address(uniform),
+                                                  C.byref(res)), allow=(GN_OK, GN_NOT_CONVERGED))
+        return res.as_dict()
+
+    def launch_count(self) -> int:
+        return self.lib.gn_launch_count(self.ctx)
+
+    def flush_l2(self):
+        self._check(self.lib.gn_flush_l2(self.ctx))

@@ -1,0 +1,456 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 fermion path: sigma-HMC trajectories per second at L = 64.
+
+Workload (one "step" = one trajectory): L = 64 (V = 262,144 sites), beta_s =
+0.85, sigma i.i.d. N(0, 2/(N_f beta_s)) on the dual sites, the reference's
+default integrator LFMN2VF with 10 steps of eps = 0.05, two pseudofermion
+flavours, every CG solve stopped at a true relative residual of 1e-10.
+Synthetic data: momenta and chi drawn N(0, 1) (seeded), as the reference
+draws them.
+
+  value      mixed-precision solver, draws already resident in HBM, CUDA events
+             on the library's stream; L2 flushed (512 MB write) before every
+             trajectory, inside the timed region.
+  e2e        the same trajectories through the host-buffer C-ABI: per step the
+             draws are copied from pinned host memory (gn_write_state), the
+             trajectory runs (gn_trajectory) and sigma / sigma-mass are read
+             back (gn_store_sigma); host wall clock.
+  roofline   the dominant kernel: the persistent CG kernel (mixed precision,
+             two flavours) of one solve; algorithmic bytes from its iteration
+             counts, duration from CUDA events.
+  cpu_baseline / --impl reference: the reference's own C code (compiled from
+             its sources into oracle/_ref/) on the host cores.
+
+Multi-GPU: one process per GPU, each an independent chain (the path does not
+shard; replicas only), max over ranks of the timed region.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+PKG = ROOT / "3d-gross-neveu-model_b200"
+for _p in (str(ROOT), str(PKG)):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+L_DEFAULT = 64
+BETA_S = 0.85
+NFLAV = 4
+METRIC = "HMC trajectories/s at L=64 (LFMN2VF, 10 x eps 0.05, CG to 1e-10 true relative residual)"
+UNIT = "traj/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--L", type=int, default=L_DEFAULT)
+    ap.add_argument("--md-steps", type=int, default=10)
+    ap.add_argument("--eps", type=float, default=0.05)
+    ap.add_argument("--tol", type=float, default=1e-10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- distributed
+def dist_setup(backend):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def dist_max(x, world, device=None):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------- clocks
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.device), "-lms", "200"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in open(self.path):
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm), "power_w_max": max(power)}
+
+
+# ---------------------------------------------------------------- reference (CPU)
+def _ref_solve_worker(args):
+    """One reference CG solve (StartX0Imposed..., conjugategradient.c:115) at L
+    from x = 0 on b = M chi, at the absolute tolerance equal to tol * |b|."""
+    L, tol, seed = args
+    sys.path.insert(0, str(ROOT))
+    from oracle.oracle import Ref
+    ref = Ref(L, build=False)
+    ref.init(1231, BETA_S, 0.05, 10)
+    rng = np.random.default_rng(seed)
+    V = L ** 3
+    ref.set_sigma(rng.normal(0.0, np.sqrt(2.0 / (NFLAV * BETA_S)), V))
+    b = ref.dirac(rng.normal(size=V).astype(complex), 0)
+    tol_abs = tol * float(np.linalg.norm(b))
+    t0 = time.perf_counter()
+    _, ok = ref.cg(b, None, tol_abs, 1)
+    dt = time.perf_counter() - t0
+    it, _ = ref.counters()
+    return dt, it
+
+
+def _port_solve(L, tol, seed):
+    sys.path.insert(0, str(ROOT))
+    from oracle.oracle import Port
+    port = Port()
+    rng = np.random.default_rng(seed)
+    V = L ** 3
+    sm = port.sigma_mass(L, rng.normal(0.0, np.sqrt(2.0 / (NFLAV * BETA_S)), V))
+    b = port.dirac(L, sm, rng.normal(size=V), 0)
+    t0 = time.perf_counter()
+    _, ok, it, _ = port.cg(L, sm, b, None, tol * float(np.linalg.norm(b)), 1)
+    return time.perf_counter() - t0, it
+
+
+def reference_available(L):
+    from oracle import build_ref
+    return build_ref.lib_path(L, 0).exists()
+
+
+def solves_per_trajectory(md_steps):
+    # 2 flavours x (1 initial solve + (2 md_steps + 1) forces), minus the first
+    # force, whose start vector is already the solution (conjugategradient.c:16-27)
+    return 2 * (1 + 2 * md_steps + 1) - 2
+
+
+def cpu_reference_rate(L, tol, md_steps, procs=1, seed=0):
+    """traj/s of the reference from a bounded sample: per process one full CG
+    solve at L, scaled by the solves of one trajectory.  Returns (rate, info)."""
+    nsol = solves_per_trajectory(md_steps)
+    if reference_available(L):
+        kind = "reference"
+        if procs == 1:
+            res = [_ref_solve_worker((L, tol, seed))]
+        else:
+            import multiprocessing as mp
+            ctx = mp.get_context("spawn")
+            with ctx.Pool(procs) as pool:
+                res = pool.map(_ref_solve_worker, [(L, tol, seed + i) for i in range(procs)])
+    else:
+        kind = "port"
+        res = [_port_solve(L, tol, seed)]
+        procs = 1
+    t_solve = statistics.median(r[0] for r in res)
+    its = statistics.median(r[1] for r in res)
+    rate = procs / (nsol * t_solve)
+    info = {"kind": kind, "cores": procs,
+            "sample": (f"{procs} process(es) x one CG solve from x=0 at L={L} to |r| < {tol:g}|b| "
+                       f"({its:.0f} iterations, {t_solve:.2f} s median), scaled by the {nsol} solves of one "
+                       f"trajectory")}
+    return rate, info
+
+
+def run_reference(a, world, rank):
+    if rank != 0:
+        return
+    ncores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    procs = max(1, min(ncores, 64))
+    for _ in range(min(a.warmup, 1)):
+        cpu_reference_rate(a.L, a.tol, a.md_steps, 1)
+    rates, infos = [], []
+    for s in range(a.steps):
+        r, info = cpu_reference_rate(a.L, a.tol, a.md_steps, procs, seed=100 * s)
+        rates.append(r)
+        infos.append(info)
+    value = statistics.median(rates)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": 1000.0 / value * infos[0]["cores"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"sigma-HMC LFMN2VF L={a.L} beta_s={BETA_S} steps={a.md_steps} eps={a.eps} "
+                                   f"CG rel {a.tol:g}", "l2": "n/a (CPU)"},
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": infos[0]["cores"], "kind": infos[0]["kind"],
+                             "sample": infos[0]["sample"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- ours (GPU)
+def cuda_events():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def run_ours(a, world, rank, local):
+    import torch
+
+    import gn_b200 as G
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    L, V = a.L, a.L ** 3
+    lat = G.Lattice(L, local)
+    stream = torch.cuda.ExternalStream(lat.stream, device=dev)
+    rng = np.random.default_rng(1231 + rank)
+    sigma0 = rng.normal(0.0, np.sqrt(2.0 / (NFLAV * BETA_S)), V)
+    nsteps = a.warmup + a.steps
+    # draws for every trajectory, resident on the device (value) and pinned on the host (e2e)
+    draws_h = torch.empty((nsteps, 3 * V), dtype=torch.float64, pin_memory=True)
+    draws_h.numpy()[:] = rng.normal(size=(nsteps, 3 * V))
+    draws_d = draws_h.to(dev)
+    torch.cuda.synchronize(dev)
+    unif = rng.uniform(size=4 * nsteps + 16)
+    upos = [0]
+
+    def uniform():
+        upos[0] += 1
+        return float(unif[(upos[0] - 1) % len(unif)])
+
+    ucb = G.DRAW_FN(uniform)
+    params = dict(tol_medium=a.tol, tol_high=a.tol, relative=True)
+
+    def traj_dev(s, prec):
+        base = draws_d[s].data_ptr()
+        return lat.trajectory_device(base, base + 8 * V, BETA_S, a.eps, a.md_steps, ucb, precision=prec, **params)
+
+    results = {}
+    for prec, name in ((G.GN_PREC_MIXED, "mixed"), (G.GN_PREC_FP64, "fp64")):
+        lat.load_sigma(sigma0)
+        for s in range(a.warmup):
+            traj_dev(s, prec)
+        l0 = lat.launch_count()
+        dist_barrier(world)
+        torch.cuda.synchronize(dev)
+        clocks = Clocks(local)
+        clocks.start()
+        e0, e1 = cuda_events()
+        e0.record(stream)
+        out = []
+        for s in range(a.warmup, nsteps):
+            lat.flush_l2()
+            out.append(traj_dev(s, prec))
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ck = clocks.stop()
+        dist_barrier(world)
+        ms = e0.elapsed_time(e1)
+        ms = dist_max(ms, world, dev)
+        results[name] = dict(ms=ms, out=out, clocks=ck, launches=(lat.launch_count() - l0) / a.steps)
+
+    # e2e: host buffers through the C-ABI
+    lat.load_sigma(sigma0)
+    hv = draws_h.numpy()
+    sig_out = np.empty(V)
+    sm_out = np.empty(V)
+    for s in range(a.warmup):
+        lat.write_state(G.GN_F_P, hv[s, :V])
+        lat.write_state(G.GN_F_CHI, hv[s, V:])
+        lat.trajectory(BETA_S, a.eps, a.md_steps, None, ucb, precision=G.GN_PREC_MIXED, **params)
+    dist_barrier(world)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for s in range(a.warmup, nsteps):
+        lat.write_state(G.GN_F_P, hv[s, :V])
+        lat.write_state(G.GN_F_CHI, hv[s, V:])
+        lat.trajectory(BETA_S, a.eps, a.md_steps, None, ucb, precision=G.GN_PREC_MIXED, **params)
+        lat.lib.gn_store_sigma(lat.ctx, sig_out.ctypes.data_as(G._dp), sm_out.ctypes.data_as(G._dp))
+    torch.cuda.synchronize(dev)
+    e2e_s = dist_max(time.perf_counter() - t0, world, dev)
+
+    # dominant kernel: one two-flavour mixed CG solve, events around the kernel
+    roof = kernel_roofline(lat, stream, a, G)
+    dirac = dirac_roofline(G, stream, dev)
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        rate, info = cpu_reference_rate(L, a.tol, a.md_steps, 1)
+        cpu = {"value": rate, "unit": UNIT, **info}
+
+    mixed, fp64 = results["mixed"], results["fp64"]
+    value = world * a.steps / (mixed["ms"] / 1000.0)
+    fp64_rate = world * a.steps / (fp64["ms"] / 1000.0)
+    peaks = load_peaks()
+    iters = [o["inner_iterations"] for o in mixed["out"]]
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": mixed["ms"] / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 inner / f64 reliable updates, f64 dH", "data": "synthetic (seeded N(0,1) momenta and chi)",
+            "config": {"workload": f"sigma-HMC LFMN2VF L={L} (V={V}) beta_s={BETA_S} steps={a.md_steps} "
+                                   f"eps={a.eps}, every CG to |r| < {a.tol:g}|b| (true residual)",
+                       "L": L, "parallelism": f"replicas x{world}",
+                       "l2": "flushed (512 MB write) before every trajectory, inside the timed region"},
+            "fp64": {"value": fp64_rate, "unit": UNIT, "ms_per_step": fp64["ms"] / a.steps,
+                     "cg_iterations_per_traj": statistics.mean(o["cg_iterations"] for o in fp64["out"])},
+            "mixed_over_fp64": value / fp64_rate,
+            "mixed_detail": {"inner_iterations_per_traj": statistics.mean(iters),
+                             "reliable_updates_per_traj": statistics.mean(o["reliable_updates"] for o in mixed["out"]),
+                             "acceptance": statistics.mean(o["accepted"] for o in mixed["out"]),
+                             "dH": [round(o["dH"], 6) for o in mixed["out"]]},
+            "e2e": {"value": world * a.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 3 * V * 8,
+                    "d2h_bytes_per_step": 2 * V * 8},
+            "roofline": roof_json(roof, peaks),
+            "dirac_roofline": roof_json(dirac, peaks),
+            "cpu_baseline": cpu,
+            "clocks": mixed["clocks"],
+            "gpu_launches": int(round(mixed["launches"] * a.steps))}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    lat.close()
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d.get("hbm_gbs", 6650.0), "src": "measured"}
+    return {"hbm_gbs": 6650.0, "src": "fallback"}
+
+
+def roof_json(r, peaks):
+    if r is None:
+        return None
+    peak = peaks["hbm_gbs"]
+    return {"bound": "hbm", "achieved": r["gbs"], "peak": peak, "unit": "GB/s", "frac": r["gbs"] / peak,
+            "traffic": r.get("traffic"), "kernel": r["kernel"], "note": r["note"] + f"; peak {peaks['src']}"}
+
+
+def kernel_roofline(lat, stream, a, G):
+    """Persistent CG kernel, mixed precision, 2 flavours, b = the resident phi,
+    x = 0, tol 1e-10 relative.  Algorithmic bytes per site: inner iteration
+    8 + 40 nrhs, reliable update 80 per system, start 40 per system."""
+    V = lat.V
+    sm = lat.field_ptr(G.GN_F_SM)
+    phi = lat.field_ptr(G.GN_F_PHI)
+    x = lat.field_ptr(G.GN_F_X)
+    times = []
+    for rep in range(4):
+        lat.flush_l2()
+        e0, e1 = cuda_events()
+        e0.record(stream)
+        infos, st = lat.cg_device(sm, phi, x, 2, 1, a.tol, 1, True, 0, G.GN_PREC_MIXED)
+        e1.record(stream)
+        e1.synchronize()
+        if rep:
+            times.append(e0.elapsed_time(e1))
+    ms = statistics.median(times)
+    inner = max(i["inner_iterations"] for i in infos)
+    ru = sum(i["reliable_updates"] for i in infos)
+    nbytes = V * ((8 + 40 * 2) * inner + 80 * ru + 40 * 2)
+    return {"gbs": nbytes / (ms * 1e-3) / 1e9, "kernel": "cg_mixed_kernel<1> (2 flavours, L=%d)" % lat.L,
+            "ms": ms, "bytes": nbytes, "traffic": None,
+            "note": f"{inner} inner iterations, {ru} reliable updates, {ms:.3f} ms per launch; working set "
+                    f"{(2 * 5 * 4 + 8 * 3) * V / 1e6:.0f} MB is L2-resident within the solve"}
+
+
+def dirac_roofline(G, stream, dev):
+    """Dirac M on one FP64 plane at L = 128 (V = 2,097,152), L2 flushed before
+    every launch.  Algorithmic bytes 3 * 8 * V (psi, sm in; out)."""
+    L = 128
+    lat = G.Lattice(L, dev.index)
+    sm = lat.field_ptr(G.GN_F_SM)
+    X = lat.field_ptr(G.GN_F_X)
+    Y = lat.field_ptr(G.GN_F_Y)
+    s = torch_stream = None
+    import torch
+    torch_stream = torch.cuda.ExternalStream(lat.stream, device=dev)
+    times = []
+    for rep in range(12):
+        lat.flush_l2()
+        e0, e1 = cuda_events()
+        e0.record(torch_stream)
+        lat.dirac_device(sm, X, Y, 1, G.GN_OP_M)
+        e1.record(torch_stream)
+        e1.synchronize()
+        if rep >= 2:
+            times.append(e0.elapsed_time(e1))
+    ms = statistics.median(times)
+    V = L ** 3
+    nbytes = 3 * 8 * V
+    lat.close()
+    return {"gbs": nbytes / (ms * 1e-3) / 1e9, "kernel": "dirac_kernel<double,M> L=128 cold", "ms": ms,
+            "bytes": nbytes, "traffic": None, "note": f"{ms * 1e3:.1f} us per launch, L2 flushed before each"}
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        world, rank, local = dist_setup("gloo")
+        run_reference(a, world, rank)
+    else:
+        world, rank, local = dist_setup("nccl")
+        run_ours(a, world, rank, local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

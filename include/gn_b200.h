@@ -1,0 +1,212 @@
+/*
+ * gn_b200.h -- C-ABI of the B200 (sm_100a) fermion hot path of the Z2
+ * Gross-Neveu sigma-HMC code alefrajoe/3D-Gross-Neveu-model.
+ *
+ * Plain pointers and sizes only.  One gn_context per lattice size L (even,
+ * 4 <= L <= 256) and device.  Every field is a real array in the reference's
+ * "fermion lexicographic" order (coordinate.c:25-40, :301-313):
+ *   lexicographic n = (x0*L + x1)*L + x2, x2 = time fastest,
+ *   fermion index   = n/2 + ((x0+x1+x2) % 2) * V/2   (even sites first),
+ * V = L^3.  A complex fermion field (the reference stores `double _Complex`)
+ * is passed as two planes of V doubles: real parts, then imaginary parts
+ * (ncomp = 2); ncomp = 1 passes real fields (every field of the sigma path is
+ * real; only the condensate's phase vector is complex).
+ *
+ * Functions taking host pointers copy in, run on the GPU and copy out before
+ * returning.  They replace the reference functions cited beside them with the
+ * same argument meaning; the reference's `struct`-based signatures are
+ * provided on top of these by gn_dropin.h.
+ *
+ * Return values: GN_OK (0) or a negative gn_status; the solvers return
+ * GN_NOT_CONVERGED (1) where the reference returns `false`.
+ * gn_last_error() describes the last failure of the calling thread.
+ */
+#ifndef GN_B200_H
+#define GN_B200_H
+
+#include <stddef.h>
+
+#if defined(__GNUC__)
+#define GN_API __attribute__((visibility("default")))
+#else
+#define GN_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct gn_context gn_context;
+
+enum gn_status {
+  GN_OK = 0,
+  GN_NOT_CONVERGED = 1, /* CG hit its iteration cap: the reference's `return false` */
+  GN_ERR_ARG = -1,      /* bad argument (size, null pointer, L) */
+  GN_ERR_CUDA = -2,     /* a CUDA call failed */
+  GN_ERR_TIMEOUT = -3,  /* a device-side wait ran out (bounded barrier) */
+  GN_ERR_ABORTED = -4,  /* gn_request_abort() stopped a solve */
+  GN_ERR_NO_DEVICE = -5 /* no usable sm_100 device */
+};
+
+enum gn_op { GN_OP_M = 0, GN_OP_MT = 1, GN_OP_SUB_M = 2 };
+enum gn_precision { GN_PREC_FP64 = 0, GN_PREC_MIXED = 1 };
+enum gn_integrator { GN_LFMN2VF = 0, GN_LF2 = 1, GN_LFMN2 = 2 };
+
+/* Per right-hand side outcome of a solve. */
+typedef struct gn_cg_info {
+  int status;          /* 1 converged (counted), 2 start vector already good (not counted), 3 cap, 4 error */
+  int counted;         /* 1 when the reference adds `iterations` to kit->iterations and bumps kit->CG_call */
+  long long iterations;
+  double residual;     /* final |r| of the stopping test */
+  double b_norm;       /* |b| */
+  long long inner_iterations; /* mixed precision: low-precision iterations (else = iterations) */
+  long long reliable_updates; /* mixed precision: FP64 true-residual recomputations */
+} gn_cg_info;
+
+/* Parameters of one sigma-HMC trajectory (moleculardynamics.c:859, :1018, :1234). */
+typedef struct gn_hmc_params {
+  double beta_s;       /* info->beta_scalar */
+  double eps;          /* info->epsilon_sigma_HMC */
+  int steps;           /* info->steps_sigma_HMC (>= 2, info.c:66) */
+  int integrator;      /* gn_integrator; the reference default is GN_LFMN2VF (macro.h:71) */
+  double tol_medium;   /* MEDIUM_PRECISION_INVERSION (1e-3) for the MD forces */
+  double tol_high;     /* HIGH_PRECISION_INVERSION (1e-9) for H0 / H1 */
+  int relative;        /* 0: stop at |r| < tol (reference); 1: at |r| < tol |b| */
+  int precision;       /* gn_precision of the solver */
+} gn_hmc_params;
+
+typedef struct gn_traj_result {
+  int ok;              /* 0 when a solve failed (sigma restored, no uniform drawn) */
+  int accepted;
+  double dH, H0, H1;
+  double cg_iterations; /* added to kit->iterations */
+  long long cg_calls;   /* added to kit->CG_call */
+  double distance;      /* added to lat->distance_sigma */
+  long long inner_iterations, reliable_updates;
+} gn_traj_result;
+
+/* ---- context ---------------------------------------------------------- */
+GN_API int gn_create(gn_context **ctx, int L, int device);
+GN_API void gn_destroy(gn_context *ctx);
+GN_API const char *gn_last_error(void);
+GN_API long long gn_volume(const gn_context *ctx);
+/* Ask a running solve on this context to stop (from another host thread). */
+GN_API void gn_request_abort(gn_context *ctx, int on);
+
+/* ---- host-buffer operators (one call = one reference function) -------- */
+
+/* ComputeFullSigmaMass, sigma.c:75-94: sm(x) = 1/8 sum of sigma over the 8
+ * dual sites of the cube at x. */
+GN_API int gn_sigma_mass(gn_context *ctx, const double *sigma, double *sigmamass);
+
+/* op GN_OP_M:     out = M in      (DiracFermion, dirac.c:46-82)
+ * op GN_OP_MT:    out = M^T in    (AdjDiracFermion, dirac.c:88-123)
+ * op GN_OP_SUB_M: out = out - M in (SubtractDiracFermion, dirac.c:213-247)
+ * in/out hold ncomp planes of V doubles. */
+GN_API int gn_dirac(gn_context *ctx, const double *sigmamass, const double *in, double *out, int ncomp, int op);
+
+/* CG on A = M M^T (conjugategradient.c:13-107 for variant 0, which first tests
+ * the incoming x as the reference does under START_X0_NULL; :115-182 for
+ * variant 1, which starts from x = 0).  nrhs independent systems, each of
+ * ncomp planes: b and x hold nrhs*ncomp*V doubles; x is in/out.  Stops when
+ * |r| < tol (relative = 0, the reference's absolute test) or |r| < tol |b|.
+ * max_iter <= 0 means the reference's cap, V + 1 (macro.h:134).
+ * Returns GN_OK when every system converged, else GN_NOT_CONVERGED. */
+GN_API int gn_cg(gn_context *ctx, const double *sigmamass, const double *b, double *x, int nrhs, int ncomp, double tol,
+          int variant, int relative, long long max_iter, int precision, gn_cg_info *info);
+
+/* ComputeSigmaForce (moleculardynamics.c:631-647): for both flavours X_f =
+ * (M M^T)^-1 phi_f by variant-0 CG from the incoming X_f (tolerance tol), then
+ * Y_f = M^T X_f and F = sum_f 1/8 sum_corners X_f Y_f - (N_f beta_s / 2) sigma.
+ * phi, X, Y hold 2*V doubles (flavour 0 then 1); X in/out, Y and force out.
+ * info[2] (may be NULL). */
+GN_API int gn_sigma_force(gn_context *ctx, double beta_s, const double *sigma, const double *sigmamass, const double *phi,
+                   double *X, double *Y, double tol, double *force, int precision, gn_cg_info *info);
+
+/* ComputeFullEnergyForSigma (moleculardynamics.c:299-319):
+ * H = 1/2 sum P^2 + 1/2 sum_f phi_f . X_f + (N_f beta_s / 4) sum sigma^2. */
+GN_API int gn_energy(gn_context *ctx, double beta_s, const double *sigma, const double *P, const double *phi,
+              const double *X, double *H);
+
+/* EvolveCoordinatesSigma (moleculardynamics.c:824-836): sigma += eps P, then
+ * sigmamass recomputed.  sigma and sigmamass are in/out and out. */
+GN_API int gn_evolve_sigma(gn_context *ctx, double *sigma, double *sigmamass, const double *P, double eps);
+
+/* EvolveMomentaSigma (moleculardynamics.c:843-848): P += eps F. */
+GN_API int gn_evolve_momenta(gn_context *ctx, double *P, const double *F, double eps);
+
+/* ComputeCondensateDirac (condensate.c:114-244) with CONDENSATE_PRECISION 1
+ * and Z2 noise drawn by uniform() (the reference's Casuale, random.c:28),
+ * V draws per noise vector, in the reference's order.
+ * target (2V: complex planes) is target_inverted, in/out (each solve first
+ * tests it, as the reference does); D (2V) receives kit->Ddag_inverted_phi_obs.
+ * out[11] = tr1, |tr1|, tr2, tr4, mu2, mu4, chi, |chi|, chi_p, c12 without
+ * sigma, c12 with sigma.  cg_iterations / cg_calls (may be NULL) receive the
+ * amounts the reference adds to kit->iterations / kit->CG_call. */
+GN_API int gn_condensate(gn_context *ctx, const double *sigmamass, double tol, double *target, double *D,
+                  double (*uniform)(void), double *out, double *cg_iterations, long long *cg_calls, int precision);
+
+/* ---- resident sigma-HMC state ------------------------------------------ */
+
+/* Upload sigma (V doubles) as the resident field; sigmamass is recomputed. */
+GN_API int gn_load_sigma(gn_context *ctx, const double *sigma);
+/* Download the resident sigma and sigmamass (either may be NULL). */
+GN_API int gn_store_sigma(gn_context *ctx, double *sigma, double *sigmamass);
+
+/* Resident vectors for gn_read_state / gn_write_state. */
+enum gn_field { GN_F_P = 0, GN_F_F = 1, GN_F_CHI = 2, GN_F_PHI = 3, GN_F_X = 4, GN_F_Y = 5 };
+/* P and F are V doubles; CHI, PHI, X (kit->inverted_phi), Y (kit->inverted_phi_obs) are 2V. */
+GN_API int gn_read_state(gn_context *ctx, int field, double *out);
+GN_API int gn_write_state(gn_context *ctx, int field, const double *in);
+
+/* One sigma-HMC trajectory on the resident state, the body of
+ * LeapFrog2MinimumNormSigmaVelocityFirst (moleculardynamics.c:1234-1434) or of
+ * LeapFrog2Sigma (:859-1005) / LeapFrog2MinimumNormSigma (:1018-1221):
+ * P and chi_0, chi_1 are drawn on the host with gauss() (V each, in that
+ * order; the reference's Gauss1), phi_f = M chi_f, every solve and MD step
+ * runs on the device, dH is formed in FP64 and the Metropolis test
+ * uniform() <= exp(-dH) is made on the host with the reference's uniform.  On
+ * rejection sigma is restored.  If gauss is NULL, P and chi are taken from the
+ * resident GN_F_P / GN_F_CHI buffers instead (already on the device).
+ * Returns GN_OK, or GN_NOT_CONVERGED when a solve failed (then res->ok = 0 and
+ * sigma is restored, as in the reference). */
+GN_API int gn_trajectory(gn_context *ctx, const gn_hmc_params *params, double (*gauss)(void), double (*uniform)(void),
+                  gn_traj_result *res);
+
+/* ---- device-resident entry points ------------------------------------- */
+
+/* The context's CUDA stream (a cudaStream_t); every device-pointer call below
+ * is ordered on it. */
+GN_API void *gn_stream(gn_context *ctx);
+
+/* Device pointer of a resident field: GN_F_* above, or GN_F_SIGMA / GN_F_SM
+ * (the current sigma and sigmamass, V doubles each). */
+enum { GN_F_SIGMA = 6, GN_F_SM = 7 };
+GN_API double *gn_field_ptr(gn_context *ctx, int field);
+
+/* gn_dirac on device pointers; asynchronous on gn_stream(ctx). */
+GN_API int gn_dirac_device(gn_context *ctx, const double *sigmamass, const double *in, double *out, int ncomp, int op);
+
+/* gn_cg on device pointers (b, x: nrhs*ncomp*V doubles each, not aliased);
+ * returns after the solve (it reads the per-system outcome back). */
+GN_API int gn_cg_device(gn_context *ctx, const double *sigmamass, const double *b, double *x, int nrhs, int ncomp,
+                        double tol, int variant, int relative, long long max_iter, int precision, gn_cg_info *info);
+
+/* gn_trajectory with the draws already on the device: P (V doubles) and
+ * chi (2V doubles, flavour 0 then 1) are device pointers, copied into the
+ * resident buffers on gn_stream(ctx); the Metropolis uniform still comes from
+ * uniform() on the host. */
+GN_API int gn_trajectory_device(gn_context *ctx, const gn_hmc_params *params, const double *P, const double *chi,
+                                double (*uniform)(void), gn_traj_result *res);
+
+/* Number of kernels this context has launched so far. */
+GN_API long long gn_launch_count(gn_context *ctx);
+
+/* Overwrite a device buffer larger than the L2 cache on gn_stream(ctx), so the
+ * next kernel starts cold (used by benchmarks). */
+GN_API int gn_flush_l2(gn_context *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GN_B200_H */
