@@ -62,6 +62,8 @@ def parse():
     ap.add_argument("--eps", type=float, default=0.05)
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--case", choices=["cg64", "dirac128", "traj64"], default=None,
+                    help="run one small case for a profiler instead of the benchmark")
     return ap.parse_args()
 
 
@@ -410,7 +412,7 @@ def kernel_roofline(lat, stream, a, G):
                     f"{(2 * 5 * 4 + 8 * 3) * V / 1e6:.0f} MB is L2-resident within the solve"}
 
 
-def dirac_roofline(G, stream, dev):
+def dirac_roofline(G, stream, dev, reps=12):
     """Dirac M on one FP64 plane at L = 128 (V = 2,097,152), L2 flushed before
     every launch.  Algorithmic bytes 3 * 8 * V (psi, sm in; out)."""
     L = 128
@@ -418,18 +420,17 @@ def dirac_roofline(G, stream, dev):
     sm = lat.field_ptr(G.GN_F_SM)
     X = lat.field_ptr(G.GN_F_X)
     Y = lat.field_ptr(G.GN_F_Y)
-    s = torch_stream = None
     import torch
     torch_stream = torch.cuda.ExternalStream(lat.stream, device=dev)
     times = []
-    for rep in range(12):
+    for rep in range(reps):
         lat.flush_l2()
         e0, e1 = cuda_events()
         e0.record(torch_stream)
         lat.dirac_device(sm, X, Y, 1, G.GN_OP_M)
         e1.record(torch_stream)
         e1.synchronize()
-        if rep >= 2:
+        if rep >= min(2, reps - 1):
             times.append(e0.elapsed_time(e1))
     ms = statistics.median(times)
     V = L ** 3
@@ -439,8 +440,43 @@ def dirac_roofline(G, stream, dev):
             "bytes": nbytes, "traffic": None, "note": f"{ms * 1e3:.1f} us per launch, L2 flushed before each"}
 
 
+def run_case(a):
+    """Small cases for ncu: cg64 = one two-flavour CG solve at L=64 in FP64 and in
+    mixed precision; dirac128 = 3 cold Dirac applies at L=128; traj64 = one
+    mixed-precision trajectory at L=64."""
+    import torch
+
+    import gn_b200 as G
+    dev = torch.device("cuda", 0)
+    if a.case == "dirac128":
+        r = dirac_roofline(G, None, dev, reps=3)
+        print(json.dumps(r))
+        return
+    L, V = 64, 64 ** 3
+    lat = G.Lattice(L, 0)
+    rng = np.random.default_rng(1231)
+    lat.load_sigma(rng.normal(0.0, np.sqrt(2.0 / (NFLAV * BETA_S)), V))
+    draws = torch.tensor(rng.normal(size=3 * V), dtype=torch.float64, device=dev)
+    torch.cuda.synchronize(dev)
+    if a.case == "traj64":
+        r = lat.trajectory_device(draws.data_ptr(), draws.data_ptr() + 8 * V, BETA_S, a.eps, a.md_steps, None,
+                                  tol_medium=a.tol, tol_high=a.tol, relative=True, precision=G.GN_PREC_MIXED)
+        print(json.dumps(r))
+        return
+    lat.write_state(G.GN_F_CHI, draws[V:].cpu().numpy())
+    lat.dirac_device(lat.field_ptr(G.GN_F_SM), lat.field_ptr(G.GN_F_CHI), lat.field_ptr(G.GN_F_PHI), 2, G.GN_OP_M)
+    for prec in (G.GN_PREC_FP64, G.GN_PREC_MIXED):
+        infos, st = lat.cg_device(lat.field_ptr(G.GN_F_SM), lat.field_ptr(G.GN_F_PHI), lat.field_ptr(G.GN_F_X), 2, 1,
+                                  a.tol, 1, True, 0, prec)
+        print(json.dumps({"precision": prec, "status": st, "info": infos}))
+    lat.close()
+
+
 def main():
     a = parse()
+    if a.case:
+        run_case(a)
+        return
     if a.impl == "reference":
         world, rank, local = dist_setup("gloo")
         run_reference(a, world, rank)
