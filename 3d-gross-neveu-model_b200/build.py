@@ -29,6 +29,7 @@ UNITS = {
     "engine.cu": ["--fmad=false"],
     "mixed.cu": [],
     "capi.cu": [],
+    "noalloc.cu": ["--fmad=false"],
 }
 CORE_LIB = LIB / "libgn_b200.so"
 DROPIN_LIB = LIB / "libgn_dropin.so"
