@@ -18,12 +18,11 @@
 // r += (-a) Ap, p = r + b p; no FMA in the FP64 build); only the order of the
 // global sums differs (tree instead of serial).
 #pragma once
-#include "device_common.cuh"
+#include "phase_sync.cuh"
 
 namespace gn {
 
 constexpr int kMaxRhs = 4;
-constexpr int kCgThreads = 256;
 
 enum CgStatus : int {
   kCgRunning = 0,
@@ -56,47 +55,18 @@ struct CgArgs {
   int rel;      // 0: stop at |r| < tol; 1: stop at |r| < tol |b|
   double tol;
   long long max_iter;
-  double *partials;  // [2 slots][2 quantities][kMaxRhs][gridDim.x]
-  GridBar *bar;
+  double *partials;  // [2 slots][kSyncQ][gridDim.x]
+  PhaseBar *bar;
   int *err;
   const int *abort_flag;  // host-mapped; nonzero asks the kernel to stop
   CgState *state;         // [kMaxRhs]
 };
 
-// Every block sums the partials of one slot (8 values per block) and leaves the
-// totals in s_val[0..7].  Warp j sums quantity j; fixed order.
-__device__ __forceinline__ void collect8(const double *part, int nb, double *s_val) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  if (w < 2 * kMaxRhs) {
-    const double *p = part + size_t(w) * nb;
-    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-    int b = lane;
-    for (; b + 96 < nb; b += 128) {
-      s0 += p[b];
-      s1 += p[b + 32];
-      s2 += p[b + 64];
-      s3 += p[b + 96];
-    }
-    for (; b < nb; b += 32) s0 += p[b];
-    double s = warp_sum((s0 + s1) + (s2 + s3));
-    if (lane == 0) s_val[w] = s;
-  }
-  __syncthreads();
-}
-
-template <typename T>
-__device__ __forceinline__ void publish8(double (&v)[2 * kMaxRhs], double *smem, double *part, int nb) {
-  block_sum<2 * kMaxRhs>(v, smem);
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int j = 0; j < 2 * kMaxRhs; j++) part[size_t(j) * nb + blockIdx.x] = v[j];
-  }
-}
-
-template <typename T, int NC>
-__global__ void __launch_bounds__(kCgThreads) cg_kernel(CgArgs<T> a) {
-  __shared__ double s_red[32 * 2 * kMaxRhs];
-  __shared__ double s_val[2 * kMaxRhs];
+// NR: right-hand-side slots unrolled (>= nrhs); BS: threads per block.
+template <typename T, int NC, int NR, int BS>
+__global__ void __launch_bounds__(BS, 1) cg_kernel(CgArgs<T> a) {
+  __shared__ SyncShared sh;
+  double *const s_val = sh.val;
   __shared__ double s_alpha[kMaxRhs], s_beta[kMaxRhs], s_rr[kMaxRhs], s_tau[kMaxRhs];
   __shared__ int s_active[kMaxRhs], s_status[kMaxRhs];
   __shared__ long long s_iters[kMaxRhs];
@@ -104,13 +74,11 @@ __global__ void __launch_bounds__(kCgThreads) cg_kernel(CgArgs<T> a) {
 
   const Geom g = a.g;
   const uint32_t V = uint32_t(g.V);
-  const int nb = gridDim.x;
   const uint32_t stride = gridDim.x * blockDim.x;
   const uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
   double *part0 = a.partials;
-  double *part1 = a.partials + size_t(2 * kMaxRhs) * nb;
-  unsigned gen = 0;
-  if (threadIdx.x == 0) gen = ld_acquire(&a.bar->gen);
+  double *part1 = a.partials + size_t(kSyncQ + 1) * gridDim.x;
+  unsigned long long nph = 0;  // phases ended so far (same count in every block)
   const T *__restrict__ sm = a.sm;
 
   if (threadIdx.x < kMaxRhs) {
@@ -131,7 +99,7 @@ __global__ void __launch_bounds__(kCgThreads) cg_kernel(CgArgs<T> a) {
       const Site s = make_site(g, i);
       const T smi = sm[i];
 #pragma unroll
-      for (int k = 0; k < kMaxRhs; k++) {
+      for (int k = 0; k < NR; k++) {
         if (k >= a.nrhs) break;
 #pragma unroll
         for (int c = 0; c < NC; c++) {
@@ -141,9 +109,11 @@ __global__ void __launch_bounds__(kCgThreads) cg_kernel(CgArgs<T> a) {
         }
       }
     }
-    ok = grid_barrier(a.bar, gen, a.err);
-    // r = b - M t ; sums r^2 and b^2
     double acc[2 * kMaxRhs];
+#pragma unroll
+    for (int j = 0; j < 2 * kMaxRhs; j++) acc[j] = 0.0;
+    ok = end_phase<1>(acc, sh, part1, a.bar, nph++, a.err);
+    // r = b - M t ; sums r^2 and b^2
 #pragma unroll
     for (int j = 0; j < 2 * kMaxRhs; j++) acc[j] = 0.0;
     if (ok) {
@@ -151,7 +121,7 @@ __global__ void __launch_bounds__(kCgThreads) cg_kernel(CgArgs<T> a) {
         const Site s = make_site(g, i);
         const T smi = sm[i];
 #pragma unroll
-        for (int k = 0; k < kMaxRhs; k++) {
+        for (int k = 0; k < NR; k++) {
           if (k >= a.nrhs) break;
 #pragma unroll
           for (int c = 0; c < NC; c++) {
@@ -161,18 +131,16 @@ __global__ void __launch_bounds__(kCgThreads) cg_kernel(CgArgs<T> a) {
             const T ri = apply_sub_M<T>(s, bi, smi, n);
             a.r[k][size_t(c) * V + i] = ri;
             acc[k] += double(ri) * double(ri);
-            acc[kMaxRhs + k] += double(bi) * double(bi);
+            acc[NR + k] += double(bi) * double(bi);
           }
         }
       }
     }
-    publish8<T>(acc, s_red, part0, nb);
-    ok = grid_barrier(a.bar, gen, a.err) && ok;
-    collect8(part0, nb, s_val);
+    ok = end_phase<2 * NR>(acc, sh, part0, a.bar, nph++, a.err) && ok;
     if (threadIdx.x < kMaxRhs) {
       const int k = threadIdx.x;
       if (k < a.nrhs) {
-        const double bb = s_val[kMaxRhs + k];
+        const double bb = s_val[NR + k];
         s_b2[k] = bb;
         s_r2[k] = s_val[k];
         s_tau[k] = a.rel ? a.tol * sqrt(bb) : a.tol;
@@ -192,7 +160,7 @@ __global__ void __launch_bounds__(kCgThreads) cg_kernel(CgArgs<T> a) {
     if (ok) {
       for (uint32_t i = i0; i < V; i += stride) {
 #pragma unroll
-        for (int k = 0; k < kMaxRhs; k++) {
+        for (int k = 0; k < NR; k++) {
           if (k >= a.nrhs || !s_active[k]) continue;
 #pragma unroll
           for (int c = 0; c < NC; c++) {
@@ -206,9 +174,7 @@ __global__ void __launch_bounds__(kCgThreads) cg_kernel(CgArgs<T> a) {
         }
       }
     }
-    publish8<T>(acc, s_red, part1, nb);
-    ok = grid_barrier(a.bar, gen, a.err) && ok;
-    collect8(part1, nb, s_val);
+    ok = end_phase<NR>(acc, sh, part1, a.bar, nph++, a.err) && ok;
     if (threadIdx.x < kMaxRhs) {
       const int k = threadIdx.x;
       if (k < a.nrhs && s_active[k]) {
@@ -234,6 +200,11 @@ __global__ void __launch_bounds__(kCgThreads) cg_kernel(CgArgs<T> a) {
 #pragma unroll
     for (int k = 0; k < kMaxRhs; k++) any |= (k < a.nrhs) ? s_active[k] : 0;
     if (!any) break;
+    // the host's abort request lives in mapped host memory: one thread reads it
+    // every 16 iterations, and the value is only used at the end of phase B
+    int abort_req = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && a.abort_flag != nullptr && (it & 15) == 0)
+      abort_req = *(volatile const int *)a.abort_flag;
     // phase A: p = r + beta p_old (it > 0), t = M^T p, sum t^2
     double acc[2 * kMaxRhs];
 #pragma unroll
@@ -242,7 +213,7 @@ __global__ void __launch_bounds__(kCgThreads) cg_kernel(CgArgs<T> a) {
       const Site s = make_site(g, i);
       const T smi = sm[i];
 #pragma unroll
-      for (int k = 0; k < kMaxRhs; k++) {
+      for (int k = 0; k < NR; k++) {
         if (k >= a.nrhs || !s_active[k]) continue;
         const T beta = T(s_beta[k]);
         T *const pn = (it & 1) ? a.p1[k] : a.p0[k];
@@ -266,10 +237,8 @@ __global__ void __launch_bounds__(kCgThreads) cg_kernel(CgArgs<T> a) {
         }
       }
     }
-    publish8<T>(acc, s_red, part0, nb);
-    ok = grid_barrier(a.bar, gen, a.err);
+    ok = end_phase<NR>(acc, sh, part0, a.bar, nph++, a.err);
     if (!ok) break;
-    collect8(part0, nb, s_val);
     if (threadIdx.x < kMaxRhs) {
       const int k = threadIdx.x;
       if (k < a.nrhs && s_active[k]) s_alpha[k] = s_rr[k] / s_val[k];
@@ -282,7 +251,7 @@ __global__ void __launch_bounds__(kCgThreads) cg_kernel(CgArgs<T> a) {
       const Site s = make_site(g, i);
       const T smi = sm[i];
 #pragma unroll
-      for (int k = 0; k < kMaxRhs; k++) {
+      for (int k = 0; k < NR; k++) {
         if (k >= a.nrhs || !s_active[k]) continue;
         const T alpha = T(s_alpha[k]);
         const T malpha = -alpha;
@@ -301,10 +270,8 @@ __global__ void __launch_bounds__(kCgThreads) cg_kernel(CgArgs<T> a) {
         }
       }
     }
-    publish8<T>(acc, s_red, part1, nb);
-    ok = grid_barrier(a.bar, gen, a.err);
+    ok = end_phase<NR>(acc, sh, part1, a.bar, nph++, a.err, abort_req);
     if (!ok) break;
-    collect8(part1, nb, s_val);
     if (threadIdx.x < kMaxRhs) {
       const int k = threadIdx.x;
       if (k < a.nrhs && s_active[k]) {
@@ -322,8 +289,10 @@ __global__ void __launch_bounds__(kCgThreads) cg_kernel(CgArgs<T> a) {
     }
     // host abort request: block 0's view decides for everyone at the next phase
     __syncthreads();
-    if (a.abort_flag != nullptr) {
-      if (threadIdx.x == 0 && blockIdx.x == 0 && *(volatile const int *)a.abort_flag) atomicExch(a.err, 2);
+    if (sh.flag != 0) {  // block 0 saw the host's abort request at the last phase end
+      if (threadIdx.x == 0 && blockIdx.x == 0) atomicExch(a.err, 2);
+      ok = false;
+      break;
     }
   }
   // ---------------------------------------------------------------- results

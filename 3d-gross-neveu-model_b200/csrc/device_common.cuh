@@ -37,13 +37,26 @@ __device__ __forceinline__ Nb<T> gather7(const Site &s, uint32_t i, Load ld) {
   return n;
 }
 
+// Each hopping term is (+-1/2) psi, an exact product, so adding the term
+// with the sign of eta equals the reference's t += (0.5 eta) psi bit for bit.
+template <typename T>
+__device__ __forceinline__ T hop_add(T t, T v, uint32_t neg, int bit) {
+  const T h = T(0.5) * v;
+  return ((neg >> bit) & 1u) ? t - h : t + h;
+}
+template <typename T>
+__device__ __forceinline__ T hop_sub(T t, T v, uint32_t neg, int bit) {
+  const T h = T(0.5) * v;
+  return ((neg >> bit) & 1u) ? t + h : t - h;
+}
+
 template <typename T>
 __device__ __forceinline__ T apply_M(const Site &s, T sm, const Nb<T> &n) {
   T t = sm * n.c;
 #pragma unroll
   for (int d = 0; d < 3; d++) {
-    t = t + (T(0.5) * T(s.eta_up[d])) * n.up[d];
-    t = t - (T(0.5) * T(s.eta_dn[d])) * n.dn[d];
+    t = hop_add(t, n.up[d], s.neg, d);
+    t = hop_sub(t, n.dn[d], s.neg, 3 + d);
   }
   return t;
 }
@@ -53,8 +66,8 @@ __device__ __forceinline__ T apply_Mt(const Site &s, T sm, const Nb<T> &n) {
   T t = sm * n.c;
 #pragma unroll
   for (int d = 0; d < 3; d++) {
-    t = t - (T(0.5) * T(s.eta_up[d])) * n.up[d];
-    t = t + (T(0.5) * T(s.eta_dn[d])) * n.dn[d];
+    t = hop_sub(t, n.up[d], s.neg, d);
+    t = hop_add(t, n.dn[d], s.neg, 3 + d);
   }
   return t;
 }
@@ -65,8 +78,8 @@ __device__ __forceinline__ T apply_sub_M(const Site &s, T out, T sm, const Nb<T>
   T t = out - sm * n.c;
 #pragma unroll
   for (int d = 0; d < 3; d++) {
-    t = t - (T(0.5) * T(s.eta_up[d])) * n.up[d];
-    t = t + (T(0.5) * T(s.eta_dn[d])) * n.dn[d];
+    t = hop_sub(t, n.up[d], s.neg, d);
+    t = hop_add(t, n.dn[d], s.neg, 3 + d);
   }
   return t;
 }

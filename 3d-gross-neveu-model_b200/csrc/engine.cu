@@ -8,6 +8,7 @@
 
 #include "engine.h"
 #include "errors.h"
+#include "launch.h"
 #include "ops_kernels.cuh"
 
 namespace gn {
@@ -61,7 +62,7 @@ Engine::Engine(int L, int device) : L_(L), device_(device) {
   cg_work_ = (double *)alloc(size_t(kMaxRhs) * kNumWorkVecs * 2 * V * d);
   max_blocks_ = num_sms_ * 8;
   partials_ = (double *)alloc(size_t(32) * max_blocks_ * d);
-  bar_ = (GridBar *)alloc(sizeof(GridBar));
+  bar_ = (PhaseBar *)alloc(sizeof(PhaseBar));
   err_ = (int *)alloc(sizeof(int));
   state_ = (CgState *)alloc(sizeof(CgState) * kMaxRhs);
   check(cudaHostAlloc((void **)&h_partials_, size_t(32) * max_blocks_ * d, cudaHostAllocDefault), "cudaHostAlloc");
@@ -161,18 +162,36 @@ void Engine::cond_fill(int mode, const signed char *signs, const double *table, 
   launches++;
 }
 
-int Engine::cg_blocks(int ncomp, bool mixed) {
-  int &cached = cg_blocks_cache_[mixed ? 1 : 0][ncomp - 1];
+// Instantiated solver kernels: (planes, RHS slots) = (1, 1), (1, 2), (1, 4), (2, 1), (2, 2).
+int rhs_slots(int nrhs) { return nrhs <= 1 ? 1 : (nrhs <= 2 ? 2 : 4); }
+
+// Block shape of a solve: the tunable shape for one plane and up to two
+// systems (the hot cases), the fixed shape otherwise.
+int threads_for(int ncomp, int nrhs) { return (ncomp == 1 && nrhs <= 2) ? solver_threads() : kSolverThreads; }
+
+const void *Engine::fp64_kernel_ptr(int ncomp, int nrhs) {
+  const int nr = rhs_slots(nrhs);
+  constexpr int B = kSolverThreads;
+  const bool wide = solver_threads() == 768;
+  if (ncomp == 1) {
+    if (nr == 1) return wide ? (const void *)cg_kernel<double, 1, 1, 768> : (const void *)cg_kernel<double, 1, 1, 512>;
+    if (nr == 2) return wide ? (const void *)cg_kernel<double, 1, 2, 768> : (const void *)cg_kernel<double, 1, 2, 512>;
+    return (const void *)cg_kernel<double, 1, 4, B>;
+  }
+  if (nr == 1) return (const void *)cg_kernel<double, 2, 1, B>;
+  if (nr == 2) return (const void *)cg_kernel<double, 2, 2, B>;
+  throw GnError(GN_ERR_ARG, "complex systems: at most 2 right-hand sides per solve");
+}
+
+int Engine::cg_blocks(int ncomp, int nrhs, bool mixed) {
+  const int nr = rhs_slots(nrhs);
+  int &cached = cg_blocks_cache_[mixed ? 1 : 0][ncomp - 1][nr == 1 ? 0 : (nr == 2 ? 1 : 2)];
   if (cached) return cached;
-  int per_sm = 0;
-  const void *fn = mixed ? mixed_kernel_ptr(ncomp)
-                         : (ncomp == 1 ? (const void *)cg_kernel<double, 1> : (const void *)cg_kernel<double, 2>);
-  check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kCgThreads, 0), "occupancy");
-  if (per_sm < 1) throw GnError(GN_ERR_CUDA, "CG kernel cannot be resident");
-  int64_t want = (V_ + kCgThreads - 1) / kCgThreads;
-  int64_t cap = int64_t(per_sm) * num_sms_;
-  if (cap > max_blocks_) cap = max_blocks_;
-  cached = int(want < cap ? want : cap);
+  const void *fn = mixed ? mixed_kernel_ptr(ncomp, nrhs) : fp64_kernel_ptr(ncomp, nrhs);
+  const int bs = threads_for(ncomp, nrhs);
+  const int capacity = coop_capacity(fn, bs);
+  if (capacity < 1) throw GnError(GN_ERR_CUDA, "CG kernel cannot be resident as a cooperative grid");
+  cached = solver_grid(V_, capacity, max_blocks_, bs);
   return cached;
 }
 
@@ -205,12 +224,10 @@ int Engine::solve(const double *sm, const double *const *b, double *const *x, in
   a.err = err_;
   a.abort_flag = d_abort_;
   a.state = state_;
-  check(cudaMemsetAsync(bar_, 0, sizeof(unsigned), stream_), "memset");
+  check(cudaMemsetAsync(bar_, 0, sizeof(PhaseBar), stream_), "memset");
   check(cudaMemsetAsync(err_, 0, sizeof(int), stream_), "memset");
-  const int nb = cg_blocks(ncomp, false);
-  void *args[] = {(void *)&a};
-  const void *fn = ncomp == 1 ? (const void *)cg_kernel<double, 1> : (const void *)cg_kernel<double, 2>;
-  check(cudaLaunchCooperativeKernel(fn, dim3(nb), dim3(kCgThreads), args, 0, stream_), "cg_kernel launch");
+  const int nb = cg_blocks(ncomp, nrhs, false);
+  check(launch_solver(fp64_kernel_ptr(ncomp, nrhs), nb, threads_for(ncomp, nrhs), a, stream_), "cg_kernel launch");
   launches++;
   return finish_solve(nrhs, info);
 }

@@ -92,11 +92,12 @@ class Engine {
  private:
   int finish_solve(int nrhs, SolveInfo *info);
   void mixed_init();
-  const void *mixed_kernel_ptr(int ncomp);
+  const void *mixed_kernel_ptr(int ncomp, int nrhs);
+  const void *fp64_kernel_ptr(int ncomp, int nrhs);
   int solve_mixed(const double *sm, const double *const *b, double *const *x, int nrhs, int ncomp, double tol,
                   int variant, int rel, long long max_iter, SolveInfo *info);
   void *alloc(size_t bytes);
-  int cg_blocks(int ncomp, bool mixed);
+  int cg_blocks(int ncomp, int nrhs, bool mixed);
 
   int L_, device_;
   int64_t V_;
@@ -117,7 +118,7 @@ class Engine {
   float *sm32_ = nullptr;
   double *partials_ = nullptr;
   double *h_partials_ = nullptr;
-  GridBar *bar_ = nullptr;
+  PhaseBar *bar_ = nullptr;
   int *err_ = nullptr;
   CgState *state_ = nullptr;
   CgState *h_state_ = nullptr;
@@ -125,8 +126,13 @@ class Engine {
   int *d_abort_ = nullptr;
   double *h_stage_ = nullptr;
   int max_blocks_ = 0;
-  int cg_blocks_cache_[2][2] = {{0, 0}, {0, 0}};
+  int cg_blocks_cache_[2][2][3] = {};
 };
+
+// Number of right-hand-side slots (1, 2 or 4) of the solver instantiation used for nrhs systems.
+int rhs_slots(int nrhs);
+// Threads per block of the solver used for nrhs systems of ncomp planes.
+int threads_for(int ncomp, int nrhs);
 
 // Host-side compensated sum of (hi, lo) block partials.
 double sum_partials(const double *part, int nb, int q);

@@ -19,23 +19,27 @@
 
 namespace gn {
 
-// Exact division by a small constant via one 64-bit multiply: q = (n*m) >> 36,
-// m = ceil(2^36 / d).  Exact for n * d < 2^36, i.e. for every index used here
-// (n < 2^27, d <= 512).
+// Exact division by a small constant d <= 512 for n < 2^24: a float
+// reciprocal estimate (n is exact in float) corrected by one step, so the
+// quotient is exact.
 struct FastDiv {
-  uint64_t m;
+  float inv;
   uint32_t d;
 };
 
 inline FastDiv make_fastdiv(uint32_t d) {
   FastDiv f;
   f.d = d;
-  f.m = ((uint64_t(1) << 36) + d - 1) / d;
+  f.inv = 1.0f / float(d);
   return f;
 }
 
 __host__ __device__ __forceinline__ uint32_t fdiv(uint32_t n, const FastDiv &f) {
-  return uint32_t((uint64_t(n) * f.m) >> 36);
+  uint32_t q = uint32_t(float(n) * f.inv);
+  const int32_t r = int32_t(n) - int32_t(q * f.d);
+  if (r < 0) q--;
+  else if (r >= int32_t(f.d)) q++;
+  return q;
 }
 
 // Lattice constants passed by value to every kernel.
@@ -60,18 +64,19 @@ inline Geom make_geom(int L) {
   return g;
 }
 
-// Everything the stencils need about one site.
+// Everything the stencils need about one site.  The staggered phases are
+// kept as sign bits: bit mu of neg set <=> eta_pp(x, mu) = -1, bit 3+mu set
+// <=> eta_mm(x, mu) = -1.
 struct Site {
   uint32_t x0, x1, x2, par;
-  uint32_t qbase;             // first index of the opposite parity half
   uint32_t nb_up[3], nb_dn[3];  // fermion indices of x + mu, x - mu
-  float eta_up[3], eta_dn[3];   // +-1: eta_pp(x, mu), eta_mm(x, mu)
+  uint32_t neg;
 };
 
 __host__ __device__ __forceinline__ void site_coords(const Geom &g, uint32_t i, uint32_t &x0, uint32_t &x1, uint32_t &x2,
-                                            uint32_t &par, uint32_t &row, uint32_t &k) {
+                                                     uint32_t &par, uint32_t &row, uint32_t &k) {
   par = i >= uint32_t(g.half) ? 1u : 0u;
-  uint32_t h = i - par * uint32_t(g.half);
+  const uint32_t h = i - par * uint32_t(g.half);
   row = fdiv(h, g.div_Lh);
   k = h - row * uint32_t(g.Lh);
   x0 = fdiv(row, g.div_L);
@@ -79,35 +84,36 @@ __host__ __device__ __forceinline__ void site_coords(const Geom &g, uint32_t i, 
   x2 = 2u * k + ((par + x0 + x1) & 1u);
 }
 
+// Neighbours as offsets from the half index h = row*(L/2) + k: x0 +- 1 is a
+// whole plane (L*L/2) away, x1 +- 1 one row (L/2), the time neighbours are at
+// k or k +- 1 of the same row; each wraps periodically.
 __host__ __device__ __forceinline__ Site make_site(const Geom &g, uint32_t i) {
   Site s;
   uint32_t row, k;
   site_coords(g, i, s.x0, s.x1, s.x2, s.par, row, k);
-  const uint32_t L = uint32_t(g.L), Lh = uint32_t(g.Lh);
-  s.qbase = (1u - s.par) * uint32_t(g.half);
-  // x0 +- 1
-  const uint32_t x0u = (s.x0 + 1u == L) ? 0u : s.x0 + 1u;
-  const uint32_t x0d = (s.x0 == 0u) ? L - 1u : s.x0 - 1u;
-  const uint32_t x1u = (s.x1 + 1u == L) ? 0u : s.x1 + 1u;
-  const uint32_t x1d = (s.x1 == 0u) ? L - 1u : s.x1 - 1u;
-  const uint32_t x2u = (s.x2 + 1u == L) ? 0u : s.x2 + 1u;
-  const uint32_t x2d = (s.x2 == 0u) ? L - 1u : s.x2 - 1u;
-  s.nb_up[0] = s.qbase + (x0u * L + s.x1) * Lh + k;
-  s.nb_dn[0] = s.qbase + (x0d * L + s.x1) * Lh + k;
-  s.nb_up[1] = s.qbase + (s.x0 * L + x1u) * Lh + k;
-  s.nb_dn[1] = s.qbase + (s.x0 * L + x1d) * Lh + k;
-  s.nb_up[2] = s.qbase + row * Lh + (x2u >> 1);
-  s.nb_dn[2] = s.qbase + row * Lh + (x2d >> 1);
-  const float e1 = (s.x0 & 1u) ? -1.f : 1.f;
-  const float e2 = ((s.x0 + s.x1) & 1u) ? -1.f : 1.f;
-  s.eta_up[0] = 1.f;
-  s.eta_dn[0] = 1.f;
-  s.eta_up[1] = e1;
-  s.eta_dn[1] = e1;
-  s.eta_up[2] = (s.x2 == L - 1u) ? -e2 : e2;
-  s.eta_dn[2] = (s.x2 == 0u) ? -e2 : e2;
+  const uint32_t L = uint32_t(g.L), Lh = uint32_t(g.Lh), P = uint32_t(g.plane);
+  const uint32_t h = row * Lh + k;
+  const uint32_t qb = (1u - s.par) * uint32_t(g.half);
+  s.nb_up[0] = qb + ((s.x0 + 1u == L) ? h - (L - 1u) * P : h + P);
+  s.nb_dn[0] = qb + ((s.x0 == 0u) ? h + (L - 1u) * P : h - P);
+  s.nb_up[1] = qb + ((s.x1 + 1u == L) ? h - (L - 1u) * Lh : h + Lh);
+  s.nb_dn[1] = qb + ((s.x1 == 0u) ? h + (L - 1u) * Lh : h - Lh);
+  if ((s.x2 & 1u) == 0u) {  // x2 = 2k: x2+1 -> k, x2-1 -> k-1
+    s.nb_up[2] = qb + h;
+    s.nb_dn[2] = qb + ((k == 0u) ? h + Lh - 1u : h - 1u);
+  } else {  // x2 = 2k+1: x2+1 -> k+1, x2-1 -> k
+    s.nb_up[2] = qb + ((k + 1u == Lh) ? h + 1u - Lh : h + 1u);
+    s.nb_dn[2] = qb + h;
+  }
+  const uint32_t e1 = s.x0 & 1u, e2 = (s.x0 + s.x1) & 1u;
+  const uint32_t up2 = e2 ^ (s.x2 == L - 1u ? 1u : 0u);
+  const uint32_t dn2 = e2 ^ (s.x2 == 0u ? 1u : 0u);
+  s.neg = (e1 << 1) | (up2 << 2) | (e1 << 4) | (dn2 << 5);
   return s;
 }
+
+__host__ __device__ __forceinline__ float eta_up(const Site &s, int d) { return (s.neg >> d) & 1u ? -1.f : 1.f; }
+__host__ __device__ __forceinline__ float eta_dn(const Site &s, int d) { return (s.neg >> (3 + d)) & 1u ? -1.f : 1.f; }
 
 // Fermion index of the site at lattice coordinates (any values mod L).
 __host__ __device__ __forceinline__ uint32_t site_index(const Geom &g, int c0, int c1, int c2) {

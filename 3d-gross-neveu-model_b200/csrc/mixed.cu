@@ -5,12 +5,13 @@
 
 #include "engine.h"
 #include "errors.h"
+#include "launch.h"
 #include "mixed_kernel.cuh"
 
 namespace gn {
 
 constexpr int kMixedVecs = 5;  // r^, p^0, p^1, t^, x^ per right-hand side
-constexpr double kDelta = 0.1;  // reliable update when |r^| drops by this factor
+constexpr double kDelta = 0.01;  // reliable update when |r^| drops by this factor
 constexpr int kReliableEvery = 50;
 
 void Engine::mixed_init() {
@@ -19,8 +20,18 @@ void Engine::mixed_init() {
   sm32_ = (float *)alloc(V * sizeof(float));
 }
 
-const void *Engine::mixed_kernel_ptr(int ncomp) {
-  return ncomp == 1 ? (const void *)cg_mixed_kernel<1> : (const void *)cg_mixed_kernel<2>;
+const void *Engine::mixed_kernel_ptr(int ncomp, int nrhs) {
+  const int nr = rhs_slots(nrhs);
+  constexpr int B = kSolverThreads;
+  const bool wide = solver_threads() == 768;
+  if (ncomp == 1) {
+    if (nr == 1) return wide ? (const void *)cg_mixed_kernel<1, 1, 768> : (const void *)cg_mixed_kernel<1, 1, 512>;
+    if (nr == 2) return wide ? (const void *)cg_mixed_kernel<1, 2, 768> : (const void *)cg_mixed_kernel<1, 2, 512>;
+    return (const void *)cg_mixed_kernel<1, 4, B>;
+  }
+  if (nr == 1) return (const void *)cg_mixed_kernel<2, 1, B>;
+  if (nr == 2) return (const void *)cg_mixed_kernel<2, 2, B>;
+  throw GnError(GN_ERR_ARG, "complex systems: at most 2 right-hand sides per solve");
 }
 
 int Engine::solve_mixed(const double *sm, const double *const *b, double *const *x, int nrhs, int ncomp, double tol,
@@ -54,11 +65,10 @@ int Engine::solve_mixed(const double *sm, const double *const *b, double *const 
   a.err = err_;
   a.abort_flag = d_abort_;
   a.state = state_;
-  check(cudaMemsetAsync(bar_, 0, sizeof(unsigned), stream_), "memset");
+  check(cudaMemsetAsync(bar_, 0, sizeof(PhaseBar), stream_), "memset");
   check(cudaMemsetAsync(err_, 0, sizeof(int), stream_), "memset");
-  const int nb = cg_blocks(ncomp, true);
-  void *args[] = {(void *)&a};
-  check(cudaLaunchCooperativeKernel(mixed_kernel_ptr(ncomp), dim3(nb), dim3(kCgThreads), args, 0, stream_),
+  const int nb = cg_blocks(ncomp, nrhs, true);
+  check(launch_solver(mixed_kernel_ptr(ncomp, nrhs), nb, threads_for(ncomp, nrhs), a, stream_),
         "cg_mixed_kernel launch");
   launches++;
   return finish_solve(nrhs, info);

@@ -44,16 +44,16 @@ struct MixedArgs {
   double delta;  // reliable update when |r^| < delta * max |r^| since the last one
   int n_ru;      // ... or after this many inner iterations
   double *partials;
-  GridBar *bar;
+  PhaseBar *bar;
   int *err;
   const int *abort_flag;
   CgState *state;
 };
 
-template <int NC>
-__global__ void __launch_bounds__(kCgThreads) cg_mixed_kernel(MixedArgs a) {
-  __shared__ double s_red[32 * 2 * kMaxRhs];
-  __shared__ double s_val[2 * kMaxRhs];
+template <int NC, int NR, int BS>
+__global__ void __launch_bounds__(BS, 1) cg_mixed_kernel(MixedArgs a) {
+  __shared__ SyncShared sh;
+  double *const s_val = sh.val;
   __shared__ double s_alpha[kMaxRhs], s_beta[kMaxRhs], s_rr[kMaxRhs], s_tau[kMaxRhs], s_rmax[kMaxRhs];
   __shared__ double s_r2[kMaxRhs], s_b2[kMaxRhs];
   __shared__ int s_active[kMaxRhs], s_status[kMaxRhs], s_ru[kMaxRhs], s_since[kMaxRhs], s_nru[kMaxRhs];
@@ -62,13 +62,11 @@ __global__ void __launch_bounds__(kCgThreads) cg_mixed_kernel(MixedArgs a) {
 
   const Geom g = a.g;
   const uint32_t V = uint32_t(g.V);
-  const int nb = gridDim.x;
   const uint32_t stride = gridDim.x * blockDim.x;
   const uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
   double *part0 = a.partials;
-  double *part1 = a.partials + size_t(2 * kMaxRhs) * nb;
-  unsigned gen = 0;
-  if (threadIdx.x == 0) gen = ld_acquire(&a.bar->gen);
+  double *part1 = a.partials + size_t(kSyncQ + 1) * gridDim.x;
+  unsigned long long nph = 0;  // phases ended so far (same count in every block)
   const double *__restrict__ sm = a.sm;
 
   if (threadIdx.x < kMaxRhs) {
@@ -92,7 +90,7 @@ __global__ void __launch_bounds__(kCgThreads) cg_mixed_kernel(MixedArgs a) {
       const Site s = make_site(g, i);
       const double smi = sm[i];
 #pragma unroll
-      for (int k = 0; k < kMaxRhs; k++) {
+      for (int k = 0; k < NR; k++) {
         if (k >= a.nrhs) break;
 #pragma unroll
         for (int c = 0; c < NC; c++) {
@@ -102,7 +100,9 @@ __global__ void __launch_bounds__(kCgThreads) cg_mixed_kernel(MixedArgs a) {
         }
       }
     }
-    ok = grid_barrier(a.bar, gen, a.err);
+#pragma unroll
+    for (int j = 0; j < 2 * kMaxRhs; j++) acc[j] = 0.0;
+    ok = end_phase<1>(acc, sh, part1, a.bar, nph++, a.err);
 #pragma unroll
     for (int j = 0; j < 2 * kMaxRhs; j++) acc[j] = 0.0;
     if (ok) {
@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(kCgThreads) cg_mixed_kernel(MixedArgs a) {
         const Site s = make_site(g, i);
         const double smi = sm[i];
 #pragma unroll
-        for (int k = 0; k < kMaxRhs; k++) {
+        for (int k = 0; k < NR; k++) {
           if (k >= a.nrhs) break;
 #pragma unroll
           for (int c = 0; c < NC; c++) {
@@ -119,18 +119,16 @@ __global__ void __launch_bounds__(kCgThreads) cg_mixed_kernel(MixedArgs a) {
             const double bi = a.b[k][size_t(c) * V + i];
             const double ri = apply_sub_M<double>(s, bi, smi, n);
             acc[k] += ri * ri;
-            acc[kMaxRhs + k] += bi * bi;
+            acc[NR + k] += bi * bi;
           }
         }
       }
     }
-    publish8<double>(acc, s_red, part0, nb);
-    ok = grid_barrier(a.bar, gen, a.err) && ok;
-    collect8(part0, nb, s_val);
+    ok = end_phase<2 * NR>(acc, sh, part0, a.bar, nph++, a.err) && ok;
     if (threadIdx.x < kMaxRhs) {
       const int k = threadIdx.x;
       if (k < a.nrhs) {
-        const double bb = s_val[kMaxRhs + k];
+        const double bb = s_val[NR + k];
         s_b2[k] = bb;
         s_r2[k] = s_val[k];
         s_tau[k] = a.rel ? a.tol * sqrt(bb) : a.tol;
@@ -149,7 +147,7 @@ __global__ void __launch_bounds__(kCgThreads) cg_mixed_kernel(MixedArgs a) {
     for (uint32_t i = i0; i < V; i += stride) {
       a.sm32[i] = float(sm[i]);
 #pragma unroll
-      for (int k = 0; k < kMaxRhs; k++) {
+      for (int k = 0; k < NR; k++) {
         if (k >= a.nrhs || !s_active[k]) continue;
 #pragma unroll
         for (int c = 0; c < NC; c++) {
@@ -161,24 +159,22 @@ __global__ void __launch_bounds__(kCgThreads) cg_mixed_kernel(MixedArgs a) {
           a.rh[k][j] = bf;
           a.ph0[k][j] = bf;
           acc[k] += double(bf) * double(bf);
-          acc[kMaxRhs + k] += bi * bi;
+          acc[NR + k] += bi * bi;
         }
       }
     }
   }
-  publish8<double>(acc, s_red, part1, nb);
-  ok = grid_barrier(a.bar, gen, a.err) && ok;
-  collect8(part1, nb, s_val);
+  ok = end_phase<2 * NR>(acc, sh, part1, a.bar, nph++, a.err) && ok;
   if (threadIdx.x < kMaxRhs) {
     const int k = threadIdx.x;
     if (k < a.nrhs && s_active[k]) {
       s_rr[k] = s_val[k];
       s_rmax[k] = sqrt(s_val[k]);
-      s_r2[k] = s_val[kMaxRhs + k];
-      s_b2[k] = s_val[kMaxRhs + k];
+      s_r2[k] = s_val[NR + k];
+      s_b2[k] = s_val[NR + k];
       if (a.variant == 1) {
-        s_tau[k] = a.rel ? a.tol * sqrt(s_val[kMaxRhs + k]) : a.tol;
-        if (sqrt(s_val[kMaxRhs + k]) < s_tau[k]) {
+        s_tau[k] = a.rel ? a.tol * sqrt(s_val[NR + k]) : a.tol;
+        if (sqrt(s_val[NR + k]) < s_tau[k]) {
           s_active[k] = 0;
           s_status[k] = kCgConvergedStart;
         }
@@ -194,6 +190,11 @@ __global__ void __launch_bounds__(kCgThreads) cg_mixed_kernel(MixedArgs a) {
 #pragma unroll
     for (int k = 0; k < kMaxRhs; k++) any |= (k < a.nrhs) ? s_active[k] : 0;
     if (!any) break;
+    // the host's abort request lives in mapped host memory: one thread reads it
+    // every 16 iterations, and the value is only used at the end of phase B
+    int abort_req = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && a.abort_flag != nullptr && (it & 15) == 0)
+      abort_req = *(volatile const int *)a.abort_flag;
     // A: p^ = r^ + beta p^, t^ = M^T p^
 #pragma unroll
     for (int j = 0; j < 2 * kMaxRhs; j++) acc[j] = 0.0;
@@ -201,7 +202,7 @@ __global__ void __launch_bounds__(kCgThreads) cg_mixed_kernel(MixedArgs a) {
       const Site s = make_site(g, i);
       const float smi = a.sm32[i];
 #pragma unroll
-      for (int k = 0; k < kMaxRhs; k++) {
+      for (int k = 0; k < NR; k++) {
         if (k >= a.nrhs || !s_active[k]) continue;
         const float beta = float(s_beta[k]);
         float *const pn = (it & 1) ? a.ph1[k] : a.ph0[k];
@@ -225,10 +226,8 @@ __global__ void __launch_bounds__(kCgThreads) cg_mixed_kernel(MixedArgs a) {
         }
       }
     }
-    publish8<double>(acc, s_red, part0, nb);
-    ok = grid_barrier(a.bar, gen, a.err);
+    ok = end_phase<NR>(acc, sh, part0, a.bar, nph++, a.err);
     if (!ok) break;
-    collect8(part0, nb, s_val);
     if (threadIdx.x < kMaxRhs) {
       const int k = threadIdx.x;
       if (k < a.nrhs && s_active[k]) s_alpha[k] = s_rr[k] / s_val[k];
@@ -241,7 +240,7 @@ __global__ void __launch_bounds__(kCgThreads) cg_mixed_kernel(MixedArgs a) {
       const Site s = make_site(g, i);
       const float smi = a.sm32[i];
 #pragma unroll
-      for (int k = 0; k < kMaxRhs; k++) {
+      for (int k = 0; k < NR; k++) {
         if (k >= a.nrhs || !s_active[k]) continue;
         const float alpha = float(s_alpha[k]);
         const float *const pn = (it & 1) ? a.ph1[k] : a.ph0[k];
@@ -258,10 +257,8 @@ __global__ void __launch_bounds__(kCgThreads) cg_mixed_kernel(MixedArgs a) {
         }
       }
     }
-    publish8<double>(acc, s_red, part1, nb);
-    ok = grid_barrier(a.bar, gen, a.err);
+    ok = end_phase<NR>(acc, sh, part1, a.bar, nph++, a.err, abort_req);
     if (!ok) break;
-    collect8(part1, nb, s_val);
     if (threadIdx.x == 0) s_any_ru = 0;
     __syncthreads();
     if (threadIdx.x < kMaxRhs) {
@@ -290,7 +287,7 @@ __global__ void __launch_bounds__(kCgThreads) cg_mixed_kernel(MixedArgs a) {
         const Site s = make_site(g, i);
         const double smi = sm[i];
 #pragma unroll
-        for (int k = 0; k < kMaxRhs; k++) {
+        for (int k = 0; k < NR; k++) {
           if (k >= a.nrhs || !s_ru[k]) continue;
 #pragma unroll
           for (int c = 0; c < NC; c++) {
@@ -302,7 +299,9 @@ __global__ void __launch_bounds__(kCgThreads) cg_mixed_kernel(MixedArgs a) {
           }
         }
       }
-      ok = grid_barrier(a.bar, gen, a.err);
+#pragma unroll
+      for (int j = 0; j < 2 * kMaxRhs; j++) acc[j] = 0.0;
+      ok = end_phase<1>(acc, sh, part0, a.bar, nph++, a.err);
       if (!ok) break;
       // D: x += x^, x^ = 0, r = b - M t, r^ = (float) r
 #pragma unroll
@@ -311,7 +310,7 @@ __global__ void __launch_bounds__(kCgThreads) cg_mixed_kernel(MixedArgs a) {
         const Site s = make_site(g, i);
         const double smi = sm[i];
 #pragma unroll
-        for (int k = 0; k < kMaxRhs; k++) {
+        for (int k = 0; k < NR; k++) {
           if (k >= a.nrhs || !s_ru[k]) continue;
 #pragma unroll
           for (int c = 0; c < NC; c++) {
@@ -326,10 +325,8 @@ __global__ void __launch_bounds__(kCgThreads) cg_mixed_kernel(MixedArgs a) {
           }
         }
       }
-      publish8<double>(acc, s_red, part0, nb);
-      ok = grid_barrier(a.bar, gen, a.err);
+      ok = end_phase<NR>(acc, sh, part1, a.bar, nph++, a.err);
       if (!ok) break;
-      collect8(part0, nb, s_val);
       if (threadIdx.x < kMaxRhs) {
         const int k = threadIdx.x;
         if (k < a.nrhs && s_ru[k]) {
@@ -350,8 +347,10 @@ __global__ void __launch_bounds__(kCgThreads) cg_mixed_kernel(MixedArgs a) {
       }
       __syncthreads();
     }
-    if (a.abort_flag != nullptr) {
-      if (threadIdx.x == 0 && blockIdx.x == 0 && *(volatile const int *)a.abort_flag) atomicExch(a.err, 2);
+    if (sh.flag != 0) {  // block 0 saw the host's abort request at the last phase end
+      if (threadIdx.x == 0 && blockIdx.x == 0) atomicExch(a.err, 2);
+      ok = false;
+      break;
     }
   }
   // ---------------------------------------------------------------- results

@@ -29,20 +29,26 @@
 #include <mutex>
 
 #include "../../include/gn_b200.h"
-#include "cg_kernel.cuh"
+#include "launch.h"
 
 namespace {
 
 using gn::CgArgs;
 using gn::CgState;
-using gn::GridBar;
+using gn::PhaseBar;
 
 constexpr int kNoAllocMaxL = 32;
 constexpr size_t kMaxV = size_t(kNoAllocMaxL) * kNoAllocMaxL * kNoAllocMaxL;  // 32768 sites
-constexpr int kMaxBlocks = int(kMaxV / gn::kCgThreads);                         // one site per thread at most
+constexpr int kMaxBlocks = int((kMaxV + 511) / 512);  // one site per thread at most (blocks of >= 512 threads)
+// the same solver instantiation and block shape as gn_cg_device for one real system
+inline const void *solver_kernel() {
+  return gn::solver_threads() == 768 ? (const void *)gn::cg_kernel<double, 1, 1, 768>
+                                     : (const void *)gn::cg_kernel<double, 1, 1, 512>;
+}
 constexpr size_t kVecWords = 4 * kMaxV;                                         // r, p0, p1, t
-constexpr size_t kPartialWords = size_t(2 * 2 * gn::kMaxRhs) * kMaxBlocks;      // 2 slots x 8 sums per block
-constexpr size_t kControlWords = 16;                                            // barrier, error flag, state
+constexpr size_t kPartialWords = size_t(2 * (gn::kSyncQ + 1)) * kMaxBlocks;      // 2 slots x (8 sums + flag) per block
+constexpr size_t kBarWords = sizeof(gn::PhaseBar) / sizeof(double);
+constexpr size_t kControlWords = kBarWords + 8;                                 // barrier, error flag, state
 constexpr size_t kScratchWords = kVecWords + kPartialWords + kControlWords;
 
 static __device__ __align__(256) double g_noalloc_scratch[kScratchWords];
@@ -50,8 +56,7 @@ static __device__ __align__(256) double g_noalloc_scratch[kScratchWords];
 constexpr int kMaxDevices = 64;
 struct DeviceSetup {
   double *scratch = nullptr;  // device address of g_noalloc_scratch on this device
-  int blocks_per_sm = 0;
-  int num_sms = 0;
+  int capacity = 0;           // co-resident blocks of the solver kernel
 };
 DeviceSetup g_setup[kMaxDevices];
 std::mutex g_setup_mutex;
@@ -95,13 +100,9 @@ extern "C" GN_API int gn_cg_noalloc(int L, const double *sigmamass, const double
       void *p = nullptr;
       const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
       if (e != cudaSuccess || p == nullptr) return err(GN_ERR_CUDA, "gn_cg_noalloc: cudaGetSymbolAddress failed");
-      int per_sm = 0;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gn::cg_kernel<double, 1>, gn::kCgThreads, 0) !=
-              cudaSuccess ||
-          per_sm < 1)
-        return err(GN_ERR_CUDA, "gn_cg_noalloc: occupancy query failed");
-      s.blocks_per_sm = per_sm;
-      s.num_sms = prop.multiProcessorCount;
+      const int capacity = gn::coop_capacity(solver_kernel(), gn::solver_threads());
+      if (capacity < 1) return err(GN_ERR_CUDA, "gn_cg_noalloc: occupancy query failed");
+      s.capacity = capacity;
       s.scratch = static_cast<double *>(p);
     }
   }
@@ -113,9 +114,9 @@ extern "C" GN_API int gn_cg_noalloc(int L, const double *sigmamass, const double
   double *vec = base;
   double *partials = base + kVecWords;
   double *control = base + kVecWords + kPartialWords;
-  GridBar *bar = reinterpret_cast<GridBar *>(control);
-  int *errflag = reinterpret_cast<int *>(control + 1);
-  CgState *state = reinterpret_cast<CgState *>(control + 2);
+  PhaseBar *bar = reinterpret_cast<PhaseBar *>(control);
+  int *errflag = reinterpret_cast<int *>(control + kBarWords);
+  CgState *state = reinterpret_cast<CgState *>(control + kBarWords + 2);
   if (cudaMemsetAsync(control, 0, kControlWords * sizeof(double), st) != cudaSuccess)
     return err(GN_ERR_CUDA, "gn_cg_noalloc: clearing the control words failed");
 
@@ -139,13 +140,8 @@ extern "C" GN_API int gn_cg_noalloc(int L, const double *sigmamass, const double
   a.err = errflag;
   a.abort_flag = nullptr;
   a.state = state;
-  long long want = (long long)((V + gn::kCgThreads - 1) / gn::kCgThreads);
-  long long cap = (long long)s.blocks_per_sm * s.num_sms;
-  if (cap > kMaxBlocks) cap = kMaxBlocks;
-  const int nb = int(want < cap ? want : cap);
-  void *args[] = {(void *)&a};
-  if (cudaLaunchCooperativeKernel((const void *)gn::cg_kernel<double, 1>, dim3(nb), dim3(gn::kCgThreads), args, 0,
-                                  st) != cudaSuccess)
+  const int nb = gn::solver_grid(int64_t(V), s.capacity, kMaxBlocks, gn::solver_threads());
+  if (gn::launch_solver(solver_kernel(), nb, gn::solver_threads(), a, st) != cudaSuccess)
     return err(GN_ERR_CUDA, "gn_cg_noalloc: kernel launch failed");
 
   // ---- outcome (into host stack memory; no allocation)

@@ -9,20 +9,42 @@ constexpr int kOpThreads = 256;
 
 // Dirac apply on ncomp planes: op 0 = M, 1 = M^T, 2 = out -= M in.
 // Algorithmic traffic 3 words per site and plane (in, sm, out; +1 read for op 2).
+// Each thread takes kDiracBatch sites per round and issues all their loads
+// before any arithmetic, so that enough bytes are in flight to cover the
+// memory latency (a one-site-per-round loop leaves the kernel latency bound).
+constexpr int kDiracBatch = 4;
+
 template <typename T, int OP>
 __global__ void __launch_bounds__(kOpThreads) dirac_kernel(Geom g, const T *__restrict__ sm, const T *__restrict__ in,
-                                                          T *out, int ncomp) {
+                                                          T *__restrict__ out, int ncomp) {
   const uint32_t V = uint32_t(g.V);
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x) {
-    const Site s = make_site(g, i);
-    const T smi = sm[i];
-    for (int c = 0; c < ncomp; c++) {
-      const T *pv = in + size_t(c) * V;
-      const Nb<T> n = gather7<T>(s, i, [&](uint32_t j) { return __ldg(pv + j); });
-      T *o = out + size_t(c) * V + i;
-      if (OP == 0) *o = apply_M<T>(s, smi, n);
-      else if (OP == 1) *o = apply_Mt<T>(s, smi, n);
-      else *o = apply_sub_M<T>(s, *o, smi, n);
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (int c = 0; c < ncomp; c++) {
+    const T *pv = in + size_t(c) * V;
+    T *ov = out + size_t(c) * V;
+    for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < V; i0 += kDiracBatch * stride) {
+      Site s[kDiracBatch];
+      Nb<T> n[kDiracBatch];
+      T smi[kDiracBatch], o[kDiracBatch];
+#pragma unroll
+      for (int b = 0; b < kDiracBatch; b++) {
+        const uint32_t i = i0 + b * stride;
+        if (i < V) {
+          s[b] = make_site(g, i);
+          smi[b] = __ldg(sm + i);
+          n[b] = gather7<T>(s[b], i, [&](uint32_t j) { return __ldg(pv + j); });
+          if (OP == 2) o[b] = ov[i];
+        }
+      }
+#pragma unroll
+      for (int b = 0; b < kDiracBatch; b++) {
+        const uint32_t i = i0 + b * stride;
+        if (i < V) {
+          if (OP == 0) ov[i] = apply_M<T>(s[b], smi[b], n[b]);
+          else if (OP == 1) ov[i] = apply_Mt<T>(s[b], smi[b], n[b]);
+          else ov[i] = apply_sub_M<T>(s[b], o[b], smi[b], n[b]);
+        }
+      }
     }
   }
 }

@@ -1,0 +1,102 @@
+// phase_sync.cuh -- end-of-phase synchronisation of the persistent solvers:
+// every block's partial sums are reduced, the grid waits until every block has
+// finished the phase, and every block gets the grid totals.
+//
+// Costs measured on B200 that shaped it: a block reduction of 8 doubles with
+// three block barriers took 1.1 us, a __threadfence 0.4 us, and every block
+// arriving on the barrier word adds about 8 ns (arrivals serialise on one
+// address).  So: only the quantities a phase needs are reduced, with one block
+// barrier; the grid barrier is a 64-bit monotonic arrival counter written with
+// red.release and polled with ld.acquire (no separate fences); and the solvers
+// run few, large blocks.  Every order is fixed, so all blocks compute the same
+// totals bit for bit.
+#pragma once
+#include "device_common.cuh"
+
+namespace gn {
+
+constexpr int kSyncQ = 8;  // largest number of quantities reduced at one phase end
+
+// Monotonic arrival counter: phase n is complete when it reaches
+// (n+1) * gridDim.x.  (Spreading arrivals over several counters polled by
+// several lanes was measured slower: every acquire load is a fence.)
+struct PhaseBar {
+  unsigned long long arrived;
+  unsigned long long pad[15];
+};
+
+__device__ __forceinline__ void red_release_add64(unsigned long long *p, unsigned long long v) {
+  asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void fence_acquire() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
+struct SyncShared {
+  double red[32 * kSyncQ];  // per-warp sums
+  double val[kSyncQ];       // grid totals of the last phase
+  int ok;
+  int flag;                 // block 0's flag word of the last phase
+};
+
+// End of phase number `phase` (counted from 0 in every block alike).  acc[]
+// holds this thread's contributions to NQ quantities; on return sh.val[0..NQ)
+// holds the grid totals in every block, and sh.flag the word block 0 put in
+// `flag` (the same value in every block).  Returns false if this block's wait
+// timed out (it then sets *err; the other blocks time out at their next wait).
+// part_slot: [NQ][gridDim.x] partials followed by one flag word.
+template <int NQ>
+__device__ __forceinline__ bool end_phase(double (&acc)[kSyncQ], SyncShared &sh, double *part_slot, PhaseBar *bar,
+                                          unsigned long long phase, int *err, int flag = 0) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NQ; q++) {
+    const double v = warp_sum(acc[q]);
+    if (lane == 0) sh.red[q * 32 + w] = v;
+  }
+  __syncthreads();
+  if (w == 0) {
+    double tot[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) tot[q] = warp_sum(lane < nw ? sh.red[q * 32 + lane] : 0.0);
+    if (lane == 0) {
+#pragma unroll
+      for (int q = 0; q < NQ; q++) part_slot[size_t(q) * gridDim.x + blockIdx.x] = tot[q];
+      if (blockIdx.x == 0) reinterpret_cast<int *>(part_slot + size_t(NQ) * gridDim.x)[0] = flag;
+      // arrive (release: the block's writes of this phase, ordered before by the
+      // block barrier, become visible with it), poll with relaxed loads, and
+      // acquire once the count is complete
+      red_release_add64(&bar->arrived, 1ull);
+      const unsigned long long target = (phase + 1ull) * gridDim.x;
+      unsigned spins = 0;
+      int ok = 1;
+      while (ld_relaxed64(&bar->arrived) < target) {
+        if (++spins > (1u << 22)) {  // ~ a second: give up, report, return
+          atomicExch(err, 1);
+          ok = 0;
+          break;
+        }
+      }
+      fence_acquire();
+      sh.ok = ok;
+    }
+  }
+  __syncthreads();
+  // grid totals, summed by every block in the same order
+  if (w < NQ) {
+    const double *p = part_slot + size_t(w) * gridDim.x;
+    double s = 0.0;
+    for (int b = lane; b < int(gridDim.x); b += 32) s += p[b];
+    s = warp_sum(s);
+    if (lane == 0) sh.val[w] = s;
+  } else if (threadIdx.x == blockDim.x - 1) {
+    sh.flag = reinterpret_cast<const int *>(part_slot + size_t(NQ) * gridDim.x)[0];
+  }
+  __syncthreads();
+  return sh.ok != 0;
+}
+
+}  // namespace gn

@@ -62,7 +62,7 @@ def parse():
     ap.add_argument("--eps", type=float, default=0.05)
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--case", choices=["cg64", "dirac128", "traj64"], default=None,
+    ap.add_argument("--case", choices=["cg64", "dirac128", "traj64", "cgscan"], default=None,
                     help="run one small case for a profiler instead of the benchmark")
     return ap.parse_args()
 
@@ -452,6 +452,9 @@ def run_case(a):
         r = dirac_roofline(G, None, dev, reps=3)
         print(json.dumps(r))
         return
+    if a.case == "cgscan":
+        cg_scan(G, dev)
+        return
     L, V = 64, 64 ** 3
     lat = G.Lattice(L, 0)
     rng = np.random.default_rng(1231)
@@ -470,6 +473,36 @@ def run_case(a):
                                   a.tol, 1, True, 0, prec)
         print(json.dumps({"precision": prec, "status": st, "info": infos}))
     lat.close()
+
+
+def cg_scan(G, dev, iters=100):
+    """Time per iteration of the persistent solvers against L: two flavours,
+    exactly `iters` iterations (tolerance 0), FP64 and mixed, CUDA events."""
+    import torch
+    for L in (8, 16, 24, 32, 48, 64, 96, 128):
+        V = L ** 3
+        lat = G.Lattice(L, dev.index)
+        rng = np.random.default_rng(L)
+        lat.load_sigma(rng.normal(0.0, np.sqrt(2.0 / (NFLAV * BETA_S)), V))
+        lat.write_state(G.GN_F_PHI, rng.normal(size=2 * V))
+        stream = torch.cuda.ExternalStream(lat.stream, device=dev)
+        row = {"L": L, "V": V}
+        for prec, name in ((G.GN_PREC_FP64, "fp64"), (G.GN_PREC_MIXED, "mixed")):
+            ts = []
+            for rep in range(3):
+                e0, e1 = cuda_events()
+                e0.record(stream)
+                infos, st = lat.cg_device(lat.field_ptr(G.GN_F_SM), lat.field_ptr(G.GN_F_PHI),
+                                          lat.field_ptr(G.GN_F_X), 2, 1, 0.0, 1, False, iters, prec)
+                e1.record(stream)
+                e1.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            ms = min(ts)
+            wbytes = 8 if prec == G.GN_PREC_FP64 else 4
+            row[name + "_us_per_iter"] = round(1000.0 * ms / iters, 2)
+            row[name + "_GBs"] = round(V * (2 * wbytes + 20 * wbytes) * iters / (ms * 1e-3) / 1e9, 1)
+        print(json.dumps(row), flush=True)
+        lat.close()
 
 
 def main():
