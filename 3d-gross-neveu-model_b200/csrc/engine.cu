@@ -99,10 +99,19 @@ void Engine::sigma_mass(const double *sigma, const double *P, double eps, double
 }
 
 void Engine::dirac(const double *sm, const double *in, double *out, int ncomp, int op) {
-  const int nb = op_blocks(V_, num_sms_);
-  if (op == GN_OP_M) dirac_kernel<double, 0><<<nb, kOpThreads, 0, stream_>>>(g_, sm, in, out, ncomp);
-  else if (op == GN_OP_MT) dirac_kernel<double, 1><<<nb, kOpThreads, 0, stream_>>>(g_, sm, in, out, ncomp);
-  else dirac_kernel<double, 2><<<nb, kOpThreads, 0, stream_>>>(g_, sm, in, out, ncomp);
+  if (L_ % 4 == 0) {  // two sites per thread, 128-bit loads
+    const dim3 grid(unsigned((V_ / 2 + kOpThreads - 1) / kOpThreads), unsigned(ncomp));
+    if (op == GN_OP_M) dirac_pair_kernel<0><<<grid, kOpThreads, 0, stream_>>>(g_, sm, in, out);
+    else if (op == GN_OP_MT) dirac_pair_kernel<1><<<grid, kOpThreads, 0, stream_>>>(g_, sm, in, out);
+    else dirac_pair_kernel<2><<<grid, kOpThreads, 0, stream_>>>(g_, sm, in, out);
+    check(cudaGetLastError(), "dirac_pair_kernel");
+    launches++;
+    return;
+  }
+  const dim3 grid(unsigned((V_ + kOpThreads - 1) / kOpThreads), unsigned(ncomp));
+  if (op == GN_OP_M) dirac_kernel<double, 0><<<grid, kOpThreads, 0, stream_>>>(g_, sm, in, out);
+  else if (op == GN_OP_MT) dirac_kernel<double, 1><<<grid, kOpThreads, 0, stream_>>>(g_, sm, in, out);
+  else dirac_kernel<double, 2><<<grid, kOpThreads, 0, stream_>>>(g_, sm, in, out);
   check(cudaGetLastError(), "dirac_kernel");
   launches++;
 }
@@ -311,7 +320,7 @@ static void count_flavours(const SolveInfo *info, int n, double &iters, long lon
 
 int Engine::trajectory(const gn_hmc_params &hp, double (*gauss)(void), double (*uniform)(void), const double *pre_P,
                        const double *pre_chi, gn_traj_result *res) {
-  if (hp.steps < 2) throw GnError(GN_ERR_ARG, "steps must be >= 2 (info.c:66)");
+  if (hp.steps < 1) throw GnError(GN_ERR_ARG, "steps must be >= 1");
   if (hp.integrator < 0 || hp.integrator > 2) throw GnError(GN_ERR_ARG, "unknown integrator");
   const size_t V = size_t(V_);
   memset(res, 0, sizeof *res);

@@ -62,7 +62,7 @@ def parse():
     ap.add_argument("--eps", type=float, default=0.05)
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--case", choices=["cg64", "dirac128", "traj64", "cgscan"], default=None,
+    ap.add_argument("--case", choices=["cg64", "dirac128", "dirac256", "traj64", "cgscan"], default=None,
                     help="run one small case for a profiler instead of the benchmark")
     return ap.parse_args()
 
@@ -412,44 +412,47 @@ def kernel_roofline(lat, stream, a, G):
                     f"{(2 * 5 * 4 + 8 * 3) * V / 1e6:.0f} MB is L2-resident within the solve"}
 
 
-def dirac_roofline(G, stream, dev, reps=12):
-    """Dirac M on one FP64 plane at L = 128 (V = 2,097,152), L2 flushed before
-    every launch.  Algorithmic bytes 3 * 8 * V (psi, sm in; out)."""
-    L = 128
+def dirac_roofline(G, stream, dev, reps=20, L=256):
+    """Dirac M on one FP64 plane at L = 256 (V = 16,777,216): psi, sm and the
+    output are 384 MB, three times the L2, so back-to-back launches run from
+    HBM (no flush needed); `reps` launches between two CUDA events.
+    Algorithmic bytes 3 * 8 * V per launch (psi, sm in; out)."""
+    import torch
     lat = G.Lattice(L, dev.index)
+    V = L ** 3
     sm = lat.field_ptr(G.GN_F_SM)
     X = lat.field_ptr(G.GN_F_X)
     Y = lat.field_ptr(G.GN_F_Y)
-    import torch
     torch_stream = torch.cuda.ExternalStream(lat.stream, device=dev)
+    for _ in range(3):
+        lat.dirac_device(sm, X, Y, 1, G.GN_OP_M)
     times = []
-    for rep in range(reps):
-        lat.flush_l2()
+    for rep in range(3):
         e0, e1 = cuda_events()
         e0.record(torch_stream)
-        lat.dirac_device(sm, X, Y, 1, G.GN_OP_M)
+        for _ in range(reps):
+            lat.dirac_device(sm, X, Y, 1, G.GN_OP_M)
         e1.record(torch_stream)
         e1.synchronize()
-        if rep >= min(2, reps - 1):
-            times.append(e0.elapsed_time(e1))
-    ms = statistics.median(times)
-    V = L ** 3
+        times.append(e0.elapsed_time(e1) / reps)
+    ms = min(times)
     nbytes = 3 * 8 * V
     lat.close()
-    return {"gbs": nbytes / (ms * 1e-3) / 1e9, "kernel": "dirac_kernel<double,M> L=128 cold", "ms": ms,
-            "bytes": nbytes, "traffic": None, "note": f"{ms * 1e3:.1f} us per launch, L2 flushed before each"}
+    return {"gbs": nbytes / (ms * 1e-3) / 1e9, "kernel": f"dirac_pair_kernel<M> L={L} (inputs 3x L2)", "ms": ms,
+            "bytes": nbytes, "traffic": None,
+            "note": f"{ms * 1e3:.1f} us per launch, {reps} back-to-back launches on 384 MB (> L2)"}
 
 
 def run_case(a):
     """Small cases for ncu: cg64 = one two-flavour CG solve at L=64 in FP64 and in
-    mixed precision; dirac128 = 3 cold Dirac applies at L=128; traj64 = one
+    mixed precision; dirac128 / dirac256 = 3 Dirac applies at L=128 / 256; traj64 = one
     mixed-precision trajectory at L=64."""
     import torch
 
     import gn_b200 as G
     dev = torch.device("cuda", 0)
-    if a.case == "dirac128":
-        r = dirac_roofline(G, None, dev, reps=3)
+    if a.case in ("dirac128", "dirac256"):
+        r = dirac_roofline(G, None, dev, reps=3, L=128 if a.case == "dirac128" else 256)
         print(json.dumps(r))
         return
     if a.case == "cgscan":

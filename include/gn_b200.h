@@ -67,7 +67,7 @@ typedef struct gn_cg_info {
 typedef struct gn_hmc_params {
   double beta_s;       /* info->beta_scalar */
   double eps;          /* info->epsilon_sigma_HMC */
-  int steps;           /* info->steps_sigma_HMC (>= 2, info.c:66) */
+  int steps;           /* info->steps_sigma_HMC (>= 1; the reference's StartInfo rejects 1, info.c:66) */
   int integrator;      /* gn_integrator; the reference default is GN_LFMN2VF (macro.h:71) */
   double tol_medium;   /* MEDIUM_PRECISION_INVERSION (1e-3) for the MD forces */
   double tol_high;     /* HIGH_PRECISION_INVERSION (1e-9) for H0 / H1 */

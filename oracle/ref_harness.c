@@ -287,3 +287,42 @@ void gnref_condensate(double tol, double *out)
                            &out[9], &out[10], &g_vec, &g_kit.inverted_phi_obs.flav[0], &g_info, &g_fcor, tol, &g_kit,
                            0);
 }
+
+/* ---------------- struct layouts (for the drop-in's ABI check) ---------------- */
+#include <stddef.h>
+/* out[] = sizeof and offsets of the members the drop-in layer reads or writes */
+int gnref_layout(long *out)
+{
+    int n = 0;
+    out[n++] = sizeof(struct Lattice);
+    out[n++] = offsetof(struct Lattice, sigma);
+    out[n++] = offsetof(struct Lattice, sigmamass);
+    out[n++] = offsetof(struct Lattice, eta_pbc);
+    out[n++] = offsetof(struct Lattice, distance_sigma);
+    out[n++] = offsetof(struct Lattice, done_sigma);
+    out[n++] = sizeof(struct Fermioncoor);
+    out[n++] = sizeof(struct Fermionkit);
+    out[n++] = offsetof(struct Fermionkit, chi);
+    out[n++] = offsetof(struct Fermionkit, phi);
+    out[n++] = offsetof(struct Fermionkit, inverted_phi);
+    out[n++] = offsetof(struct Fermionkit, inverted_phi_obs);
+    out[n++] = offsetof(struct Fermionkit, Ddag_inverted_phi_obs);
+    out[n++] = offsetof(struct Fermionkit, iterations);
+    out[n++] = offsetof(struct Fermionkit, CG_call);
+    out[n++] = sizeof(struct Info);
+    out[n++] = offsetof(struct Info, beta_scalar);
+    out[n++] = offsetof(struct Info, epsilon_link_HMC);
+    out[n++] = offsetof(struct Info, steps_link_HMC);
+    out[n++] = offsetof(struct Info, epsilon_sigma_HMC);
+    out[n++] = offsetof(struct Info, steps_sigma_HMC);
+    out[n++] = offsetof(struct Info, hybrid_done_acceptance_link);
+    out[n++] = offsetof(struct Info, hybrid_accepted_sigma);
+    out[n++] = offsetof(struct Info, hybrid_done_acceptance_sigma);
+    out[n++] = offsetof(struct Info, local_acceptance_sigma);
+    out[n++] = offsetof(struct Info, delta_H_link);
+    out[n++] = offsetof(struct Info, story_sigma);
+    out[n++] = sizeof(struct Forcesigma);
+    out[n++] = sizeof(struct Momentasigma);
+    out[n++] = sizeof(struct RandomVec);
+    return n;
+}

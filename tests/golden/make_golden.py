@@ -133,7 +133,17 @@ def condensate_fixture(L, seed=1231):
                         counters=np.array(ref.counters()))
 
 
+def layout_fixture():
+    """The reference's struct layouts (sizes and member offsets) for the drop-in ABI check."""
+    import ctypes as C
+    ref = Ref(8)
+    out = (C.c_long * 64)()
+    n = ref.lib.gnref_layout(out)
+    np.save(HERE / "layout_reference.npy", np.array(out[:n], dtype=np.int64))
+
+
 def main():
+    layout_fixture()
     for L in (4, 8, 16):
         ops_fixture(L)
     hmc_fixture(8, 0, 20, 0.2, 2)       # the README command line: beta_s 0.85, eps 0.2, 2 steps, seed 1231

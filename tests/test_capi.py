@@ -53,3 +53,28 @@ def test_bad_lattice_size_rejected(core_lib):
     ctx = C.c_void_p()
     assert lib.gn_create(C.byref(ctx), 7, 0) != 0  # odd L: the fermion order needs even L
     assert not ctx.value
+
+
+def test_dropin_exports_every_declared_symbol(core_lib):
+    lib = LIBDIR / "libgn_dropin.so"
+    assert lib.exists(), "build the library first (python 3d-gross-neveu-model_b200/build.py)"
+    names = declared("gn_dropin.h")
+    assert len(names) >= 21
+    missing = set(names) - exported(lib)
+    assert not missing, missing
+
+
+def test_dropin_struct_layout_matches_reference(tmp_path):
+    """The drop-in restates the reference's structs; their sizes and member
+    offsets must equal the reference build's (recorded by
+    tests/golden/make_golden.py from the reference's own headers)."""
+    import subprocess
+
+    import numpy as np
+    exe = tmp_path / "layout_probe"
+    subprocess.run(["gcc", "-std=gnu11", f"-I{INCLUDE}", str(ROOT / "tests" / "golden" / "layout_probe.c"), "-o",
+                    str(exe)], check=True)
+    got = np.array([int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout
+                    .split()])
+    ref = np.load(ROOT / "tests" / "golden" / "layout_reference.npy")
+    assert np.array_equal(got, ref), (got, ref)

@@ -1,0 +1,44 @@
+"""The reference-signature drop-in (include/gn_dropin.h) interposed under the
+reference's own code: the reference's harness calls its integrator, its
+condensate and its Dirac operator by name, and the dynamic linker binds them to
+the GPU versions.  With the reference's own dSFMT stream (seed 1231) the
+results must equal the golden fixtures made by the reference alone: dH to
+1e-10, every accept/reject decision, sigma to 1e-12, the CG counters.
+
+Runs in a subprocess so that no earlier test has bound the reference's
+symbols in this process.  Needs the reference build under oracle/_ref/ (made
+by __graft_entry__.build() where the reference tree exists)."""
+import json
+import subprocess
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = Path(__file__).resolve().parent.parent
+GOLD = ROOT / "tests" / "golden"
+
+
+def test_dropin_under_reference_driver(port):
+    from oracle import build_ref
+    if not build_ref.lib_path(8, 0).exists():
+        pytest.skip("reference build oracle/_ref/libgnref_L8_i0.so not present")
+    r = subprocess.run([sys.executable, str(ROOT / "tests" / "dropin_driver.py"), str(GOLD / "golden_L8_hmc_i0.npz"),
+                        str(GOLD / "golden_L8_cond.npz")], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    g = dict(np.load(GOLD / "golden_L8_hmc_i0.npz"))
+    assert np.max(np.abs(np.array(out["dH"]) - g["dH"])) < 1e-10
+    assert out["accepted"] == [int(a) for a in g["accepted"]]
+    assert max(out["sigma_rel"]) < 1e-12
+    assert [tuple(c) for c in out["counters"]] == [tuple(c) for c in g["counters"]]
+    c = dict(np.load(GOLD / "golden_L8_cond.npz"))
+    for k in range(11):
+        assert abs(out["condensate"][k] - c["out"][k]) <= 1e-11 * max(abs(c["out"][k]), 1e-3)
+    assert tuple(out["condensate_counters"]) == tuple(c["counters"])
+    # DiracFermion called by the reference's harness equals the reference's own M, bit for bit
+    L = 8
+    assert np.array_equal(np.array(out["M_psi"]), port.dirac(L, np.array(out["sm"]), np.array(out["psi"]), 0))
