@@ -30,6 +30,7 @@ UNITS = {
     "mixed.cu": [],
     "capi.cu": [],
     "noalloc.cu": ["--fmad=false"],
+    "exact.cu": ["--fmad=false"],
 }
 CORE_LIB = LIB / "libgn_b200.so"
 DROPIN_LIB = LIB / "libgn_dropin.so"

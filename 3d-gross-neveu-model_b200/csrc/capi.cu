@@ -91,6 +91,13 @@ void gn_destroy(gn_context *ctx) {
   delete ctx;
 }
 
+int gn_set_parity_mode(gn_context *ctx, int on) {
+  return guarded(ctx, [&](gn::Engine &E) {
+    E.exact = on != 0;
+    return GN_OK;
+  });
+}
+
 long long gn_volume(const gn_context *ctx) { return (ctx && ctx->eng) ? (long long)ctx->eng->V() : 0; }
 
 void gn_request_abort(gn_context *ctx, int on) {
@@ -130,7 +137,7 @@ int gn_cg(gn_context *ctx, const double *sigmamass, const double *b, double *x, 
           int variant, int relative, long long max_iter, int precision, gn_cg_info *info) {
   if (!sigmamass || !b || !x) return fail(GN_ERR_ARG, "null pointer");
   if (nrhs < 1 || nrhs > gn::kMaxRhs || ncomp < 1 || ncomp > 2) return fail(GN_ERR_ARG, "bad nrhs or ncomp");
-  if (variant < 0 || variant > 1 || precision < 0 || precision > 1) return fail(GN_ERR_ARG, "bad variant/precision");
+  if (variant < 0 || variant > 1 || precision < 0 || precision > 2) return fail(GN_ERR_ARG, "bad variant/precision");
   return guarded(ctx, [&](gn::Engine &E) {
     const size_t V = size_t(E.V()), n = size_t(nrhs) * ncomp * V;
     double *d_sm = ctx->io, *d_b = ctx->io + V, *d_x = ctx->io + V + n;
@@ -169,7 +176,10 @@ int gn_sigma_force(gn_context *ctx, double beta_s, const double *sigma, const do
     gn::SolveInfo si[2];
     const int st = E.solve(d_sm, bs, xs, 2, 1, tol, 0, 0, 0, precision, si);
     if (st == GN_OK) {
+      const bool saved = E.exact;
+      E.exact = saved || precision == GN_PREC_FP64_EXACT;
       E.dirac(d_sm, d_X, d_Y, 2, GN_OP_MT);
+      E.exact = saved;
       E.force(d_X, d_Y, d_s, beta_s, d_F, nullptr, 0.0);
       down(E, Y, d_Y, 2 * V);
       down(E, force, d_F, V);
@@ -338,7 +348,7 @@ int gn_cg_device(gn_context *ctx, const double *sigmamass, const double *b, doub
                  int variant, int relative, long long max_iter, int precision, gn_cg_info *info) {
   if (!sigmamass || !b || !x) return fail(GN_ERR_ARG, "null pointer");
   if (nrhs < 1 || nrhs > gn::kMaxRhs || ncomp < 1 || ncomp > 2) return fail(GN_ERR_ARG, "bad nrhs or ncomp");
-  if (variant < 0 || variant > 1 || precision < 0 || precision > 1) return fail(GN_ERR_ARG, "bad variant/precision");
+  if (variant < 0 || variant > 1 || precision < 0 || precision > 2) return fail(GN_ERR_ARG, "bad variant/precision");
   return guarded(ctx, [&](gn::Engine &E) {
     const size_t V = size_t(E.V());
     const double *bs[gn::kMaxRhs];

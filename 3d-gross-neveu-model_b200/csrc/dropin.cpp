@@ -244,7 +244,11 @@ void GNB200_SetTolerances(double medium, double high) {
   g_tol_medium = medium;
   g_tol_high = high;
 }
-void GNB200_SetPrecision(int precision) { g_precision = precision; }
+void GNB200_SetPrecision(int precision) {
+  g_precision = precision;
+  // the operators without a precision argument follow the exact mode too
+  if (gn_set_parity_mode(ctx(), precision == GN_PREC_FP64_EXACT) != GN_OK) fatal("gn_set_parity_mode");
+}
 gn_context *GNB200_Context(void) { return ctx(); }
 
 void DiracFermion(const Lattice *lat, const Fermion *fermion, Fermion *target, const Info *, const Fermioncoor *) {

@@ -99,6 +99,10 @@ void Engine::sigma_mass(const double *sigma, const double *P, double eps, double
 }
 
 void Engine::dirac(const double *sm, const double *in, double *out, int ncomp, int op) {
+  if (exact && op == GN_OP_MT) {
+    mt_exact(sm, in, out, ncomp);
+    return;
+  }
   if (L_ % 4 == 0) {  // two sites per thread, 128-bit loads
     const dim3 grid(unsigned((V_ / 2 + kOpThreads - 1) / kOpThreads), unsigned(ncomp));
     if (op == GN_OP_M) dirac_pair_kernel<0><<<grid, kOpThreads, 0, stream_>>>(g_, sm, in, out);
@@ -146,6 +150,10 @@ double sum_partials(const double *part, int nb, int q) {
 }
 
 void Engine::energy_terms(const double *P, const double *phi, const double *X, const double *sigma, double out[3]) {
+  if (exact) {
+    energy_exact(P, phi, X, sigma, out);
+    return;
+  }
   const int nb = op_blocks(V_, num_sms_);
   energy_kernel<double><<<nb, kOpThreads, 0, stream_>>>(uint32_t(V_), P, phi, X, sigma, partials_);
   check(cudaGetLastError(), "energy_kernel");
@@ -209,6 +217,7 @@ int Engine::solve(const double *sm, const double *const *b, double *const *x, in
   if (nrhs < 1 || nrhs > kMaxRhs || ncomp < 1 || ncomp > 2) throw GnError(GN_ERR_ARG, "bad nrhs / ncomp");
   if (max_iter <= 0) max_iter = V_ + 1;  // MAX_CONJUGATE_GRADIENT_ITERATION, macro.h:134
   if (precision == GN_PREC_MIXED) return solve_mixed(sm, b, x, nrhs, ncomp, tol, variant, rel, max_iter, info);
+  if (precision == GN_PREC_FP64_EXACT) return solve_exact(sm, b, x, nrhs, ncomp, tol, variant, rel, max_iter, info);
   const size_t V = size_t(V_);
   CgArgs<double> a;
   memset(&a, 0, sizeof a);
@@ -324,6 +333,11 @@ int Engine::trajectory(const gn_hmc_params &hp, double (*gauss)(void), double (*
   if (hp.integrator < 0 || hp.integrator > 2) throw GnError(GN_ERR_ARG, "unknown integrator");
   const size_t V = size_t(V_);
   memset(res, 0, sizeof *res);
+  struct ExactScope {  // parity mode for the trajectory's operators, restored on every exit
+    bool &flag, saved;
+    ExactScope(bool &f, bool on) : flag(f), saved(f) { flag = flag || on; }
+    ~ExactScope() { flag = saved; }
+  } exact_scope(exact, hp.precision == GN_PREC_FP64_EXACT);
   // draws: P, chi_0, chi_1 (moleculardynamics.c:1240-1247), uploaded in one copy
   if (gauss != nullptr) {
     double *h = h_stage_;
@@ -422,6 +436,20 @@ int Engine::trajectory(const gn_hmc_params &hp, double (*gauss)(void), double (*
 int Engine::condensate(const double *sm, double tol, double *target, double *D, double (*uniform)(void),
                        double out[11], double *iterations, long long *calls, int precision) {
   const size_t V = size_t(V_);
+  struct ExactScope {
+    bool &flag, saved;
+    ExactScope(bool &f, bool on) : flag(f), saved(f) { flag = flag || on; }
+    ~ExactScope() { flag = saved; }
+  } exact_scope(exact, precision == GN_PREC_FP64_EXACT);
+  // dot products: the compensated tree, or the reference's serial loop in parity mode
+  auto dots = [&](const double *v, const double *Dv, double q[4]) {
+    if (exact) {
+      cond_dots_exact(v, Dv, q);
+    } else {
+      cond_dots(v, Dv, q);
+      q[3] = q[0];
+    }
+  };
   double *vec = scratch_[0];
   double *z = scratch_[1];
   signed char *h_signs = reinterpret_cast<signed char *>(h_stage_);
@@ -443,14 +471,14 @@ int Engine::condensate(const double *sm, double tol, double *target, double *D, 
     check(cudaMemcpyAsync(signs_, h_signs, V, cudaMemcpyHostToDevice, stream_), "upload signs");
     cond_fill(0, signs_, nullptr, nullptr, vec);
   };
-  double q[3];
+  double q[4];
   for (int k = 0; k < 11; k++) out[k] = 0.0;
   double temp[4];
   for (int p = 0; p < 4; p++) {
     z2();
     solve1(vec);
     dirac(sm, target, D, 2, GN_OP_MT);
-    cond_dots(vec, D, q);
+    dots(vec, D, q);
     temp[p] = q[0];
   }
   const double tr0 = temp[0], tr1 = temp[1], tr2 = temp[2], tr3 = temp[3];
@@ -462,7 +490,7 @@ int Engine::condensate(const double *sm, double tol, double *target, double *D, 
   cond_fill(1, nullptr, nullptr, nullptr, vec);
   solve1(vec);
   dirac(sm, target, D, 2, GN_OP_MT);
-  cond_dots(vec, D, q);
+  dots(vec, D, q);
   out[4] = q[1];
   out[5] = out[4] * out[4];
   out[6] = double(int(V)) * out[4];
@@ -482,7 +510,7 @@ int Engine::condensate(const double *sm, double tol, double *target, double *D, 
     cond_fill(2, nullptr, table_, nullptr, vec);
     solve1(vec);
     dirac(sm, target, D, 2, GN_OP_MT);
-    cond_dots(vec, D, q);
+    dots(vec, D, q);
     out[8] = q[2] * double(int(V));
   }
   // <chibar1 chi2> without sigma (condensate.c:201-212)
@@ -492,8 +520,8 @@ int Engine::condensate(const double *sm, double tol, double *target, double *D, 
   dirac(sm, target, D, 2, GN_OP_MT);
   solve1(D);
   dirac(sm, target, D, 2, GN_OP_MT);
-  cond_dots(z, D, q);
-  out[9] = q[0];
+  dots(z, D, q);
+  out[9] = q[3];
   // with sigma-mass insertions (condensate.c:216-230)
   z2();
   check(cudaMemcpyAsync(z, vec, 2 * V * sizeof(double), cudaMemcpyDeviceToDevice, stream_), "copy z");
@@ -503,8 +531,8 @@ int Engine::condensate(const double *sm, double tol, double *target, double *D, 
   cond_fill(3, nullptr, nullptr, sm, D);
   solve1(D);
   dirac(sm, target, D, 2, GN_OP_MT);
-  cond_dots(z, D, q);
-  out[10] = q[0];
+  dots(z, D, q);
+  out[10] = q[3];
   check(cudaStreamSynchronize(stream_), "condensate");
   return all_ok ? GN_OK : GN_NOT_CONVERGED;
 }

@@ -74,6 +74,10 @@ class Engine {
   double *table() { return table_; }
   double distance = 0.0;  // lat->distance_sigma of the resident state
   long long launches = 0; // kernels launched by this engine (for launch accounting)
+  // Parity mode: M^T in the reference's scatter order and serial sums in the
+  // energy and the condensate (set by gn_set_parity_mode and by the
+  // operations run with precision GN_PREC_FP64_EXACT).
+  bool exact = false;
 
   // One trajectory on the resident state; see gn_trajectory in gn_b200.h.
   int trajectory(const gn_hmc_params &hp, double (*gauss)(void), double (*uniform)(void), const double *pre_P,
@@ -91,6 +95,11 @@ class Engine {
 
  private:
   int finish_solve(int nrhs, SolveInfo *info);
+  int solve_exact(const double *sm, const double *const *b, double *const *x, int nrhs, int ncomp, double tol,
+                  int variant, int rel, long long max_iter, SolveInfo *info);
+  void mt_exact(const double *sm, const double *in, double *out, int ncomp);
+  void energy_exact(const double *P, const double *phi, const double *X, const double *sigma, double out[3]);
+  void cond_dots_exact(const double *v, const double *D, double out[4]);
   void mixed_init();
   const void *mixed_kernel_ptr(int ncomp, int nrhs);
   const void *fp64_kernel_ptr(int ncomp, int nrhs);

@@ -22,7 +22,7 @@ LIB_PATH = PKG / "lib" / "libgn_b200.so"
 
 GN_OK, GN_NOT_CONVERGED = 0, 1
 GN_OP_M, GN_OP_MT, GN_OP_SUB_M = 0, 1, 2
-GN_PREC_FP64, GN_PREC_MIXED = 0, 1
+GN_PREC_FP64, GN_PREC_MIXED, GN_PREC_FP64_EXACT = 0, 1, 2
 GN_LFMN2VF, GN_LF2, GN_LFMN2 = 0, 1, 2
 GN_F_P, GN_F_F, GN_F_CHI, GN_F_PHI, GN_F_X, GN_F_Y, GN_F_SIGMA, GN_F_SM = range(8)
 STATUS_NAMES = {0: "GN_OK", 1: "GN_NOT_CONVERGED", -1: "GN_ERR_ARG", -2: "GN_ERR_CUDA", -3: "GN_ERR_TIMEOUT",
@@ -106,6 +106,7 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
                                   C.POINTER(TrajResult)], C.c_int),
         "gn_launch_count": ([v], C.c_longlong),
         "gn_flush_l2": ([v], C.c_int),
+        "gn_set_parity_mode": ([v, C.c_int], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -295,6 +296,10 @@ class Lattice:
         self._check(self.lib.gn_trajectory(self.ctx, C.byref(hp), fn_address(gauss), fn_address(uniform),
                                            C.byref(res)), allow=(GN_OK, GN_NOT_CONVERGED))
         return res.as_dict()
+
+    def set_parity_mode(self, on=True):
+        """M^T and the energy in the reference's exact order (see GN_PREC_FP64_EXACT)."""
+        self._check(self.lib.gn_set_parity_mode(self.ctx, int(on)))
 
     def request_abort(self, on=True):
         self.lib.gn_request_abort(self.ctx, int(on))

@@ -49,7 +49,12 @@ enum gn_status {
 };
 
 enum gn_op { GN_OP_M = 0, GN_OP_MT = 1, GN_OP_SUB_M = 2 };
-enum gn_precision { GN_PREC_FP64 = 0, GN_PREC_MIXED = 1 };
+/* GN_PREC_FP64: FP64, tree-ordered global sums (fast).  GN_PREC_MIXED: FP32
+ * iterations with FP64 reliable updates.  GN_PREC_FP64_EXACT: FP64 in the
+ * reference's exact order of operations -- serial sums, M^T in the order of
+ * the reference's scatter -- reproducing its results bit for bit (real fields);
+ * one block per solve, so meant for parity runs at small L. */
+enum gn_precision { GN_PREC_FP64 = 0, GN_PREC_MIXED = 1, GN_PREC_FP64_EXACT = 2 };
 enum gn_integrator { GN_LFMN2VF = 0, GN_LF2 = 1, GN_LFMN2 = 2 };
 
 /* Per right-hand side outcome of a solve. */
@@ -92,6 +97,10 @@ GN_API const char *gn_last_error(void);
 GN_API long long gn_volume(const gn_context *ctx);
 /* Ask a running solve on this context to stop (from another host thread). */
 GN_API void gn_request_abort(gn_context *ctx, int on);
+
+/* Parity mode for the operators that take no precision argument (gn_dirac's
+ * M^T, gn_energy): on = the reference's exact order of operations. */
+GN_API int gn_set_parity_mode(gn_context *ctx, int on);
 
 /* ---- host-buffer operators (one call = one reference function) -------- */
 

@@ -94,7 +94,7 @@ struct RandomVec { struct Fermion *vec; };
 GN_API void GNB200_SetLattice(int L);
 GN_API void GNB200_SetRandom(double (*gauss)(void), double (*uniform)(void));
 GN_API void GNB200_SetTolerances(double medium, double high);
-GN_API void GNB200_SetPrecision(int precision); /* GN_PREC_FP64 (default) or GN_PREC_MIXED */
+GN_API void GNB200_SetPrecision(int precision); /* GN_PREC_FP64 (default), GN_PREC_MIXED or GN_PREC_FP64_EXACT */
 GN_API gn_context *GNB200_Context(void);      /* the library's context (created on first use) */
 
 /* ---- dirac.c ------------------------------------------------------------- */

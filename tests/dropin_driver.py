@@ -10,7 +10,8 @@ go through the dynamic linker and bind to the drop-in's versions, which run on
 the GPU; the random numbers come from the reference's own Gauss1 / Casuale,
 found by name.
 
-usage: python tests/dropin_driver.py <golden hmc .npz> <golden condensate .npz>
+usage: python tests/dropin_driver.py <golden hmc .npz> <golden condensate .npz> [exact]
+("exact" selects GN_PREC_FP64_EXACT, the reference's exact order of operations)
 """
 import ctypes as C
 import json
@@ -30,6 +31,8 @@ def main():
     L = int(hmc["L"])
     drop = C.CDLL(str(ROOT / "3d-gross-neveu-model_b200" / "lib" / "libgn_dropin.so"), mode=C.RTLD_GLOBAL)
     drop.GNB200_SetLattice(L)
+    if len(sys.argv) > 3 and sys.argv[3] == "exact":
+        drop.GNB200_SetPrecision(2)
     from oracle import build_ref
     from oracle.oracle import Ref
     path = build_ref.lib_path(L, int(hmc["integrator"]))
@@ -45,6 +48,7 @@ def main():
             ok, accepted, dH = ref.trajectory(acc)
             s = ref.sigma()
             out["dH"].append(dH)
+            out.setdefault("sigma_equal", []).append(bool(np.array_equal(s, hmc["sigma_final"][t])))
             out["accepted"].append(int(accepted))
             out["sigma_rel"].append(float(np.max(np.abs(s - hmc["sigma_final"][t])) / np.max(np.abs(hmc["sigma_final"][t]))))
             out["counters"].append(list(ref.counters()))

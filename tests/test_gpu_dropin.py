@@ -42,3 +42,21 @@ def test_dropin_under_reference_driver(port):
     # DiracFermion called by the reference's harness equals the reference's own M, bit for bit
     L = 8
     assert np.array_equal(np.array(out["M_psi"]), port.dirac(L, np.array(out["sm"]), np.array(out["psi"]), 0))
+
+
+def test_dropin_exact_mode_is_bit_identical():
+    """GNB200_SetPrecision(GN_PREC_FP64_EXACT): the reference's driver code on
+    the GPU reproduces the reference's own run bit for bit."""
+    from oracle import build_ref
+    if not build_ref.lib_path(8, 0).exists():
+        pytest.skip("reference build oracle/_ref/libgnref_L8_i0.so not present")
+    r = subprocess.run([sys.executable, str(ROOT / "tests" / "dropin_driver.py"), str(GOLD / "golden_L8_hmc_i0.npz"),
+                        str(GOLD / "golden_L8_cond.npz"), "exact"], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    g = dict(np.load(GOLD / "golden_L8_hmc_i0.npz"))
+    assert out["dH"] == [float(v) for v in g["dH"]]
+    assert all(out["sigma_equal"])
+    assert [tuple(c) for c in out["counters"]] == [tuple(c) for c in g["counters"]]
+    c = dict(np.load(GOLD / "golden_L8_cond.npz"))
+    assert out["condensate"] == [float(v) for v in c["out"]]
