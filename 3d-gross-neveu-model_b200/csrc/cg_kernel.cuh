@@ -8,8 +8,8 @@
 // every block reduces the per-block partial sums itself (same order in every
 // block, so every block computes bit-identical scalars and takes the same
 // branches).  Up to kMaxRhs independent right-hand sides run in lock step (the
-// two pseudofermion flavours share one sweep of sm and of the geometry), each
-// with its own alpha, beta and stopping test, exactly as separate solves.
+// two pseudofermion flavours share every barrier), each with its own alpha,
+// beta and stopping test, exactly as separate solves.
 //
 // Per iteration, two phases (12 words of traffic per site and RHS):
 //   A: p <- r + beta p (on the fly at the 7 stencil points), t = M^T p, sum t^2
@@ -17,8 +17,14 @@
 // The update formulas and their rounding follow the reference (x += a p,
 // r += (-a) Ap, p = r + b p; no FMA in the FP64 build); only the order of the
 // global sums differs (tree instead of serial).
+//
+// A sweep's work unit is one (system, row item) pair (rowvec.cuh; items of
+// W = 2 sites with 128-bit loads when L/2 is even), one unit per thread where
+// the grid allows: the systems' loads are then all in flight at once instead
+// of one system after the other, and a phase is one latency round.
 #pragma once
 #include "phase_sync.cuh"
+#include "rowvec.cuh"
 
 namespace gn {
 
@@ -62,20 +68,70 @@ struct CgArgs {
   CgState *state;         // [kMaxRhs]
 };
 
-// NR: right-hand-side slots unrolled (>= nrhs); BS: threads per block.
-template <typename T, int NC, int NR, int BS>
+// ------------------------------------------------------------------ work units
+// The systems a sweep covers (block-shared, the same in every block).
+struct SysList {
+  int n;
+  int k[kMaxRhs];
+};
+
+// Rebuilds the list from a per-system flag (thread 0; the caller synchronises).
+__device__ __forceinline__ void sys_list_from(SysList &sl, const int *flag, int nrhs) {
+  int n = 0;
+  for (int k = 0; k < nrhs; k++)
+    if (flag[k]) sl.k[n++] = k;
+  sl.n = n;
+}
+
+// f(k, j) for every (system k of the list, item j < NI): the items of one
+// system are contiguous in the unit numbering, so a warp reads contiguous
+// vectors of one system.
+template <typename F>
+__device__ __forceinline__ void for_units(uint32_t NI, const SysList &sl, F f) {
+  const uint32_t total = uint32_t(sl.n) * NI;
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < total; u += gridDim.x * blockDim.x) {
+    uint32_t j = u;
+    int ka = 0;
+    while (j >= NI) {
+      j -= NI;
+      ka++;
+    }
+    f(sl.k[ka], j);
+  }
+}
+
+// Per-system selections without dynamic indexing (which would move the
+// kernel's argument arrays and the accumulators to local memory).
+template <int NR, typename P>
+__device__ __forceinline__ P pick(const P (&arr)[kMaxRhs], int k) {
+  P p = arr[0];
+#pragma unroll
+  for (int q = 1; q < NR; q++)
+    if (q == k) p = arr[q];
+  return p;
+}
+template <int NR>
+__device__ __forceinline__ void acc_add(double (&acc)[2 * kMaxRhs], int slot, double v) {
+#pragma unroll
+  for (int q = 0; q < 2 * NR; q++)
+    if (q == slot) acc[q] += v;
+}
+
+// NR: right-hand-side slots unrolled (>= nrhs); BS: threads per block; W:
+// sites per item (divides L/2).
+template <typename T, int NC, int NR, int BS, int W>
 __global__ void __launch_bounds__(BS, 1) cg_kernel(CgArgs<T> a) {
   __shared__ SyncShared sh;
   double *const s_val = sh.val;
   __shared__ double s_alpha[kMaxRhs], s_beta[kMaxRhs], s_rr[kMaxRhs], s_tau[kMaxRhs];
-  __shared__ int s_active[kMaxRhs], s_status[kMaxRhs];
+  __shared__ int s_active[kMaxRhs], s_status[kMaxRhs], s_all[kMaxRhs];
   __shared__ long long s_iters[kMaxRhs];
   __shared__ double s_r2[kMaxRhs], s_b2[kMaxRhs];
+  __shared__ SysList s_run, s_every;  // systems still iterating / all systems
 
   const Geom g = a.g;
   const uint32_t V = uint32_t(g.V);
-  const uint32_t stride = gridDim.x * blockDim.x;
-  const uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t NI = row_items<W>(g);
   double *part0 = a.partials;
   double *part1 = a.partials + size_t(kSyncQ + 1) * gridDim.x;
   unsigned long long nph = 0;  // phases ended so far (same count in every block)
@@ -84,57 +140,76 @@ __global__ void __launch_bounds__(BS, 1) cg_kernel(CgArgs<T> a) {
   if (threadIdx.x < kMaxRhs) {
     const int k = threadIdx.x;
     s_active[k] = k < a.nrhs;
+    s_all[k] = k < a.nrhs;
     s_status[k] = k < a.nrhs ? kCgRunning : kCgConverged;
     s_iters[k] = 0;
     s_alpha[k] = s_beta[k] = s_rr[k] = s_r2[k] = s_b2[k] = 0.0;
     s_tau[k] = a.tol;
   }
   __syncthreads();
+  if (threadIdx.x == 0) {
+    sys_list_from(s_every, s_all, a.nrhs);
+    sys_list_from(s_run, s_active, a.nrhs);
+  }
+  __syncthreads();
   bool ok = true;
+  double acc[2 * kMaxRhs];
+  auto zero_acc = [&]() {
+#pragma unroll
+    for (int q = 0; q < 2 * kMaxRhs; q++) acc[q] = 0.0;
+  };
 
   // ---------------------------------------------------------------- start
   if (a.variant == 0) {
     // t = M^T x_in
-    for (uint32_t i = i0; i < V; i += stride) {
-      const Site s = make_site(g, i);
-      const T smi = sm[i];
+    for_units(NI, s_every, [&](int k, uint32_t j) {
+      const RowItem it = make_item<W>(g, j);
+      T smi[W];
+      vload<T, W>(sm + it.own, smi);
+      const T *xk = pick<NR>(a.x, k);
+      T *tk = pick<NR>(a.t, k);
 #pragma unroll
-      for (int k = 0; k < NR; k++) {
-        if (k >= a.nrhs) break;
-#pragma unroll
-        for (int c = 0; c < NC; c++) {
-          const T *xv = a.x[k] + size_t(c) * V;
-          const Nb<T> n = gather7<T>(s, i, [&](uint32_t j) { return xv[j]; });
-          a.t[k][size_t(c) * V + i] = apply_Mt<T>(s, smi, n);
-        }
+      for (int c = 0; c < NC; c++) {
+        Nb<T> n[W];
+        T o[W];
+        gather_item<T, W>(it, xk + size_t(c) * V, n);
+        item_Mt<T, W>(it, smi, n, o);
+        vstore<T, W>(tk + size_t(c) * V + it.own, o);
       }
-    }
-    double acc[2 * kMaxRhs];
-#pragma unroll
-    for (int j = 0; j < 2 * kMaxRhs; j++) acc[j] = 0.0;
+    });
+    zero_acc();
     ok = end_phase<1>(acc, sh, part1, a.bar, nph++, a.err);
     // r = b - M t ; sums r^2 and b^2
-#pragma unroll
-    for (int j = 0; j < 2 * kMaxRhs; j++) acc[j] = 0.0;
+    zero_acc();
     if (ok) {
-      for (uint32_t i = i0; i < V; i += stride) {
-        const Site s = make_site(g, i);
-        const T smi = sm[i];
+      for_units(NI, s_every, [&](int k, uint32_t j) {
+        const RowItem it = make_item<W>(g, j);
+        T smi[W];
+        vload<T, W>(sm + it.own, smi);
+        const T *tk = pick<NR>(a.t, k);
+        const T *bk = pick<NR>(a.b, k);
+        T *rk = pick<NR>(a.r, k);
 #pragma unroll
-        for (int k = 0; k < NR; k++) {
-          if (k >= a.nrhs) break;
+        for (int c = 0; c < NC; c++) {
+          const size_t off = size_t(c) * V + it.own;
+          Nb<T> n[W];
+          T bi[W], ri[W];
+          gather_item<T, W>(it, tk + size_t(c) * V, n);
+          vload<T, W>(bk + off, bi);
 #pragma unroll
-          for (int c = 0; c < NC; c++) {
-            const T *tv = a.t[k] + size_t(c) * V;
-            const Nb<T> n = gather7<T>(s, i, [&](uint32_t j) { return tv[j]; });
-            const T bi = a.b[k][size_t(c) * V + i];
-            const T ri = apply_sub_M<T>(s, bi, smi, n);
-            a.r[k][size_t(c) * V + i] = ri;
-            acc[k] += double(ri) * double(ri);
-            acc[NR + k] += double(bi) * double(bi);
+          for (int e = 0; e < W; e++) ri[e] = bi[e];
+          item_sub_M<T, W>(it, smi, n, ri);
+          vstore<T, W>(rk + off, ri);
+          double sr = 0.0, sb = 0.0;
+#pragma unroll
+          for (int e = 0; e < W; e++) {
+            sr += double(ri[e]) * double(ri[e]);
+            sb += double(bi[e]) * double(bi[e]);
           }
+          acc_add<NR>(acc, k, sr);
+          acc_add<NR>(acc, NR + k, sb);
         }
-      }
+      });
     }
     ok = end_phase<2 * NR>(acc, sh, part0, a.bar, nph++, a.err) && ok;
     if (threadIdx.x < kMaxRhs) {
@@ -151,92 +226,110 @@ __global__ void __launch_bounds__(BS, 1) cg_kernel(CgArgs<T> a) {
       }
     }
     __syncthreads();
-  }
-  // x = 0, r = b, p = b ; rr = sum b^2
-  {
-    double acc[2 * kMaxRhs];
-#pragma unroll
-    for (int j = 0; j < 2 * kMaxRhs; j++) acc[j] = 0.0;
-    if (ok) {
-      for (uint32_t i = i0; i < V; i += stride) {
-#pragma unroll
-        for (int k = 0; k < NR; k++) {
-          if (k >= a.nrhs || !s_active[k]) continue;
-#pragma unroll
-          for (int c = 0; c < NC; c++) {
-            const size_t j = size_t(c) * V + i;
-            const T bi = a.b[k][j];
-            a.x[k][j] = T(0);
-            a.r[k][j] = bi;
-            a.p0[k][j] = bi;
-            acc[k] += double(bi) * double(bi);
-          }
-        }
-      }
-    }
-    ok = end_phase<NR>(acc, sh, part1, a.bar, nph++, a.err) && ok;
-    if (threadIdx.x < kMaxRhs) {
-      const int k = threadIdx.x;
-      if (k < a.nrhs && s_active[k]) {
-        s_rr[k] = s_val[k];
-        s_r2[k] = s_val[k];
-        s_b2[k] = s_val[k];
-        if (a.variant == 1) {
-          s_tau[k] = a.rel ? a.tol * sqrt(s_val[k]) : a.tol;
-          if (sqrt(s_val[k]) < s_tau[k]) {
-            s_active[k] = 0;
-            s_status[k] = kCgConvergedStart;
-          }
-        }
-      }
-    }
+    if (threadIdx.x == 0) sys_list_from(s_run, s_active, a.nrhs);
     __syncthreads();
   }
+  // x = 0, r = b, p = b ; rr = sum b^2
+  zero_acc();
+  if (ok) {
+    for_units(NI, s_run, [&](int k, uint32_t j) {
+      const uint32_t own = make_item<W>(g, j).own;
+      const T *bk = pick<NR>(a.b, k);
+      T *xk = pick<NR>(a.x, k);
+      T *rk = pick<NR>(a.r, k);
+      T *pk = pick<NR>(a.p0, k);
+#pragma unroll
+      for (int c = 0; c < NC; c++) {
+        const size_t off = size_t(c) * V + own;
+        T bi[W], zero[W];
+        vload<T, W>(bk + off, bi);
+        double sb = 0.0;
+#pragma unroll
+        for (int e = 0; e < W; e++) {
+          zero[e] = T(0);
+          sb += double(bi[e]) * double(bi[e]);
+        }
+        acc_add<NR>(acc, k, sb);
+        vstore<T, W>(xk + off, zero);
+        vstore<T, W>(rk + off, bi);
+        vstore<T, W>(pk + off, bi);
+      }
+    });
+  }
+  ok = end_phase<NR>(acc, sh, part1, a.bar, nph++, a.err) && ok;
+  if (threadIdx.x < kMaxRhs) {
+    const int k = threadIdx.x;
+    if (k < a.nrhs && s_active[k]) {
+      s_rr[k] = s_val[k];
+      s_r2[k] = s_val[k];
+      s_b2[k] = s_val[k];
+      if (a.variant == 1) {
+        s_tau[k] = a.rel ? a.tol * sqrt(s_val[k]) : a.tol;
+        if (sqrt(s_val[k]) < s_tau[k]) {
+          s_active[k] = 0;
+          s_status[k] = kCgConvergedStart;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) sys_list_from(s_run, s_active, a.nrhs);
+  __syncthreads();
 
   // ---------------------------------------------------------------- iterations
   long long it = 0;
   for (; ok && it < a.max_iter; it++) {
-    int any = 0;
-#pragma unroll
-    for (int k = 0; k < kMaxRhs; k++) any |= (k < a.nrhs) ? s_active[k] : 0;
-    if (!any) break;
+    if (s_run.n == 0) break;
     // the host's abort request lives in mapped host memory: one thread reads it
     // every 16 iterations, and the value is only used at the end of phase B
     int abort_req = 0;
     if (blockIdx.x == 0 && threadIdx.x == 0 && a.abort_flag != nullptr && (it & 15) == 0)
       abort_req = *(volatile const int *)a.abort_flag;
+    const bool odd = (it & 1) != 0;
     // phase A: p = r + beta p_old (it > 0), t = M^T p, sum t^2
-    double acc[2 * kMaxRhs];
+    zero_acc();
+    for_units(NI, s_run, [&](int k, uint32_t j) {
+      const RowItem ri = make_item<W>(g, j);
+      T smi[W];
+      vload<T, W>(sm + ri.own, smi);
+      const T beta = T(s_beta[k]);
+      T *const pn = odd ? pick<NR>(a.p1, k) : pick<NR>(a.p0, k);
+      const T *const po = odd ? pick<NR>(a.p0, k) : pick<NR>(a.p1, k);
+      const T *rk = pick<NR>(a.r, k);
+      T *tk = pick<NR>(a.t, k);
 #pragma unroll
-    for (int j = 0; j < 2 * kMaxRhs; j++) acc[j] = 0.0;
-    for (uint32_t i = i0; i < V; i += stride) {
-      const Site s = make_site(g, i);
-      const T smi = sm[i];
+      for (int c = 0; c < NC; c++) {
+        const size_t off = size_t(c) * V;
+        Nb<T> n[W];
+        if (it == 0) {
+          gather_item<T, W>(ri, pn + off, n);
+        } else {
+          const T *rv = rk + off;
+          const T *pov = po + off;
+          gather_item<T, W>(
+              ri, n,
+              [&](uint32_t i, T(&v)[W]) {
+                T rr[W], pp[W];
+                vload<T, W>(rv + i, rr);
+                vload<T, W>(pov + i, pp);
 #pragma unroll
-      for (int k = 0; k < NR; k++) {
-        if (k >= a.nrhs || !s_active[k]) continue;
-        const T beta = T(s_beta[k]);
-        T *const pn = (it & 1) ? a.p1[k] : a.p0[k];
-        const T *const po = (it & 1) ? a.p0[k] : a.p1[k];
+                for (int e = 0; e < W; e++) v[e] = rr[e] + beta * pp[e];
+              },
+              [&](uint32_t i) { return rv[i] + beta * pov[i]; });
+          T pc[W];
 #pragma unroll
-        for (int c = 0; c < NC; c++) {
-          const size_t off = size_t(c) * V;
-          Nb<T> n;
-          if (it == 0) {
-            const T *pv = pn + off;
-            n = gather7<T>(s, i, [&](uint32_t j) { return pv[j]; });
-          } else {
-            const T *rv = a.r[k] + off;
-            const T *pov = po + off;
-            n = gather7<T>(s, i, [&](uint32_t j) { return rv[j] + beta * pov[j]; });
-            pn[off + i] = n.c;
-          }
-          const T ti = apply_Mt<T>(s, smi, n);
-          a.t[k][off + i] = ti;
-          acc[k] += double(ti) * double(ti);
+          for (int e = 0; e < W; e++) pc[e] = n[e].c;
+          vstore<T, W>(pn + off + ri.own, pc);
         }
+        T ti[W];
+        item_Mt<T, W>(ri, smi, n, ti);
+        vstore<T, W>(tk + off + ri.own, ti);
+        double st = 0.0;
+#pragma unroll
+        for (int e = 0; e < W; e++) st += double(ti[e]) * double(ti[e]);
+        acc_add<NR>(acc, k, st);
       }
-    }
+    });
     ok = end_phase<NR>(acc, sh, part0, a.bar, nph++, a.err);
     if (!ok) break;
     if (threadIdx.x < kMaxRhs) {
@@ -245,31 +338,39 @@ __global__ void __launch_bounds__(BS, 1) cg_kernel(CgArgs<T> a) {
     }
     __syncthreads();
     // phase B: Ap = M t, x += alpha p, r -= alpha Ap, sum r^2
+    zero_acc();
+    for_units(NI, s_run, [&](int k, uint32_t j) {
+      const RowItem ri = make_item<W>(g, j);
+      T smi[W];
+      vload<T, W>(sm + ri.own, smi);
+      const T alpha = T(s_alpha[k]);
+      const T malpha = -alpha;
+      const T *const pn = odd ? pick<NR>(a.p1, k) : pick<NR>(a.p0, k);
+      const T *tk = pick<NR>(a.t, k);
+      T *xk = pick<NR>(a.x, k);
+      T *rk = pick<NR>(a.r, k);
 #pragma unroll
-    for (int j = 0; j < 2 * kMaxRhs; j++) acc[j] = 0.0;
-    for (uint32_t i = i0; i < V; i += stride) {
-      const Site s = make_site(g, i);
-      const T smi = sm[i];
+      for (int c = 0; c < NC; c++) {
+        const size_t off = size_t(c) * V;
+        Nb<T> n[W];
+        T ap[W], pv[W], xv[W], rv[W];
+        gather_item<T, W>(ri, tk + off, n);
+        vload<T, W>(pn + off + ri.own, pv);
+        vload<T, W>(xk + off + ri.own, xv);
+        vload<T, W>(rk + off + ri.own, rv);
+        item_M<T, W>(ri, smi, n, ap);
+        double sr = 0.0;
 #pragma unroll
-      for (int k = 0; k < NR; k++) {
-        if (k >= a.nrhs || !s_active[k]) continue;
-        const T alpha = T(s_alpha[k]);
-        const T malpha = -alpha;
-        const T *const pn = (it & 1) ? a.p1[k] : a.p0[k];
-#pragma unroll
-        for (int c = 0; c < NC; c++) {
-          const size_t off = size_t(c) * V;
-          const T *tv = a.t[k] + off;
-          const Nb<T> n = gather7<T>(s, i, [&](uint32_t j) { return tv[j]; });
-          const T ap = apply_M<T>(s, smi, n);
-          const T pi = pn[off + i];
-          a.x[k][off + i] = a.x[k][off + i] + alpha * pi;
-          const T ri = a.r[k][off + i] + malpha * ap;
-          a.r[k][off + i] = ri;
-          acc[k] += double(ri) * double(ri);
+        for (int e = 0; e < W; e++) {
+          xv[e] = xv[e] + alpha * pv[e];
+          rv[e] = rv[e] + malpha * ap[e];
+          sr += double(rv[e]) * double(rv[e]);
         }
+        acc_add<NR>(acc, k, sr);
+        vstore<T, W>(xk + off + ri.own, xv);
+        vstore<T, W>(rk + off + ri.own, rv);
       }
-    }
+    });
     ok = end_phase<NR>(acc, sh, part1, a.bar, nph++, a.err, abort_req);
     if (!ok) break;
     if (threadIdx.x < kMaxRhs) {
@@ -287,8 +388,10 @@ __global__ void __launch_bounds__(BS, 1) cg_kernel(CgArgs<T> a) {
         s_r2[k] = r2;
       }
     }
-    // host abort request: block 0's view decides for everyone at the next phase
     __syncthreads();
+    if (threadIdx.x == 0) sys_list_from(s_run, s_active, a.nrhs);
+    __syncthreads();
+    // host abort request: block 0's view decides for everyone at the next phase
     if (sh.flag != 0) {  // block 0 saw the host's abort request at the last phase end
       if (threadIdx.x == 0 && blockIdx.x == 0) atomicExch(a.err, 2);
       ok = false;

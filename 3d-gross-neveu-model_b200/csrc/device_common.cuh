@@ -1,5 +1,6 @@
 // device_common.cuh -- building blocks shared by every kernel: the staggered
-// stencils, deterministic block reductions and a bounded grid barrier.
+// stencils and deterministic reductions.  (The solvers' grid barrier is in
+// phase_sync.cuh.)
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -121,69 +122,6 @@ __device__ __forceinline__ void two_sum(double a, double b, double &s, double &e
   s = a + b;
   double bb = s - a;
   e = (a - (s - bb)) + (b - bb);
-}
-
-// ------------------------------------------------------------------ grid barrier
-// A generation barrier for cooperative launches (all blocks co-resident).  Every
-// wait is bounded: after kSpinLimit polls (about a second) the waiting block sets
-// *err and returns false, so a kernel can never hang the device.
-struct GridBar {
-  unsigned count;
-  unsigned gen;
-};
-
-constexpr unsigned kSpinLimit = 1u << 24;
-
-__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
-  unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ unsigned atom_add_acq_rel(unsigned *p, unsigned v) {
-  unsigned old;
-  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
-  return old;
-}
-__device__ __forceinline__ void st_relaxed(unsigned *p, unsigned v) {
-  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ int ld_err(const int *p) {
-  int v;
-  asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-
-// Returns false if this block gave up waiting or another block reported an error.
-__device__ __forceinline__ bool grid_barrier(GridBar *bar, unsigned &gen_local, int *err) {
-  __syncthreads();
-  __shared__ int s_ok;
-  if (threadIdx.x == 0) {
-    int ok = 1;
-    __threadfence();
-    const unsigned g = gen_local;
-    const unsigned arrived = atom_add_acq_rel(&bar->count, 1u);
-    if (arrived == gridDim.x * gridDim.y * gridDim.z - 1u) {
-      st_relaxed(&bar->count, 0u);
-      __threadfence();
-      atom_add_acq_rel(&bar->gen, 1u);
-    } else {
-      unsigned spins = 0;
-      while (ld_acquire(&bar->gen) == g) {
-        if (++spins > kSpinLimit) {
-          atomicExch(err, 1);
-          ok = 0;
-          break;
-        }
-        __nanosleep(32);
-      }
-    }
-    __threadfence();
-    if (ld_err(err) != 0) ok = 0;
-    s_ok = ok;
-  }
-  gen_local++;
-  __syncthreads();
-  return s_ok != 0;
 }
 
 }  // namespace gn

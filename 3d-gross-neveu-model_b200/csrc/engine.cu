@@ -103,20 +103,20 @@ void Engine::dirac(const double *sm, const double *in, double *out, int ncomp, i
     mt_exact(sm, in, out, ncomp);
     return;
   }
-  if (L_ % 4 == 0) {  // two sites per thread, 128-bit loads
-    const dim3 grid(unsigned((V_ / 2 + kOpThreads - 1) / kOpThreads), unsigned(ncomp));
-    if (op == GN_OP_M) dirac_pair_kernel<0><<<grid, kOpThreads, 0, stream_>>>(g_, sm, in, out);
-    else if (op == GN_OP_MT) dirac_pair_kernel<1><<<grid, kOpThreads, 0, stream_>>>(g_, sm, in, out);
-    else dirac_pair_kernel<2><<<grid, kOpThreads, 0, stream_>>>(g_, sm, in, out);
-    check(cudaGetLastError(), "dirac_pair_kernel");
-    launches++;
-    return;
+  // W sites per thread (rowvec.cuh), 128-bit loads when L/2 is even and the arrays are 16-byte aligned
+  const void *ptrs[3] = {sm, in, out};
+  const int W = fp64_width(L_, ptrs, 3);
+  const dim3 grid(unsigned((V_ / W + kOpThreads - 1) / kOpThreads), unsigned(ncomp));
+  if (W == 2) {
+    if (op == GN_OP_M) dirac_item_kernel<2, 0><<<grid, kOpThreads, 0, stream_>>>(g_, sm, in, out);
+    else if (op == GN_OP_MT) dirac_item_kernel<2, 1><<<grid, kOpThreads, 0, stream_>>>(g_, sm, in, out);
+    else dirac_item_kernel<2, 2><<<grid, kOpThreads, 0, stream_>>>(g_, sm, in, out);
+  } else {
+    if (op == GN_OP_M) dirac_item_kernel<1, 0><<<grid, kOpThreads, 0, stream_>>>(g_, sm, in, out);
+    else if (op == GN_OP_MT) dirac_item_kernel<1, 1><<<grid, kOpThreads, 0, stream_>>>(g_, sm, in, out);
+    else dirac_item_kernel<1, 2><<<grid, kOpThreads, 0, stream_>>>(g_, sm, in, out);
   }
-  const dim3 grid(unsigned((V_ + kOpThreads - 1) / kOpThreads), unsigned(ncomp));
-  if (op == GN_OP_M) dirac_kernel<double, 0><<<grid, kOpThreads, 0, stream_>>>(g_, sm, in, out);
-  else if (op == GN_OP_MT) dirac_kernel<double, 1><<<grid, kOpThreads, 0, stream_>>>(g_, sm, in, out);
-  else dirac_kernel<double, 2><<<grid, kOpThreads, 0, stream_>>>(g_, sm, in, out);
-  check(cudaGetLastError(), "dirac_kernel");
+  check(cudaGetLastError(), "dirac_item_kernel");
   launches++;
 }
 
@@ -179,36 +179,34 @@ void Engine::cond_fill(int mode, const signed char *signs, const double *table, 
   launches++;
 }
 
-// Instantiated solver kernels: (planes, RHS slots) = (1, 1), (1, 2), (1, 4), (2, 1), (2, 2).
-int rhs_slots(int nrhs) { return nrhs <= 1 ? 1 : (nrhs <= 2 ? 2 : 4); }
-
-// Block shape of a solve: the tunable shape for one plane and up to two
-// systems (the hot cases), the fixed shape otherwise.
-int threads_for(int ncomp, int nrhs) { return (ncomp == 1 && nrhs <= 2) ? solver_threads() : kSolverThreads; }
-
-const void *Engine::fp64_kernel_ptr(int ncomp, int nrhs) {
-  const int nr = rhs_slots(nrhs);
-  constexpr int B = kSolverThreads;
-  const bool wide = solver_threads() == 768;
+template <int W>
+static const void *fp64_kernel(int ncomp, int nr) {
   if (ncomp == 1) {
-    if (nr == 1) return wide ? (const void *)cg_kernel<double, 1, 1, 768> : (const void *)cg_kernel<double, 1, 1, 512>;
-    if (nr == 2) return wide ? (const void *)cg_kernel<double, 1, 2, 768> : (const void *)cg_kernel<double, 1, 2, 512>;
-    return (const void *)cg_kernel<double, 1, 4, B>;
+    if (nr == 1) return (const void *)cg_kernel<double, 1, 1, kWideThreads, W>;
+    if (nr == 2) return (const void *)cg_kernel<double, 1, 2, kWideThreads, W>;
+    return (const void *)cg_kernel<double, 1, 4, kSolverThreads, W>;
   }
-  if (nr == 1) return (const void *)cg_kernel<double, 2, 1, B>;
-  if (nr == 2) return (const void *)cg_kernel<double, 2, 2, B>;
+  if (nr == 1) return (const void *)cg_kernel<double, 2, 1, kSolverThreads, W>;
+  if (nr == 2) return (const void *)cg_kernel<double, 2, 2, kSolverThreads, W>;
   throw GnError(GN_ERR_ARG, "complex systems: at most 2 right-hand sides per solve");
 }
 
-int Engine::cg_blocks(int ncomp, int nrhs, bool mixed) {
+const void *Engine::fp64_kernel_ptr(int ncomp, int nrhs, int w) {
   const int nr = rhs_slots(nrhs);
-  int &cached = cg_blocks_cache_[mixed ? 1 : 0][ncomp - 1][nr == 1 ? 0 : (nr == 2 ? 1 : 2)];
+  return w == 2 ? fp64_kernel<2>(ncomp, nr) : fp64_kernel<1>(ncomp, nr);
+}
+
+// Grid of a solve (cached per kernel and system count): one work unit per
+// thread of its hot sweeps (the FP64 ones of the FP64 solver, the FP32 ones of
+// the mixed solver, whose rarer FP64 sweeps then take two rounds).
+int Engine::cg_blocks(int ncomp, int nrhs, bool mixed, int w) {
+  int &cached = cg_blocks_cache_[mixed ? 1 : 0][ncomp - 1][nrhs - 1][w == 4 ? 2 : w - 1];
   if (cached) return cached;
-  const void *fn = mixed ? mixed_kernel_ptr(ncomp, nrhs) : fp64_kernel_ptr(ncomp, nrhs);
+  const void *fn = mixed ? mixed_kernel_ptr(ncomp, nrhs, w) : fp64_kernel_ptr(ncomp, nrhs, w);
   const int bs = threads_for(ncomp, nrhs);
   const int capacity = coop_capacity(fn, bs);
   if (capacity < 1) throw GnError(GN_ERR_CUDA, "CG kernel cannot be resident as a cooperative grid");
-  cached = solver_grid(V_, capacity, max_blocks_, bs);
+  cached = solver_grid(solver_units(V_, w, nrhs), capacity, max_blocks_, bs);
   return cached;
 }
 
@@ -244,8 +242,15 @@ int Engine::solve(const double *sm, const double *const *b, double *const *x, in
   a.state = state_;
   check(cudaMemsetAsync(bar_, 0, sizeof(PhaseBar), stream_), "memset");
   check(cudaMemsetAsync(err_, 0, sizeof(int), stream_), "memset");
-  const int nb = cg_blocks(ncomp, nrhs, false);
-  check(launch_solver(fp64_kernel_ptr(ncomp, nrhs), nb, threads_for(ncomp, nrhs), a, stream_), "cg_kernel launch");
+  const void *ptrs[2 * kMaxRhs + 1] = {sm};
+  for (int k = 0; k < nrhs; k++) {
+    ptrs[1 + 2 * k] = b[k];
+    ptrs[2 + 2 * k] = x[k];
+  }
+  const int w = fp64_width(L_, ptrs, 1 + 2 * nrhs);
+  const int nb = cg_blocks(ncomp, nrhs, false, w);
+  check(launch_solver(fp64_kernel_ptr(ncomp, nrhs, w), nb, threads_for(ncomp, nrhs), a, stream_),
+        "cg_kernel launch");
   launches++;
   return finish_solve(nrhs, info);
 }

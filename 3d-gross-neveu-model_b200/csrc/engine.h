@@ -101,12 +101,12 @@ class Engine {
   void energy_exact(const double *P, const double *phi, const double *X, const double *sigma, double out[3]);
   void cond_dots_exact(const double *v, const double *D, double out[4]);
   void mixed_init();
-  const void *mixed_kernel_ptr(int ncomp, int nrhs);
-  const void *fp64_kernel_ptr(int ncomp, int nrhs);
+  const void *mixed_kernel_ptr(int ncomp, int nrhs, int w);
+  const void *fp64_kernel_ptr(int ncomp, int nrhs, int w);
   int solve_mixed(const double *sm, const double *const *b, double *const *x, int nrhs, int ncomp, double tol,
                   int variant, int rel, long long max_iter, SolveInfo *info);
   void *alloc(size_t bytes);
-  int cg_blocks(int ncomp, int nrhs, bool mixed);
+  int cg_blocks(int ncomp, int nrhs, bool mixed, int w);
 
   int L_, device_;
   int64_t V_;
@@ -123,7 +123,7 @@ class Engine {
   double *table_ = nullptr;
   // solver workspace
   double *cg_work_ = nullptr;  // kMaxRhs * 4 vectors * 2 planes * V
-  float *mx_work_ = nullptr;   // mixed precision: kMaxRhs * 6 vectors * 2 planes * V
+  float *mx_work_ = nullptr;   // mixed precision: kMaxRhs * 4 vectors * 2 planes * V
   float *sm32_ = nullptr;
   double *partials_ = nullptr;
   double *h_partials_ = nullptr;
@@ -135,13 +135,8 @@ class Engine {
   int *d_abort_ = nullptr;
   double *h_stage_ = nullptr;
   int max_blocks_ = 0;
-  int cg_blocks_cache_[2][2][3] = {};
+  int cg_blocks_cache_[2][2][kMaxRhs][3] = {};  // [mixed][ncomp-1][nrhs-1][log2 w]
 };
-
-// Number of right-hand-side slots (1, 2 or 4) of the solver instantiation used for nrhs systems.
-int rhs_slots(int nrhs);
-// Threads per block of the solver used for nrhs systems of ncomp planes.
-int threads_for(int ncomp, int nrhs);
 
 // Host-side compensated sum of (hi, lo) block partials.
 double sum_partials(const double *part, int nb, int q);

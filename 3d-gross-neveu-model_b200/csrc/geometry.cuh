@@ -49,7 +49,7 @@ struct Geom {
   int64_t V;     // L^3
   int64_t half;  // V / 2
   int plane;     // L * Lh: sites of one parity in an x0-slice
-  FastDiv div_Lh, div_L;
+  FastDiv div_Lh, div_L, div_Lq;  // division by L/2, L, L/4 (the last only for L % 4 == 0)
 };
 
 inline Geom make_geom(int L) {
@@ -61,6 +61,7 @@ inline Geom make_geom(int L) {
   g.plane = L * (L / 2);
   g.div_Lh = make_fastdiv(uint32_t(L / 2));
   g.div_L = make_fastdiv(uint32_t(L));
+  g.div_Lq = make_fastdiv(uint32_t(L % 4 == 0 ? L / 4 : 1));
   return g;
 }
 

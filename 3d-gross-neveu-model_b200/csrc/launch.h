@@ -8,26 +8,31 @@
 #include <cstdlib>
 
 #include "cg_kernel.cuh"
+#include "rowvec.cuh"
 
 namespace gn {
 
 // Threads per block of the solvers: one large block per SM (launch bounds
 // (BS, 1)), because every block arriving at a grid barrier costs about 8 ns
-// (measured).  Two shapes are built: 512 threads (up to 128 registers) and 768
-// (80 registers).  solver_threads() picks one for every entry point alike: the
-// environment variable GN_SOLVER_THREADS (512 or 768, for tuning sweeps) or
-// else kDefaultSolverThreads, the shape measured fastest at every L from 8 to
-// 128 (bench.py --case cgscan).
-constexpr int kDefaultSolverThreads = 768;
-constexpr int kSolverThreads = 512;  // shape of the rarely used instantiations
+// (measured).  The hot shapes (one real plane, up to two systems: the two
+// pseudofermion flavours) use 768 threads (80 registers), measured fastest at
+// every L from 8 to 128; the rarely used ones 512 (up to 128 registers).
+constexpr int kWideThreads = 1024;
+constexpr int kSolverThreads = 512;
 
-inline int solver_threads() {
-  static const int bs = [] {
-    const char *e = getenv("GN_SOLVER_THREADS");
-    const int v = e ? atoi(e) : kDefaultSolverThreads;
-    return (v == 512 || v == 768) ? v : kDefaultSolverThreads;
-  }();
-  return bs;
+// Instantiated solver kernels: (planes, RHS slots) = (1, 1), (1, 2), (1, 4), (2, 1), (2, 2).
+inline int rhs_slots(int nrhs) { return nrhs <= 1 ? 1 : (nrhs <= 2 ? 2 : 4); }
+inline int threads_for(int ncomp, int nrhs) { return (ncomp == 1 && nrhs <= 2) ? kWideThreads : kSolverThreads; }
+
+inline bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// Sites per item of the FP64 sweeps (rowvec.cuh): 2, with 16-byte loads, when
+// L/2 is even and every array the caller passed is 16-byte aligned; else 1.
+inline int fp64_width(int L, const void *const *ptrs, int n) {
+  if (row_width(L, 2) != 2) return 1;
+  for (int i = 0; i < n; i++)
+    if (ptrs[i] != nullptr && !aligned16(ptrs[i])) return 1;
+  return 2;
 }
 
 // Largest co-resident grid (in blocks) for `fn` launched with bs threads; 0 on error.
@@ -39,10 +44,13 @@ inline int coop_capacity(const void *fn, int bs) {
   return per_sm * sms;
 }
 
-// Grid of a solve over V sites: one site per thread at most, within the
-// co-resident capacity and cap_blocks.
-inline int solver_grid(int64_t V, int capacity, int cap_blocks, int bs) {
-  int64_t want = (V + bs - 1) / bs;
+// Work units of a sweep: (system, item) pairs, items of w sites.
+inline int64_t solver_units(int64_t V, int w, int nrhs) { return int64_t(nrhs) * (V / w); }
+
+// Grid of a solve with `units` work units: one unit per thread at most, within
+// the co-resident capacity and cap_blocks.
+inline int solver_grid(int64_t units, int capacity, int cap_blocks, int bs) {
+  int64_t want = (units + bs - 1) / bs;
   int64_t cap = capacity < cap_blocks ? capacity : cap_blocks;
   return int(want < cap ? want : cap);
 }

@@ -10,9 +10,9 @@
 
 namespace gn {
 
-constexpr int kMixedVecs = 5;  // r^, p^0, p^1, t^, x^ per right-hand side
+constexpr int kMixedVecs = 4;  // r^, p^, t^, x^ per right-hand side
 constexpr double kDelta = 0.01;  // reliable update when |r^| drops by this factor
-constexpr int kReliableEvery = 50;
+constexpr int kReliableEvery = 100;
 
 void Engine::mixed_init() {
   const size_t V = size_t(V_);
@@ -20,18 +20,24 @@ void Engine::mixed_init() {
   sm32_ = (float *)alloc(V * sizeof(float));
 }
 
-const void *Engine::mixed_kernel_ptr(int ncomp, int nrhs) {
-  const int nr = rhs_slots(nrhs);
-  constexpr int B = kSolverThreads;
-  const bool wide = solver_threads() == 768;
+template <int W>
+static const void *mixed_kernel(int ncomp, int nr) {
   if (ncomp == 1) {
-    if (nr == 1) return wide ? (const void *)cg_mixed_kernel<1, 1, 768> : (const void *)cg_mixed_kernel<1, 1, 512>;
-    if (nr == 2) return wide ? (const void *)cg_mixed_kernel<1, 2, 768> : (const void *)cg_mixed_kernel<1, 2, 512>;
-    return (const void *)cg_mixed_kernel<1, 4, B>;
+    if (nr == 1) return (const void *)cg_mixed_kernel<1, 1, kWideThreads, W>;
+    if (nr == 2) return (const void *)cg_mixed_kernel<1, 2, kWideThreads, W>;
+    return (const void *)cg_mixed_kernel<1, 4, kSolverThreads, W>;
   }
-  if (nr == 1) return (const void *)cg_mixed_kernel<2, 1, B>;
-  if (nr == 2) return (const void *)cg_mixed_kernel<2, 2, B>;
+  if (nr == 1) return (const void *)cg_mixed_kernel<2, 1, kSolverThreads, W>;
+  if (nr == 2) return (const void *)cg_mixed_kernel<2, 2, kSolverThreads, W>;
   throw GnError(GN_ERR_ARG, "complex systems: at most 2 right-hand sides per solve");
+}
+
+// w: sites per item of the FP32 sweeps (1, 2 or 4)
+const void *Engine::mixed_kernel_ptr(int ncomp, int nrhs, int w) {
+  const int nr = rhs_slots(nrhs);
+  if (w == 4) return mixed_kernel<4>(ncomp, nr);
+  if (w == 2) return mixed_kernel<2>(ncomp, nr);
+  return mixed_kernel<1>(ncomp, nr);
 }
 
 int Engine::solve_mixed(const double *sm, const double *const *b, double *const *x, int nrhs, int ncomp, double tol,
@@ -48,10 +54,9 @@ int Engine::solve_mixed(const double *sm, const double *const *b, double *const 
     a.x[k] = x[k];
     a.t64[k] = cg_work_ + size_t(k) * 4 * 2 * V;
     a.rh[k] = w;
-    a.ph0[k] = w + 2 * V;
-    a.ph1[k] = w + 4 * V;
-    a.th[k] = w + 6 * V;
-    a.xh[k] = w + 8 * V;
+    a.ph[k] = w + 2 * V;
+    a.th[k] = w + 4 * V;
+    a.xh[k] = w + 6 * V;
   }
   a.nrhs = nrhs;
   a.variant = variant;
@@ -67,8 +72,16 @@ int Engine::solve_mixed(const double *sm, const double *const *b, double *const 
   a.state = state_;
   check(cudaMemsetAsync(bar_, 0, sizeof(PhaseBar), stream_), "memset");
   check(cudaMemsetAsync(err_, 0, sizeof(int), stream_), "memset");
-  const int nb = cg_blocks(ncomp, nrhs, true);
-  check(launch_solver(mixed_kernel_ptr(ncomp, nrhs), nb, threads_for(ncomp, nrhs), a, stream_),
+  // FP32 sweeps in items of up to 4 sites (float4) when the caller's FP64
+  // arrays allow the 2-site FP64 sweeps, else one site per item throughout
+  const void *ptrs[2 * kMaxRhs + 1] = {sm};
+  for (int k = 0; k < nrhs; k++) {
+    ptrs[1 + 2 * k] = b[k];
+    ptrs[2 + 2 * k] = x[k];
+  }
+  const int w = fp64_width(L_, ptrs, 1 + 2 * nrhs) == 2 ? row_width(L_, 4) : 1;
+  const int nb = cg_blocks(ncomp, nrhs, true, w);
+  check(launch_solver(mixed_kernel_ptr(ncomp, nrhs, w), nb, threads_for(ncomp, nrhs), a, stream_),
         "cg_mixed_kernel launch");
   launches++;
   return finish_solve(nrhs, info);

@@ -13,12 +13,15 @@
 // passes the tolerance; the solve stops only on the FP64 true residual, so its
 // stopping rule is the same as the FP64 solver's.
 //
-// Inner iteration, two phases (12 FP32 words per site and RHS):
-//   A: p^ <- r^ + beta p^ (on the fly at the 7 points), t^ = M^T p^, sum t^2
+// Inner iteration, two phases (11 FP32 words per site and RHS):
+//   A: p^ <- r^ + beta p^, t^ <- M^T r^ + beta t^ (= M^T p^), sum t^2
 //   B: x^ += alpha p^, r^ -= alpha M t^, sum r^2
 // Reliable update, two phases (FP64):
 //   C: t = M^T (x + x^) (on the fly at the 7 points)
 //   D: x += x^, x^ = 0, r = b - M t, r^ = (float) r, sum r^2
+// The FP32 phases sweep row items of W sites (rowvec.cuh; W = 4, one float4
+// per vector, when 4 divides L/2), the FP64 phases items of min(W, 2) sites;
+// a work unit is one (system, item) pair, as in cg_kernel.cuh.
 #pragma once
 #include "cg_kernel.cuh"
 
@@ -32,8 +35,7 @@ struct MixedArgs {
   double *x[kMaxRhs];
   double *t64[kMaxRhs];
   float *rh[kMaxRhs];
-  float *ph0[kMaxRhs];
-  float *ph1[kMaxRhs];
+  float *ph[kMaxRhs];
   float *th[kMaxRhs];
   float *xh[kMaxRhs];
   int nrhs;
@@ -50,20 +52,21 @@ struct MixedArgs {
   CgState *state;
 };
 
-template <int NC, int NR, int BS>
+template <int NC, int NR, int BS, int W>
 __global__ void __launch_bounds__(BS, 1) cg_mixed_kernel(MixedArgs a) {
+  constexpr int W64 = W >= 2 ? 2 : 1;
   __shared__ SyncShared sh;
   double *const s_val = sh.val;
   __shared__ double s_alpha[kMaxRhs], s_beta[kMaxRhs], s_rr[kMaxRhs], s_tau[kMaxRhs], s_rmax[kMaxRhs];
   __shared__ double s_r2[kMaxRhs], s_b2[kMaxRhs];
   __shared__ int s_active[kMaxRhs], s_status[kMaxRhs], s_ru[kMaxRhs], s_since[kMaxRhs], s_nru[kMaxRhs];
+  __shared__ int s_all[kMaxRhs];
   __shared__ long long s_iters[kMaxRhs];
-  __shared__ int s_any_ru;
+  __shared__ SysList s_run, s_every, s_upd;  // iterating / all / taking a reliable update
 
   const Geom g = a.g;
   const uint32_t V = uint32_t(g.V);
-  const uint32_t stride = gridDim.x * blockDim.x;
-  const uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t NI = row_items<W>(g), NI64 = row_items<W64>(g);
   double *part0 = a.partials;
   double *part1 = a.partials + size_t(kSyncQ + 1) * gridDim.x;
   unsigned long long nph = 0;  // phases ended so far (same count in every block)
@@ -72,6 +75,7 @@ __global__ void __launch_bounds__(BS, 1) cg_mixed_kernel(MixedArgs a) {
   if (threadIdx.x < kMaxRhs) {
     const int k = threadIdx.x;
     s_active[k] = k < a.nrhs;
+    s_all[k] = k < a.nrhs;
     s_status[k] = k < a.nrhs ? kCgRunning : kCgConverged;
     s_iters[k] = 0;
     s_alpha[k] = s_beta[k] = s_rr[k] = s_r2[k] = s_b2[k] = s_rmax[k] = 0.0;
@@ -81,48 +85,64 @@ __global__ void __launch_bounds__(BS, 1) cg_mixed_kernel(MixedArgs a) {
     s_nru[k] = 0;
   }
   __syncthreads();
+  if (threadIdx.x == 0) {
+    sys_list_from(s_every, s_all, a.nrhs);
+    sys_list_from(s_run, s_active, a.nrhs);
+  }
+  __syncthreads();
   bool ok = true;
   double acc[2 * kMaxRhs];
+  auto zero_acc = [&]() {
+#pragma unroll
+    for (int q = 0; q < 2 * kMaxRhs; q++) acc[q] = 0.0;
+  };
 
   // ---------------------------------------------------------------- start (FP64)
   if (a.variant == 0) {
-    for (uint32_t i = i0; i < V; i += stride) {
-      const Site s = make_site(g, i);
-      const double smi = sm[i];
+    for_units(NI64, s_every, [&](int k, uint32_t j) {
+      const RowItem it = make_item<W64>(g, j);
+      double smi[W64];
+      vload<double, W64>(sm + it.own, smi);
+      const double *xk = pick<NR>(a.x, k);
+      double *tk = pick<NR>(a.t64, k);
 #pragma unroll
-      for (int k = 0; k < NR; k++) {
-        if (k >= a.nrhs) break;
+      for (int c = 0; c < NC; c++) {
+        Nb<double> n[W64];
+        double o[W64];
+        gather_item<double, W64>(it, xk + size_t(c) * V, n);
+        item_Mt<double, W64>(it, smi, n, o);
+        vstore<double, W64>(tk + size_t(c) * V + it.own, o);
+      }
+    });
+    zero_acc();
+    ok = end_phase<1>(acc, sh, part1, a.bar, nph++, a.err);
+    zero_acc();
+    if (ok) {
+      for_units(NI64, s_every, [&](int k, uint32_t j) {
+        const RowItem it = make_item<W64>(g, j);
+        double smi[W64];
+        vload<double, W64>(sm + it.own, smi);
+        const double *tk = pick<NR>(a.t64, k);
+        const double *bk = pick<NR>(a.b, k);
 #pragma unroll
         for (int c = 0; c < NC; c++) {
-          const double *xv = a.x[k] + size_t(c) * V;
-          const Nb<double> n = gather7<double>(s, i, [&](uint32_t j) { return xv[j]; });
-          a.t64[k][size_t(c) * V + i] = apply_Mt<double>(s, smi, n);
-        }
-      }
-    }
+          Nb<double> n[W64];
+          double bi[W64], ri[W64];
+          gather_item<double, W64>(it, tk + size_t(c) * V, n);
+          vload<double, W64>(bk + size_t(c) * V + it.own, bi);
 #pragma unroll
-    for (int j = 0; j < 2 * kMaxRhs; j++) acc[j] = 0.0;
-    ok = end_phase<1>(acc, sh, part1, a.bar, nph++, a.err);
+          for (int e = 0; e < W64; e++) ri[e] = bi[e];
+          item_sub_M<double, W64>(it, smi, n, ri);
+          double sr = 0.0, sb = 0.0;
 #pragma unroll
-    for (int j = 0; j < 2 * kMaxRhs; j++) acc[j] = 0.0;
-    if (ok) {
-      for (uint32_t i = i0; i < V; i += stride) {
-        const Site s = make_site(g, i);
-        const double smi = sm[i];
-#pragma unroll
-        for (int k = 0; k < NR; k++) {
-          if (k >= a.nrhs) break;
-#pragma unroll
-          for (int c = 0; c < NC; c++) {
-            const double *tv = a.t64[k] + size_t(c) * V;
-            const Nb<double> n = gather7<double>(s, i, [&](uint32_t j) { return tv[j]; });
-            const double bi = a.b[k][size_t(c) * V + i];
-            const double ri = apply_sub_M<double>(s, bi, smi, n);
-            acc[k] += ri * ri;
-            acc[NR + k] += bi * bi;
+          for (int e = 0; e < W64; e++) {
+            sr += ri[e] * ri[e];
+            sb += bi[e] * bi[e];
           }
+          acc_add<NR>(acc, k, sr);
+          acc_add<NR>(acc, NR + k, sb);
         }
-      }
+      });
     }
     ok = end_phase<2 * NR>(acc, sh, part0, a.bar, nph++, a.err) && ok;
     if (threadIdx.x < kMaxRhs) {
@@ -139,30 +159,51 @@ __global__ void __launch_bounds__(BS, 1) cg_mixed_kernel(MixedArgs a) {
       }
     }
     __syncthreads();
+    if (threadIdx.x == 0) sys_list_from(s_run, s_active, a.nrhs);
+    __syncthreads();
   }
   // x = 0, x^ = 0, r^ = p^ = (float) b, sm32 = (float) sm ; sums r^2 (FP32 values), b^2
-#pragma unroll
-  for (int j = 0; j < 2 * kMaxRhs; j++) acc[j] = 0.0;
+  zero_acc();
   if (ok) {
-    for (uint32_t i = i0; i < V; i += stride) {
-      a.sm32[i] = float(sm[i]);
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < NI64; j += gridDim.x * blockDim.x) {
+      const uint32_t own = make_item<W64>(g, j).own;
+      double s64[W64];
+      float s32[W64];
+      vload<double, W64>(sm + own, s64);
 #pragma unroll
-      for (int k = 0; k < NR; k++) {
-        if (k >= a.nrhs || !s_active[k]) continue;
-#pragma unroll
-        for (int c = 0; c < NC; c++) {
-          const size_t j = size_t(c) * V + i;
-          const double bi = a.b[k][j];
-          const float bf = float(bi);
-          a.x[k][j] = 0.0;
-          a.xh[k][j] = 0.f;
-          a.rh[k][j] = bf;
-          a.ph0[k][j] = bf;
-          acc[k] += double(bf) * double(bf);
-          acc[NR + k] += bi * bi;
-        }
-      }
+      for (int e = 0; e < W64; e++) s32[e] = float(s64[e]);
+      vstore<float, W64>(a.sm32 + own, s32);
     }
+    for_units(NI64, s_run, [&](int k, uint32_t j) {
+      const uint32_t own = make_item<W64>(g, j).own;
+      const double *bk = pick<NR>(a.b, k);
+      double *xk = pick<NR>(a.x, k);
+      float *xhk = pick<NR>(a.xh, k);
+      float *rhk = pick<NR>(a.rh, k);
+      float *phk = pick<NR>(a.ph, k);
+#pragma unroll
+      for (int c = 0; c < NC; c++) {
+        const size_t off = size_t(c) * V + own;
+        double bi[W64], z64[W64];
+        float bf[W64], z32[W64];
+        vload<double, W64>(bk + off, bi);
+        double sf = 0.0, sb = 0.0;
+#pragma unroll
+        for (int e = 0; e < W64; e++) {
+          bf[e] = float(bi[e]);
+          z64[e] = 0.0;
+          z32[e] = 0.f;
+          sf += double(bf[e]) * double(bf[e]);
+          sb += bi[e] * bi[e];
+        }
+        acc_add<NR>(acc, k, sf);
+        acc_add<NR>(acc, NR + k, sb);
+        vstore<double, W64>(xk + off, z64);
+        vstore<float, W64>(xhk + off, z32);
+        vstore<float, W64>(rhk + off, bf);
+        vstore<float, W64>(phk + off, bf);
+      }
+    });
   }
   ok = end_phase<2 * NR>(acc, sh, part1, a.bar, nph++, a.err) && ok;
   if (threadIdx.x < kMaxRhs) {
@@ -182,50 +223,57 @@ __global__ void __launch_bounds__(BS, 1) cg_mixed_kernel(MixedArgs a) {
     }
   }
   __syncthreads();
+  if (threadIdx.x == 0) sys_list_from(s_run, s_active, a.nrhs);
+  __syncthreads();
 
   // ---------------------------------------------------------------- iterations
   long long it = 0;
   for (; ok && it < a.max_iter; it++) {
-    int any = 0;
-#pragma unroll
-    for (int k = 0; k < kMaxRhs; k++) any |= (k < a.nrhs) ? s_active[k] : 0;
-    if (!any) break;
+    if (s_run.n == 0) break;
     // the host's abort request lives in mapped host memory: one thread reads it
     // every 16 iterations, and the value is only used at the end of phase B
     int abort_req = 0;
     if (blockIdx.x == 0 && threadIdx.x == 0 && a.abort_flag != nullptr && (it & 15) == 0)
       abort_req = *(volatile const int *)a.abort_flag;
-    // A: p^ = r^ + beta p^, t^ = M^T p^
+    // A: p^ = r^ + beta p^, t^ = M^T p^ = M^T r^ + beta t^ (linearity: only r^
+    // is gathered; p^ and t^ are updated in place at the unit's own sites)
+    zero_acc();
+    for_units(NI, s_run, [&](int k, uint32_t j) {
+      const RowItem ri = make_item<W>(g, j);
+      float smi[W];
+      vload<float, W>(a.sm32 + ri.own, smi);
+      const float beta = float(s_beta[k]);
+      float *const pk = pick<NR>(a.ph, k);
+      const float *rk = pick<NR>(a.rh, k);
+      float *tk = pick<NR>(a.th, k);
 #pragma unroll
-    for (int j = 0; j < 2 * kMaxRhs; j++) acc[j] = 0.0;
-    for (uint32_t i = i0; i < V; i += stride) {
-      const Site s = make_site(g, i);
-      const float smi = a.sm32[i];
+      for (int c = 0; c < NC; c++) {
+        const size_t off = size_t(c) * V;
+        Nb<float> n[W];
+        float ti[W];
+        if (it == 0) {  // p^ = b^ (set above): t^ = M^T p^
+          gather_item<float, W>(ri, pk + off, n);
+          item_Mt<float, W>(ri, smi, n, ti);
+        } else {
+          float u[W], told[W], pold[W];
+          gather_item<float, W>(ri, rk + off, n);
+          vload<float, W>(tk + off + ri.own, told);
+          vload<float, W>(pk + off + ri.own, pold);
+          item_Mt<float, W>(ri, smi, n, u);
 #pragma unroll
-      for (int k = 0; k < NR; k++) {
-        if (k >= a.nrhs || !s_active[k]) continue;
-        const float beta = float(s_beta[k]);
-        float *const pn = (it & 1) ? a.ph1[k] : a.ph0[k];
-        const float *const po = (it & 1) ? a.ph0[k] : a.ph1[k];
-#pragma unroll
-        for (int c = 0; c < NC; c++) {
-          const size_t off = size_t(c) * V;
-          Nb<float> n;
-          if (it == 0) {
-            const float *pv = pn + off;
-            n = gather7<float>(s, i, [&](uint32_t j) { return pv[j]; });
-          } else {
-            const float *rv = a.rh[k] + off;
-            const float *pov = po + off;
-            n = gather7<float>(s, i, [&](uint32_t j) { return fmaf(beta, pov[j], rv[j]); });
-            pn[off + i] = n.c;
+          for (int e = 0; e < W; e++) {
+            ti[e] = fmaf(beta, told[e], u[e]);
+            pold[e] = fmaf(beta, pold[e], n[e].c);
           }
-          const float ti = apply_Mt<float>(s, smi, n);
-          a.th[k][off + i] = ti;
-          acc[k] += double(ti) * double(ti);
+          vstore<float, W>(pk + off + ri.own, pold);
         }
+        vstore<float, W>(tk + off + ri.own, ti);
+        double st = 0.0;
+#pragma unroll
+        for (int e = 0; e < W; e++) st += double(ti[e]) * double(ti[e]);
+        acc_add<NR>(acc, k, st);
       }
-    }
+    });
     ok = end_phase<NR>(acc, sh, part0, a.bar, nph++, a.err);
     if (!ok) break;
     if (threadIdx.x < kMaxRhs) {
@@ -234,33 +282,41 @@ __global__ void __launch_bounds__(BS, 1) cg_mixed_kernel(MixedArgs a) {
     }
     __syncthreads();
     // B: x^ += alpha p^, r^ -= alpha M t^
+    zero_acc();
+    for_units(NI, s_run, [&](int k, uint32_t j) {
+      const RowItem ri = make_item<W>(g, j);
+      float smi[W];
+      vload<float, W>(a.sm32 + ri.own, smi);
+      const float alpha = float(s_alpha[k]);
+      const float *const pn = pick<NR>(a.ph, k);
+      const float *tk = pick<NR>(a.th, k);
+      float *xhk = pick<NR>(a.xh, k);
+      float *rk = pick<NR>(a.rh, k);
 #pragma unroll
-    for (int j = 0; j < 2 * kMaxRhs; j++) acc[j] = 0.0;
-    for (uint32_t i = i0; i < V; i += stride) {
-      const Site s = make_site(g, i);
-      const float smi = a.sm32[i];
+      for (int c = 0; c < NC; c++) {
+        const size_t off = size_t(c) * V + ri.own;
+        Nb<float> n[W];
+        float ap[W], pv[W], xv[W], rv[W];
+        gather_item<float, W>(ri, tk + size_t(c) * V, n);
+        vload<float, W>(pn + off, pv);
+        vload<float, W>(xhk + off, xv);
+        vload<float, W>(rk + off, rv);
+        item_M<float, W>(ri, smi, n, ap);
+        double sr = 0.0;
 #pragma unroll
-      for (int k = 0; k < NR; k++) {
-        if (k >= a.nrhs || !s_active[k]) continue;
-        const float alpha = float(s_alpha[k]);
-        const float *const pn = (it & 1) ? a.ph1[k] : a.ph0[k];
-#pragma unroll
-        for (int c = 0; c < NC; c++) {
-          const size_t off = size_t(c) * V;
-          const float *tv = a.th[k] + off;
-          const Nb<float> n = gather7<float>(s, i, [&](uint32_t j) { return tv[j]; });
-          const float ap = apply_M<float>(s, smi, n);
-          a.xh[k][off + i] = fmaf(alpha, pn[off + i], a.xh[k][off + i]);
-          const float ri = fmaf(-alpha, ap, a.rh[k][off + i]);
-          a.rh[k][off + i] = ri;
-          acc[k] += double(ri) * double(ri);
+        for (int e = 0; e < W; e++) {
+          xv[e] = fmaf(alpha, pv[e], xv[e]);
+          rv[e] = fmaf(-alpha, ap[e], rv[e]);
+          sr += double(rv[e]) * double(rv[e]);
         }
+        acc_add<NR>(acc, k, sr);
+        vstore<float, W>(xhk + off, xv);
+        vstore<float, W>(rk + off, rv);
       }
-    }
+    });
     ok = end_phase<NR>(acc, sh, part1, a.bar, nph++, a.err, abort_req);
     if (!ok) break;
-    if (threadIdx.x == 0) s_any_ru = 0;
-    __syncthreads();
+    const int abort_seen = sh.flag;  // block 0's abort flag (the next phase ends overwrite sh.flag)
     if (threadIdx.x < kMaxRhs) {
       const int k = threadIdx.x;
       s_ru[k] = 0;
@@ -271,7 +327,6 @@ __global__ void __launch_bounds__(BS, 1) cg_mixed_kernel(MixedArgs a) {
         if (rn > s_rmax[k]) s_rmax[k] = rn;
         if (rn < s_tau[k] || rn < a.delta * s_rmax[k] || s_since[k] >= a.n_ru || !(rn == rn)) {
           s_ru[k] = 1;
-          atomicOr(&s_any_ru, 1);
           s_r2[k] = r2;  // beta is formed from the true residual below
         } else {
           s_beta[k] = r2 / s_rr[k];
@@ -281,50 +336,81 @@ __global__ void __launch_bounds__(BS, 1) cg_mixed_kernel(MixedArgs a) {
       }
     }
     __syncthreads();
-    if (s_any_ru) {
+    if (threadIdx.x == 0) sys_list_from(s_upd, s_ru, a.nrhs);
+    __syncthreads();
+    if (s_upd.n > 0) {
       // C: t = M^T (x + x^) in FP64
-      for (uint32_t i = i0; i < V; i += stride) {
-        const Site s = make_site(g, i);
-        const double smi = sm[i];
+      for_units(NI64, s_upd, [&](int k, uint32_t j) {
+        const RowItem it = make_item<W64>(g, j);
+        double smi[W64];
+        vload<double, W64>(sm + it.own, smi);
+        const double *xk = pick<NR>(a.x, k);
+        const float *xhk = pick<NR>(a.xh, k);
+        double *tk = pick<NR>(a.t64, k);
 #pragma unroll
-        for (int k = 0; k < NR; k++) {
-          if (k >= a.nrhs || !s_ru[k]) continue;
+        for (int c = 0; c < NC; c++) {
+          const size_t off = size_t(c) * V;
+          const double *xv = xk + off;
+          const float *xhv = xhk + off;
+          Nb<double> n[W64];
+          gather_item<double, W64>(
+              it, n,
+              [&](uint32_t i, double(&v)[W64]) {
+                double xx[W64];
+                float hh[W64];
+                vload<double, W64>(xv + i, xx);
+                vload<float, W64>(xhv + i, hh);
 #pragma unroll
-          for (int c = 0; c < NC; c++) {
-            const size_t off = size_t(c) * V;
-            const double *xv = a.x[k] + off;
-            const float *xhv = a.xh[k] + off;
-            const Nb<double> n = gather7<double>(s, i, [&](uint32_t j) { return xv[j] + double(xhv[j]); });
-            a.t64[k][off + i] = apply_Mt<double>(s, smi, n);
-          }
+                for (int e = 0; e < W64; e++) v[e] = xx[e] + double(hh[e]);
+              },
+              [&](uint32_t i) { return xv[i] + double(xhv[i]); });
+          double o[W64];
+          item_Mt<double, W64>(it, smi, n, o);
+          vstore<double, W64>(tk + off + it.own, o);
         }
-      }
-#pragma unroll
-      for (int j = 0; j < 2 * kMaxRhs; j++) acc[j] = 0.0;
+      });
+      zero_acc();
       ok = end_phase<1>(acc, sh, part0, a.bar, nph++, a.err);
       if (!ok) break;
       // D: x += x^, x^ = 0, r = b - M t, r^ = (float) r
+      zero_acc();
+      for_units(NI64, s_upd, [&](int k, uint32_t j) {
+        const RowItem it = make_item<W64>(g, j);
+        double smi[W64];
+        vload<double, W64>(sm + it.own, smi);
+        const double *bk = pick<NR>(a.b, k);
+        const double *tk = pick<NR>(a.t64, k);
+        double *xk = pick<NR>(a.x, k);
+        float *xhk = pick<NR>(a.xh, k);
+        float *rhk = pick<NR>(a.rh, k);
 #pragma unroll
-      for (int j = 0; j < 2 * kMaxRhs; j++) acc[j] = 0.0;
-      for (uint32_t i = i0; i < V; i += stride) {
-        const Site s = make_site(g, i);
-        const double smi = sm[i];
+        for (int c = 0; c < NC; c++) {
+          const size_t off = size_t(c) * V + it.own;
+          double xx[W64], ri[W64];
+          float hh[W64], z32[W64], rf[W64];
+          vload<double, W64>(xk + off, xx);
+          vload<float, W64>(xhk + off, hh);
 #pragma unroll
-        for (int k = 0; k < NR; k++) {
-          if (k >= a.nrhs || !s_ru[k]) continue;
-#pragma unroll
-          for (int c = 0; c < NC; c++) {
-            const size_t off = size_t(c) * V;
-            a.x[k][off + i] = a.x[k][off + i] + double(a.xh[k][off + i]);
-            a.xh[k][off + i] = 0.f;
-            const double *tv = a.t64[k] + off;
-            const Nb<double> n = gather7<double>(s, i, [&](uint32_t j) { return tv[j]; });
-            const double ri = apply_sub_M<double>(s, a.b[k][off + i], smi, n);
-            a.rh[k][off + i] = float(ri);
-            acc[k] += ri * ri;
+          for (int e = 0; e < W64; e++) {
+            xx[e] = xx[e] + double(hh[e]);
+            z32[e] = 0.f;
           }
+          vstore<double, W64>(xk + off, xx);
+          vstore<float, W64>(xhk + off, z32);
+          Nb<double> n[W64];
+          gather_item<double, W64>(it, tk + size_t(c) * V, n);
+          vload<double, W64>(bk + off, ri);
+          item_sub_M<double, W64>(it, smi, n, ri);
+          double sr = 0.0;
+#pragma unroll
+          for (int e = 0; e < W64; e++) {
+            rf[e] = float(ri[e]);
+            sr += ri[e] * ri[e];
+          }
+          acc_add<NR>(acc, k, sr);
+          vstore<float, W64>(rhk + off, rf);
         }
-      }
+      });
       ok = end_phase<NR>(acc, sh, part1, a.bar, nph++, a.err);
       if (!ok) break;
       if (threadIdx.x < kMaxRhs) {
@@ -346,8 +432,10 @@ __global__ void __launch_bounds__(BS, 1) cg_mixed_kernel(MixedArgs a) {
         }
       }
       __syncthreads();
+      if (threadIdx.x == 0) sys_list_from(s_run, s_active, a.nrhs);
+      __syncthreads();
     }
-    if (sh.flag != 0) {  // block 0 saw the host's abort request at the last phase end
+    if (abort_seen != 0) {  // block 0 saw the host's abort request at the end of phase B
       if (threadIdx.x == 0 && blockIdx.x == 0) atomicExch(a.err, 2);
       ok = false;
       break;

@@ -40,10 +40,12 @@ using gn::PhaseBar;
 constexpr int kNoAllocMaxL = 32;
 constexpr size_t kMaxV = size_t(kNoAllocMaxL) * kNoAllocMaxL * kNoAllocMaxL;  // 32768 sites
 constexpr int kMaxBlocks = int((kMaxV + 511) / 512);  // one site per thread at most (blocks of >= 512 threads)
-// the same solver instantiation and block shape as gn_cg_device for one real system
-inline const void *solver_kernel() {
-  return gn::solver_threads() == 768 ? (const void *)gn::cg_kernel<double, 1, 1, 768>
-                                     : (const void *)gn::cg_kernel<double, 1, 1, 512>;
+// the same solver instantiations, block shape and grid rule as gn_cg_device
+// for one real system; w = sites per item (1 or 2)
+constexpr int kThreads = gn::kWideThreads;
+inline const void *solver_kernel(int w) {
+  return w == 2 ? (const void *)gn::cg_kernel<double, 1, 1, kThreads, 2>
+                : (const void *)gn::cg_kernel<double, 1, 1, kThreads, 1>;
 }
 constexpr size_t kVecWords = 4 * kMaxV;                                         // r, p0, p1, t
 constexpr size_t kPartialWords = size_t(2 * (gn::kSyncQ + 1)) * kMaxBlocks;      // 2 slots x (8 sums + flag) per block
@@ -56,7 +58,7 @@ static __device__ __align__(256) double g_noalloc_scratch[kScratchWords];
 constexpr int kMaxDevices = 64;
 struct DeviceSetup {
   double *scratch = nullptr;  // device address of g_noalloc_scratch on this device
-  int capacity = 0;           // co-resident blocks of the solver kernel
+  int capacity[2] = {0, 0};  // co-resident blocks of the solver kernel, 1 and 2 sites per item
 };
 DeviceSetup g_setup[kMaxDevices];
 std::mutex g_setup_mutex;
@@ -100,9 +102,11 @@ extern "C" GN_API int gn_cg_noalloc(int L, const double *sigmamass, const double
       void *p = nullptr;
       const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
       if (e != cudaSuccess || p == nullptr) return err(GN_ERR_CUDA, "gn_cg_noalloc: cudaGetSymbolAddress failed");
-      const int capacity = gn::coop_capacity(solver_kernel(), gn::solver_threads());
-      if (capacity < 1) return err(GN_ERR_CUDA, "gn_cg_noalloc: occupancy query failed");
-      s.capacity = capacity;
+      for (int w = 1; w <= 2; w++) {
+        const int capacity = gn::coop_capacity(solver_kernel(w), kThreads);
+        if (capacity < 1) return err(GN_ERR_CUDA, "gn_cg_noalloc: occupancy query failed");
+        s.capacity[w - 1] = capacity;
+      }
       s.scratch = static_cast<double *>(p);
     }
   }
@@ -140,8 +144,10 @@ extern "C" GN_API int gn_cg_noalloc(int L, const double *sigmamass, const double
   a.err = errflag;
   a.abort_flag = nullptr;
   a.state = state;
-  const int nb = gn::solver_grid(int64_t(V), s.capacity, kMaxBlocks, gn::solver_threads());
-  if (gn::launch_solver(solver_kernel(), nb, gn::solver_threads(), a, st) != cudaSuccess)
+  const void *ptrs[3] = {sigmamass, b, x};
+  const int w = gn::fp64_width(L, ptrs, 3);
+  const int nb = gn::solver_grid(gn::solver_units(int64_t(V), w, 1), s.capacity[w - 1], kMaxBlocks, kThreads);
+  if (gn::launch_solver(solver_kernel(w), nb, kThreads, a, st) != cudaSuccess)
     return err(GN_ERR_CUDA, "gn_cg_noalloc: kernel launch failed");
 
   // ---- outcome (into host stack memory; no allocation)

@@ -1,7 +1,7 @@
 // ops_kernels.cuh -- the non-solver kernels of the sigma-HMC path.  Each one is
 // a single sweep over the V sites (grid-stride), HBM-bound.
 #pragma once
-#include "device_common.cuh"
+#include "rowvec.cuh"
 
 namespace gn {
 
@@ -9,101 +9,38 @@ constexpr int kOpThreads = 256;
 
 // Dirac apply on ncomp planes: op 0 = M, 1 = M^T, 2 = out -= M in.
 // Algorithmic traffic 3 words per site and plane (in, sm, out; +1 read for op 2).
-// One site per thread and a grid covering every site (blockIdx.y = plane), no
+// One item of W sites per thread (rowvec.cuh: W = 2 with 128-bit loads when
+// L/2 is even), a grid covering every item (blockIdx.y = plane) and no
 // grid-stride loop: few registers, so all 2048 thread slots of an SM are
 // filled and the hardware streams blocks in as others finish -- the stencil's
-// seven loads per site need that many requests in flight to cover the memory
-// latency.
-template <typename T, int OP>
-__global__ void __launch_bounds__(kOpThreads) dirac_kernel(Geom g, const T *__restrict__ sm, const T *__restrict__ in,
-                                                          T *__restrict__ out) {
-  const uint32_t V = uint32_t(g.V);
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= V) return;
-  const T *pv = in + size_t(blockIdx.y) * V;
-  T *ov = out + size_t(blockIdx.y) * V;
-  const Site s = make_site(g, i);
-  const T smi = __ldg(sm + i);
-  const Nb<T> n = gather7<T>(s, i, [&](uint32_t j) { return __ldg(pv + j); });
-  if (OP == 0) ov[i] = apply_M<T>(s, smi, n);
-  else if (OP == 1) ov[i] = apply_Mt<T>(s, smi, n);
-  else ov[i] = apply_sub_M<T>(s, ov[i], smi, n);
-}
-
-// The same apply two sites at a time with 128-bit loads, for L a multiple of
-// 4 (L/2 even).  A thread takes the sites (k, k+1), k even, of one parity row:
-// their x0 +- 1 and x1 +- 1 neighbours are the pairs (k, k+1) of rows a plane
-// or a row away in the other half, 16-byte aligned; their time neighbours are
-// the pair (k, k+1) of the same row of the other half plus one more value,
-// k-1 or k+2.  With b = (parity + x0 + x1) & 1 the site k sits at x2 = 2k + b:
-//   b = 0:  up(k) = q[k], dn(k) = q[k-1], up(k+1) = q[k+1], dn(k+1) = q[k]
-//   b = 1:  up(k) = q[k+1], dn(k) = q[k], up(k+1) = q[k+2], dn(k+1) = q[k+1]
-// (indices mod L/2); the antiperiodic sign can only fall on dn(k) at x2 = 0
-// (b = 0, k = 0) or on up(k+1) at x2 = L-1 (b = 1, k = L/2-2).  Every site is
-// computed with the same operation order as dirac_kernel.
-template <int OP>
-__global__ void __launch_bounds__(kOpThreads) dirac_pair_kernel(Geom g, const double *__restrict__ sm,
+// seven loads per item need that many requests in flight to cover the memory
+// latency.  Items run in row order with both parities of a row together, so
+// each value of `in` comes from DRAM once although it is read as a centre and
+// as a neighbour.
+template <int W, int OP>
+__global__ void __launch_bounds__(kOpThreads) dirac_item_kernel(Geom g, const double *__restrict__ sm,
                                                                const double *__restrict__ in,
                                                                double *__restrict__ out) {
-  const uint32_t V = uint32_t(g.V), half = uint32_t(g.half), quarter = half / 2u;
-  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= half) return;
+  const uint32_t V = uint32_t(g.V);
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= row_items<W>(g)) return;
   const double *pv = in + size_t(blockIdx.y) * V;
   double *ov = out + size_t(blockIdx.y) * V;
-  const uint32_t par = t >= quarter ? 1u : 0u;
-  const uint32_t h = 2u * (t - par * quarter);  // even half index: the pair (h, h+1)
-  const uint32_t row = fdiv(h, g.div_Lh);
-  const uint32_t k = h - row * uint32_t(g.Lh);
-  const uint32_t x0 = fdiv(row, g.div_L);
-  const uint32_t x1 = row - x0 * uint32_t(g.L);
-  const uint32_t L = uint32_t(g.L), Lh = uint32_t(g.Lh), P = uint32_t(g.plane);
-  const uint32_t b = (par + x0 + x1) & 1u;
-  const uint32_t own = par * half + h, qb = (1u - par) * half;
-  const double2 psi = __ldg(reinterpret_cast<const double2 *>(pv + own));
-  const double2 smv = __ldg(reinterpret_cast<const double2 *>(sm + own));
-  const double2 u0 = __ldg(reinterpret_cast<const double2 *>(pv + qb + ((x0 + 1u == L) ? h - (L - 1u) * P : h + P)));
-  const double2 d0 = __ldg(reinterpret_cast<const double2 *>(pv + qb + ((x0 == 0u) ? h + (L - 1u) * P : h - P)));
-  const double2 u1 = __ldg(reinterpret_cast<const double2 *>(pv + qb + ((x1 + 1u == L) ? h - (L - 1u) * Lh : h + Lh)));
-  const double2 d1 = __ldg(reinterpret_cast<const double2 *>(pv + qb + ((x1 == 0u) ? h + (L - 1u) * Lh : h - Lh)));
-  const double2 tq = __ldg(reinterpret_cast<const double2 *>(pv + qb + h));
-  // the extra time value: k-1 (b = 0) or k+2 (b = 1), wrapping within the row
-  const uint32_t rb = qb + row * Lh;
-  const uint32_t ke = b ? ((k + 2u == Lh) ? 0u : k + 2u) : ((k == 0u) ? Lh - 1u : k - 1u);
-  const double te = __ldg(pv + rb + ke);
-  const uint32_t e1 = x0 & 1u, e2 = (x0 + x1) & 1u;
-  // sign bits as in Site::neg: bits 0..2 forward, 3..5 backward
-  uint32_t negA = (e1 << 1) | (e2 << 2) | (e1 << 4) | (e2 << 5);
-  uint32_t negB = negA;
-  if (b == 0u && k == 0u) negA ^= 1u << 5;        // dn(k) at x2 = 0
-  if (b == 1u && k + 2u == Lh) negB ^= 1u << 2;   // up(k+1) at x2 = L-1
-  Site sA, sB;
-  sA.neg = negA;
-  sB.neg = negB;
-  Nb<double> A, B;
-  A.c = psi.x;
-  B.c = psi.y;
-  A.up[0] = u0.x; B.up[0] = u0.y;
-  A.dn[0] = d0.x; B.dn[0] = d0.y;
-  A.up[1] = u1.x; B.up[1] = u1.y;
-  A.dn[1] = d1.x; B.dn[1] = d1.y;
-  if (b == 0u) {
-    A.up[2] = tq.x; A.dn[2] = te; B.up[2] = tq.y; B.dn[2] = tq.x;
-  } else {
-    A.up[2] = tq.y; A.dn[2] = tq.x; B.up[2] = te; B.dn[2] = tq.y;
-  }
-  double2 o;
+  const RowItem it = make_item<W>(g, j);
+  Nb<double> n[W];
+  gather_item<double, W>(
+      it, n, [&](uint32_t i, double(&v)[W]) { vload<double, W>(pv + i, v); }, [&](uint32_t i) { return __ldg(pv + i); });
+  double smv[W], o[W];
+  vload<double, W>(sm + it.own, smv);
   if (OP == 0) {
-    o.x = apply_M<double>(sA, smv.x, A);
-    o.y = apply_M<double>(sB, smv.y, B);
+    item_M<double, W>(it, smv, n, o);
   } else if (OP == 1) {
-    o.x = apply_Mt<double>(sA, smv.x, A);
-    o.y = apply_Mt<double>(sB, smv.y, B);
+    item_Mt<double, W>(it, smv, n, o);
   } else {
-    const double2 prev = *reinterpret_cast<const double2 *>(ov + own);
-    o.x = apply_sub_M<double>(sA, prev.x, smv.x, A);
-    o.y = apply_sub_M<double>(sB, prev.y, smv.y, B);
+    vload<double, W>(ov + it.own, o);
+    item_sub_M<double, W>(it, smv, n, o);
   }
-  *reinterpret_cast<double2 *>(ov + own) = o;
+  vstore<double, W>(ov + it.own, o);
 }
 
 // sigma mass (sigma.c:75-94): sm(x) = 1/8 sum of sigma over the 8 dual sites

@@ -107,6 +107,13 @@ class Clocks:
         self.device = device
         self.proc = None
         self.path = None
+        self.offset = 0
+
+    def mark(self):
+        """Only samples written after this call are reported (the timed region's)."""
+        if self.proc is not None:
+            self.fh.flush()
+            self.offset = os.path.getsize(self.path)
 
     def start(self):
         try:
@@ -116,6 +123,11 @@ class Clocks:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                                           "-i", str(self.device), "-lms", "200"], stdout=self.fh,
                                          stderr=subprocess.DEVNULL)
+            # wait for the first sample: the sampler's start-up (NVML initialisation)
+            # must not fall inside a timed region
+            t0 = time.perf_counter()
+            while time.perf_counter() - t0 < 5.0 and os.path.getsize(self.path) == 0:
+                time.sleep(0.05)
         except Exception:
             self.proc = None
 
@@ -130,7 +142,10 @@ class Clocks:
         self.fh.close()
         sm, smax, reasons, power = [], [], set(), []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in open(self.path):
+        with open(self.path) as fh:
+            fh.seek(self.offset)
+            lines = fh.read().splitlines()
+        for ln in lines:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -286,14 +301,15 @@ def run_ours(a, world, rank, local):
 
     results = {}
     for prec, name in ((G.GN_PREC_MIXED, "mixed"), (G.GN_PREC_FP64, "fp64")):
+        clocks = Clocks(local)
+        clocks.start()  # sampling from before the warm-up to the end of the timed steps
         lat.load_sigma(sigma0)
         for s in range(a.warmup):
             traj_dev(s, prec)
         l0 = lat.launch_count()
         dist_barrier(world)
         torch.cuda.synchronize(dev)
-        clocks = Clocks(local)
-        clocks.start()
+        clocks.mark()
         e0, e1 = cuda_events()
         e0.record(stream)
         out = []
@@ -438,7 +454,7 @@ def dirac_roofline(G, stream, dev, reps=20, L=256):
     ms = min(times)
     nbytes = 3 * 8 * V
     lat.close()
-    return {"gbs": nbytes / (ms * 1e-3) / 1e9, "kernel": f"dirac_pair_kernel<M> L={L} (inputs 3x L2)", "ms": ms,
+    return {"gbs": nbytes / (ms * 1e-3) / 1e9, "kernel": f"dirac_item_kernel<2, M> L={L} (inputs 3x L2)", "ms": ms,
             "bytes": nbytes, "traffic": None,
             "note": f"{ms * 1e3:.1f} us per launch, {reps} back-to-back launches on 384 MB (> L2)"}
 
