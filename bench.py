@@ -47,6 +47,10 @@ for _p in (str(ROOT), str(PKG)):
 L_DEFAULT = 64
 BETA_S = 0.85
 NFLAV = 4
+# DRAM bytes per launch measured with ncu (one capture each; summaries under
+# profiles/): the dominant solver kernel at L = 64 and the Dirac apply at L = 256.
+CG_MIXED_DRAM_BYTES = 6_564_352      # 6.391 MB read + 0.173 MB written
+DIRAC256_DRAM_BYTES = 379_232_256    # 269.540 MB read + 109.692 MB written
 METRIC = "HMC trajectories/s at L=64 (LFMN2VF, 10 x eps 0.05, CG to 1e-10 true relative residual)"
 UNIT = "traj/s"
 
@@ -402,8 +406,15 @@ def roof_json(r, peaks):
 
 def kernel_roofline(lat, stream, a, G):
     """Persistent CG kernel, mixed precision, 2 flavours, b = the resident phi,
-    x = 0, tol 1e-10 relative.  Algorithmic bytes per site: inner iteration
-    8 + 40 nrhs, reliable update 80 per system, start 40 per system."""
+    x = 0, tol 1e-10 relative.  Algorithmic bytes per site (each vector read or
+    written once per phase; FP32 words of 4 B, FP64 of 8 B):
+      inner iteration  8 + 44 nrhs  (sm twice; A: r, t, p in, p, t out;
+                                     B: t, p, x^, r in, x^, r out)
+      reliable update  72 per system (C: x, x^ in, t out; D: x, x^, t, b in,
+                                      x, x^, r^ out; sm shared)
+      start            12 + 28 nrhs (b in; x, x^, r^, p^ out; sm in, sm32 out)
+    DRAM traffic per launch from ncu (--case cg64, dram__bytes_read.sum +
+    dram__bytes_write.sum of cg_mixed_kernel): the working set stays in L2."""
     V = lat.V
     sm = lat.field_ptr(G.GN_F_SM)
     phi = lat.field_ptr(G.GN_F_PHI)
@@ -421,9 +432,9 @@ def kernel_roofline(lat, stream, a, G):
     ms = statistics.median(times)
     inner = max(i["inner_iterations"] for i in infos)
     ru = sum(i["reliable_updates"] for i in infos)
-    nbytes = V * ((8 + 40 * 2) * inner + 80 * ru + 40 * 2)
-    return {"gbs": nbytes / (ms * 1e-3) / 1e9, "kernel": "cg_mixed_kernel<1> (2 flavours, L=%d)" % lat.L,
-            "ms": ms, "bytes": nbytes, "traffic": None,
+    nbytes = V * ((8 + 44 * 2) * inner + 72 * ru + 12 + 28 * 2)
+    return {"gbs": nbytes / (ms * 1e-3) / 1e9, "kernel": "cg_mixed_kernel<1, 2, 1024, 4> (2 flavours, L=%d)" % lat.L,
+            "ms": ms, "bytes": nbytes, "traffic": CG_MIXED_DRAM_BYTES if lat.L == 64 else None,
             "note": f"{inner} inner iterations, {ru} reliable updates, {ms:.3f} ms per launch; working set "
                     f"{(2 * 5 * 4 + 8 * 3) * V / 1e6:.0f} MB is L2-resident within the solve"}
 
@@ -432,7 +443,8 @@ def dirac_roofline(G, stream, dev, reps=20, L=256):
     """Dirac M on one FP64 plane at L = 256 (V = 16,777,216): psi, sm and the
     output are 384 MB, three times the L2, so back-to-back launches run from
     HBM (no flush needed); `reps` launches between two CUDA events.
-    Algorithmic bytes 3 * 8 * V per launch (psi, sm in; out)."""
+    Algorithmic bytes 3 * 8 * V per launch (psi, sm in; out).  DRAM traffic per
+    launch from ncu (--case dirac256, dram__bytes_read.sum + dram__bytes_write.sum)."""
     import torch
     lat = G.Lattice(L, dev.index)
     V = L ** 3
@@ -455,7 +467,7 @@ def dirac_roofline(G, stream, dev, reps=20, L=256):
     nbytes = 3 * 8 * V
     lat.close()
     return {"gbs": nbytes / (ms * 1e-3) / 1e9, "kernel": f"dirac_item_kernel<2, M> L={L} (inputs 3x L2)", "ms": ms,
-            "bytes": nbytes, "traffic": None,
+            "bytes": nbytes, "traffic": DIRAC256_DRAM_BYTES if L == 256 else None,
             "note": f"{ms * 1e3:.1f} us per launch, {reps} back-to-back launches on 384 MB (> L2)"}
 
 
