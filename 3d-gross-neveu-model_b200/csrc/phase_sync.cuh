@@ -7,9 +7,11 @@
 // arriving on the barrier word adds about 8 ns (arrivals serialise on one
 // address).  So: only the quantities a phase needs are reduced, with one block
 // barrier; the grid barrier is a 64-bit monotonic arrival counter written with
-// red.release and polled with ld.acquire (no separate fences); and the solvers
-// run few, large blocks.  Every order is fixed, so all blocks compute the same
-// totals bit for bit.
+// red.release, polled with relaxed loads and followed by one acquire fence;
+// and the solvers run few, large blocks.  Every order is fixed, so all blocks
+// compute the same totals bit for bit.  The barrier and the totals are two
+// calls, so that a solver can start the next phase's stencil loads before it
+// reads the other blocks' partial sums.
 #pragma once
 #include "device_common.cuh"
 
@@ -42,15 +44,16 @@ struct SyncShared {
   int flag;                 // block 0's flag word of the last phase
 };
 
-// End of phase number `phase` (counted from 0 in every block alike).  acc[]
-// holds this thread's contributions to NQ quantities; on return sh.val[0..NQ)
-// holds the grid totals in every block, and sh.flag the word block 0 put in
-// `flag` (the same value in every block).  Returns false if this block's wait
-// timed out (it then sets *err; the other blocks time out at their next wait).
-// part_slot: [NQ][gridDim.x] partials followed by one flag word.
+// End of phase number `phase` (counted from 0 in every block alike), first
+// half: publishes this block's partial sums of NQ quantities (acc[]) and the
+// flag word, and waits until every block has done the same.  The grid's
+// writes of the phase are visible to this block on return.  Returns false if
+// this block's wait timed out (it then sets *err; the other blocks time out at
+// their next wait).  part_slot: [NQ][gridDim.x] partials followed by one flag
+// word.
 template <int NQ>
-__device__ __forceinline__ bool end_phase(double (&acc)[kSyncQ], SyncShared &sh, double *part_slot, PhaseBar *bar,
-                                          unsigned long long phase, int *err, int flag = 0) {
+__device__ __forceinline__ bool phase_arrive_wait(double (&acc)[kSyncQ], SyncShared &sh, double *part_slot,
+                                                  PhaseBar *bar, unsigned long long phase, int *err, int flag = 0) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
   for (int q = 0; q < NQ; q++) {
@@ -85,7 +88,16 @@ __device__ __forceinline__ bool end_phase(double (&acc)[kSyncQ], SyncShared &sh,
     }
   }
   __syncthreads();
-  // grid totals, summed by every block in the same order
+  return sh.ok != 0;
+}
+
+// Second half: the grid totals into sh.val[0..NQ) and block 0's flag word into
+// sh.flag, summed by every block in the same order (so every block holds the
+// same bits).  Any work that does not need the totals may run between the two
+// halves: the partials' round trip then overlaps it.
+template <int NQ>
+__device__ __forceinline__ void phase_totals(SyncShared &sh, const double *part_slot) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   if (w < NQ) {
     const double *p = part_slot + size_t(w) * gridDim.x;
     double s = 0.0;
@@ -96,7 +108,16 @@ __device__ __forceinline__ bool end_phase(double (&acc)[kSyncQ], SyncShared &sh,
     sh.flag = reinterpret_cast<const int *>(part_slot + size_t(NQ) * gridDim.x)[0];
   }
   __syncthreads();
-  return sh.ok != 0;
+}
+
+// Both halves: on return sh.val[0..NQ) holds the grid totals in every block and
+// sh.flag the word block 0 put in `flag`.
+template <int NQ>
+__device__ __forceinline__ bool end_phase(double (&acc)[kSyncQ], SyncShared &sh, double *part_slot, PhaseBar *bar,
+                                          unsigned long long phase, int *err, int flag = 0) {
+  const bool ok = phase_arrive_wait<NQ>(acc, sh, part_slot, bar, phase, err, flag);
+  phase_totals<NQ>(sh, part_slot);
+  return ok;
 }
 
 }  // namespace gn
