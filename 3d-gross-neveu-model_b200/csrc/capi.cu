@@ -59,6 +59,8 @@ void fill_info(const gn::SolveInfo &s, gn_cg_info *o) {
 
 }  // namespace
 
+int gn::set_last_error(int status, const char *msg) { return fail(status, msg); }
+
 extern "C" {
 
 const char *gn_last_error(void) { return g_last_error.c_str(); }

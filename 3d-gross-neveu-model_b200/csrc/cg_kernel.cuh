@@ -61,7 +61,7 @@ struct CgArgs {
   int rel;      // 0: stop at |r| < tol; 1: stop at |r| < tol |b|
   double tol;
   long long max_iter;
-  double *partials;  // [2 slots][kSyncQ][gridDim.x]
+  double *partials;  // [2 banks][kSyncQ + 1][gridDim.x]
   PhaseBar *bar;
   int *err;
   const int *abort_flag;  // host-mapped; nonzero asks the kernel to stop
@@ -83,13 +83,13 @@ __device__ __forceinline__ void sys_list_from(SysList &sl, const int *flag, int 
   sl.n = n;
 }
 
-// f(k, j) for every (system k of the list, item j < NI): the items of one
-// system are contiguous in the unit numbering, so a warp reads contiguous
-// vectors of one system.
+// f(k, j) for every (system k of the list, item j < NI), spread over the
+// team's threads: the items of one system are contiguous in the unit
+// numbering, so a warp reads contiguous vectors of one system.
 template <typename F>
-__device__ __forceinline__ void for_units(uint32_t NI, const SysList &sl, F f) {
+__device__ __forceinline__ void for_units(uint32_t NI, const SysList &sl, const Team &t, F f) {
   const uint32_t total = uint32_t(sl.n) * NI;
-  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < total; u += gridDim.x * blockDim.x) {
+  for (uint32_t u = t.tid; u < total; u += t.nthreads) {
     uint32_t j = u;
     int ka = 0;
     while (j >= NI) {
@@ -132,9 +132,7 @@ __global__ void __launch_bounds__(BS, 1) cg_kernel(CgArgs<T> a) {
   const Geom g = a.g;
   const uint32_t V = uint32_t(g.V);
   const uint32_t NI = row_items<W>(g);
-  double *part0 = a.partials;
-  double *part1 = a.partials + size_t(kSyncQ + 1) * gridDim.x;
-  unsigned long long nph = 0;  // phases ended so far (same count in every block)
+  Team team = grid_team(a.bar, a.partials, a.err);
   const T *__restrict__ sm = a.sm;
 
   if (threadIdx.x < kMaxRhs) {
@@ -162,7 +160,7 @@ __global__ void __launch_bounds__(BS, 1) cg_kernel(CgArgs<T> a) {
   // ---------------------------------------------------------------- start
   if (a.variant == 0) {
     // t = M^T x_in
-    for_units(NI, s_every, [&](int k, uint32_t j) {
+    for_units(NI, s_every, team, [&](int k, uint32_t j) {
       const RowItem it = make_item<W>(g, j);
       T smi[W];
       vload<T, W>(sm + it.own, smi);
@@ -178,11 +176,11 @@ __global__ void __launch_bounds__(BS, 1) cg_kernel(CgArgs<T> a) {
       }
     });
     zero_acc();
-    ok = end_phase<1>(acc, sh, part1, a.bar, nph++, a.err);
+    ok = end_phase<1>(acc, sh, team);
     // r = b - M t ; sums r^2 and b^2
     zero_acc();
     if (ok) {
-      for_units(NI, s_every, [&](int k, uint32_t j) {
+      for_units(NI, s_every, team, [&](int k, uint32_t j) {
         const RowItem it = make_item<W>(g, j);
         T smi[W];
         vload<T, W>(sm + it.own, smi);
@@ -211,7 +209,7 @@ __global__ void __launch_bounds__(BS, 1) cg_kernel(CgArgs<T> a) {
         }
       });
     }
-    ok = end_phase<2 * NR>(acc, sh, part0, a.bar, nph++, a.err) && ok;
+    ok = end_phase<2 * NR>(acc, sh, team) && ok;
     if (threadIdx.x < kMaxRhs) {
       const int k = threadIdx.x;
       if (k < a.nrhs) {
@@ -232,7 +230,7 @@ __global__ void __launch_bounds__(BS, 1) cg_kernel(CgArgs<T> a) {
   // x = 0, r = b, p = b ; rr = sum b^2
   zero_acc();
   if (ok) {
-    for_units(NI, s_run, [&](int k, uint32_t j) {
+    for_units(NI, s_run, team, [&](int k, uint32_t j) {
       const uint32_t own = make_item<W>(g, j).own;
       const T *bk = pick<NR>(a.b, k);
       T *xk = pick<NR>(a.x, k);
@@ -256,7 +254,7 @@ __global__ void __launch_bounds__(BS, 1) cg_kernel(CgArgs<T> a) {
       }
     });
   }
-  ok = end_phase<NR>(acc, sh, part1, a.bar, nph++, a.err) && ok;
+  ok = end_phase<NR>(acc, sh, team) && ok;
   if (threadIdx.x < kMaxRhs) {
     const int k = threadIdx.x;
     if (k < a.nrhs && s_active[k]) {
@@ -288,7 +286,7 @@ __global__ void __launch_bounds__(BS, 1) cg_kernel(CgArgs<T> a) {
     const bool odd = (it & 1) != 0;
     // phase A: p = r + beta p_old (it > 0), t = M^T p, sum t^2
     zero_acc();
-    for_units(NI, s_run, [&](int k, uint32_t j) {
+    for_units(NI, s_run, team, [&](int k, uint32_t j) {
       const RowItem ri = make_item<W>(g, j);
       T smi[W];
       vload<T, W>(sm + ri.own, smi);
@@ -330,7 +328,7 @@ __global__ void __launch_bounds__(BS, 1) cg_kernel(CgArgs<T> a) {
         acc_add<NR>(acc, k, st);
       }
     });
-    ok = end_phase<NR>(acc, sh, part0, a.bar, nph++, a.err);
+    ok = end_phase<NR>(acc, sh, team);
     if (!ok) break;
     if (threadIdx.x < kMaxRhs) {
       const int k = threadIdx.x;
@@ -339,7 +337,7 @@ __global__ void __launch_bounds__(BS, 1) cg_kernel(CgArgs<T> a) {
     __syncthreads();
     // phase B: Ap = M t, x += alpha p, r -= alpha Ap, sum r^2
     zero_acc();
-    for_units(NI, s_run, [&](int k, uint32_t j) {
+    for_units(NI, s_run, team, [&](int k, uint32_t j) {
       const RowItem ri = make_item<W>(g, j);
       T smi[W];
       vload<T, W>(sm + ri.own, smi);
@@ -371,7 +369,7 @@ __global__ void __launch_bounds__(BS, 1) cg_kernel(CgArgs<T> a) {
         vstore<T, W>(rk + off + ri.own, rv);
       }
     });
-    ok = end_phase<NR>(acc, sh, part1, a.bar, nph++, a.err, abort_req);
+    ok = end_phase<NR>(acc, sh, team, abort_req);
     if (!ok) break;
     if (threadIdx.x < kMaxRhs) {
       const int k = threadIdx.x;

@@ -7,6 +7,7 @@
 #include <stdexcept>
 
 #include "engine.h"
+#include "schedule.h"
 #include "errors.h"
 #include "launch.h"
 #include "ops_kernels.cuh"
@@ -276,47 +277,6 @@ int Engine::finish_solve(int nrhs, SolveInfo *info) {
 }
 
 // ------------------------------------------------------------------ trajectory
-// Integrator schedules (moleculardynamics.c:859-1005, :1018-1221, :1234-1434)
-// as op lists: F force (medium / high tolerance), P momentum step, Q sigma
-// step, S X0-imposed solve at high tolerance.
-enum { OP_F_MED = 1, OP_F_HIGH, OP_P, OP_Q, OP_S_HIGH };
-struct Op {
-  int op;
-  double c;
-};
-
-static std::vector<Op> schedule(int integrator, double eps, int step) {
-  std::vector<Op> v;
-  const double lam = 0.1931833275037836;  // MAGIC_LAMBDA, macro.h:169
-  auto push = [&](int o, double c) { v.push_back({o, c}); };
-  if (integrator == GN_LFMN2VF) {
-    push(OP_F_MED, 0); push(OP_P, lam * eps); push(OP_Q, eps / 2.0);
-    push(OP_F_MED, 0); push(OP_P, (1.0 - (2.0 * lam)) * eps); push(OP_Q, eps / 2.0);
-    for (int s = 1; s < step - 1; s++) {
-      push(OP_F_MED, 0); push(OP_P, 2.0 * lam * eps); push(OP_Q, eps / 2.0);
-      push(OP_F_MED, 0); push(OP_P, (1.0 - (2.0 * lam)) * eps); push(OP_Q, eps / 2.0);
-    }
-    push(OP_F_MED, 0); push(OP_P, 2.0 * lam * eps); push(OP_Q, eps / 2.0);
-    push(OP_F_MED, 0); push(OP_P, (1.0 - (2.0 * lam)) * eps); push(OP_Q, eps / 2.0);
-    push(OP_F_HIGH, 0); push(OP_P, lam * eps);
-  } else if (integrator == GN_LF2) {
-    push(OP_F_MED, 0); push(OP_P, eps / 2.0);
-    for (int s = 0; s < step - 1; s++) { push(OP_Q, eps); push(OP_F_MED, 0); push(OP_P, eps); }
-    push(OP_Q, eps); push(OP_F_HIGH, 0); push(OP_P, eps / 2.0);
-  } else {
-    push(OP_Q, lam * eps); push(OP_F_MED, 0); push(OP_P, eps / 2.0);
-    push(OP_Q, (1.0 - (2.0 * lam)) * eps); push(OP_F_MED, 0); push(OP_P, eps / 2.0);
-    for (int s = 1; s < step - 1; s++) {
-      push(OP_Q, 2.0 * lam * eps); push(OP_F_MED, 0); push(OP_P, eps / 2.0);
-      push(OP_Q, (1.0 - (2.0 * lam)) * eps); push(OP_F_MED, 0); push(OP_P, eps / 2.0);
-    }
-    push(OP_Q, 2.0 * lam * eps); push(OP_F_MED, 0); push(OP_P, eps / 2.0);
-    push(OP_Q, (1 - (2.0 * lam)) * eps); push(OP_F_MED, 0); push(OP_P, eps / 2.0);
-    push(OP_Q, lam * eps); push(OP_S_HIGH, 0);
-  }
-  return v;
-}
-
 // kit->iterations / kit->CG_call bookkeeping of a flavour loop that stops at
 // the first failure (moleculardynamics.c:593-597).
 static void count_flavours(const SolveInfo *info, int n, double &iters, long long &calls, long long &inner,

@@ -11,4 +11,7 @@ struct GnError : std::runtime_error {
   GnError(int s, const std::string &m) : std::runtime_error(m), status(s) {}
 };
 
+// Records the message gn_last_error() returns (thread-local) and returns status.
+int set_last_error(int status, const char *msg);
+
 }  // namespace gn

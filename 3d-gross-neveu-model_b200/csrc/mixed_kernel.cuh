@@ -52,24 +52,30 @@ struct MixedArgs {
   CgState *state;
 };
 
-template <int NC, int NR, int BS, int W>
-__global__ void __launch_bounds__(BS, 1) cg_mixed_kernel(MixedArgs a) {
+// Block-shared state of one solve (the same values in every block of the team).
+struct MixedShared {
+  double alpha[kMaxRhs], beta[kMaxRhs], rr[kMaxRhs], tau[kMaxRhs], rmax[kMaxRhs], r2[kMaxRhs], b2[kMaxRhs];
+  int active[kMaxRhs], status[kMaxRhs], ru[kMaxRhs], since[kMaxRhs], nru[kMaxRhs], all[kMaxRhs];
+  long long iters[kMaxRhs];
+  SysList run, every, upd;  // systems iterating / all systems / taking a reliable update
+};
+
+// One mixed-precision solve by a team (all its threads call it; a.bar,
+// a.partials and a.err are not used: the team's own are).
+template <int NC, int NR, int W>
+__device__ __forceinline__ void mixed_solve(const MixedArgs &a, Team &team, SyncShared &sh, MixedShared &ms) {
   constexpr int W64 = W >= 2 ? 2 : 1;
-  __shared__ SyncShared sh;
   double *const s_val = sh.val;
-  __shared__ double s_alpha[kMaxRhs], s_beta[kMaxRhs], s_rr[kMaxRhs], s_tau[kMaxRhs], s_rmax[kMaxRhs];
-  __shared__ double s_r2[kMaxRhs], s_b2[kMaxRhs];
-  __shared__ int s_active[kMaxRhs], s_status[kMaxRhs], s_ru[kMaxRhs], s_since[kMaxRhs], s_nru[kMaxRhs];
-  __shared__ int s_all[kMaxRhs];
-  __shared__ long long s_iters[kMaxRhs];
-  __shared__ SysList s_run, s_every, s_upd;  // iterating / all / taking a reliable update
+  double *const s_alpha = ms.alpha, *const s_beta = ms.beta, *const s_rr = ms.rr, *const s_tau = ms.tau;
+  double *const s_rmax = ms.rmax, *const s_r2 = ms.r2, *const s_b2 = ms.b2;
+  int *const s_active = ms.active, *const s_status = ms.status, *const s_ru = ms.ru, *const s_since = ms.since;
+  int *const s_nru = ms.nru, *const s_all = ms.all;
+  long long *const s_iters = ms.iters;
+  SysList &s_run = ms.run, &s_every = ms.every, &s_upd = ms.upd;
 
   const Geom g = a.g;
   const uint32_t V = uint32_t(g.V);
   const uint32_t NI = row_items<W>(g), NI64 = row_items<W64>(g);
-  double *part0 = a.partials;
-  double *part1 = a.partials + size_t(kSyncQ + 1) * gridDim.x;
-  unsigned long long nph = 0;  // phases ended so far (same count in every block)
   const double *__restrict__ sm = a.sm;
 
   if (threadIdx.x < kMaxRhs) {
@@ -99,7 +105,7 @@ __global__ void __launch_bounds__(BS, 1) cg_mixed_kernel(MixedArgs a) {
 
   // ---------------------------------------------------------------- start (FP64)
   if (a.variant == 0) {
-    for_units(NI64, s_every, [&](int k, uint32_t j) {
+    for_units(NI64, s_every, team, [&](int k, uint32_t j) {
       const RowItem it = make_item<W64>(g, j);
       double smi[W64];
       vload<double, W64>(sm + it.own, smi);
@@ -115,10 +121,10 @@ __global__ void __launch_bounds__(BS, 1) cg_mixed_kernel(MixedArgs a) {
       }
     });
     zero_acc();
-    ok = end_phase<1>(acc, sh, part1, a.bar, nph++, a.err);
+    ok = end_phase<1>(acc, sh, team);
     zero_acc();
     if (ok) {
-      for_units(NI64, s_every, [&](int k, uint32_t j) {
+      for_units(NI64, s_every, team, [&](int k, uint32_t j) {
         const RowItem it = make_item<W64>(g, j);
         double smi[W64];
         vload<double, W64>(sm + it.own, smi);
@@ -144,7 +150,7 @@ __global__ void __launch_bounds__(BS, 1) cg_mixed_kernel(MixedArgs a) {
         }
       });
     }
-    ok = end_phase<2 * NR>(acc, sh, part0, a.bar, nph++, a.err) && ok;
+    ok = end_phase<2 * NR>(acc, sh, team) && ok;
     if (threadIdx.x < kMaxRhs) {
       const int k = threadIdx.x;
       if (k < a.nrhs) {
@@ -165,7 +171,7 @@ __global__ void __launch_bounds__(BS, 1) cg_mixed_kernel(MixedArgs a) {
   // x = 0, x^ = 0, r^ = p^ = (float) b, sm32 = (float) sm ; sums r^2 (FP32 values), b^2
   zero_acc();
   if (ok) {
-    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < NI64; j += gridDim.x * blockDim.x) {
+    for (uint32_t j = team.tid; j < NI64; j += team.nthreads) {
       const uint32_t own = make_item<W64>(g, j).own;
       double s64[W64];
       float s32[W64];
@@ -174,7 +180,7 @@ __global__ void __launch_bounds__(BS, 1) cg_mixed_kernel(MixedArgs a) {
       for (int e = 0; e < W64; e++) s32[e] = float(s64[e]);
       vstore<float, W64>(a.sm32 + own, s32);
     }
-    for_units(NI64, s_run, [&](int k, uint32_t j) {
+    for_units(NI64, s_run, team, [&](int k, uint32_t j) {
       const uint32_t own = make_item<W64>(g, j).own;
       const double *bk = pick<NR>(a.b, k);
       double *xk = pick<NR>(a.x, k);
@@ -205,7 +211,7 @@ __global__ void __launch_bounds__(BS, 1) cg_mixed_kernel(MixedArgs a) {
       }
     });
   }
-  ok = end_phase<2 * NR>(acc, sh, part1, a.bar, nph++, a.err) && ok;
+  ok = end_phase<2 * NR>(acc, sh, team) && ok;
   if (threadIdx.x < kMaxRhs) {
     const int k = threadIdx.x;
     if (k < a.nrhs && s_active[k]) {
@@ -233,12 +239,12 @@ __global__ void __launch_bounds__(BS, 1) cg_mixed_kernel(MixedArgs a) {
     // the host's abort request lives in mapped host memory: one thread reads it
     // every 16 iterations, and the value is only used at the end of phase B
     int abort_req = 0;
-    if (blockIdx.x == 0 && threadIdx.x == 0 && a.abort_flag != nullptr && (it & 15) == 0)
+    if (team.brank == 0 && threadIdx.x == 0 && a.abort_flag != nullptr && (it & 15) == 0)
       abort_req = *(volatile const int *)a.abort_flag;
     // A: p^ = r^ + beta p^, t^ = M^T p^ = M^T r^ + beta t^ (linearity: only r^
     // is gathered; p^ and t^ are updated in place at the unit's own sites)
     zero_acc();
-    for_units(NI, s_run, [&](int k, uint32_t j) {
+    for_units(NI, s_run, team, [&](int k, uint32_t j) {
       const RowItem ri = make_item<W>(g, j);
       float smi[W];
       vload<float, W>(a.sm32 + ri.own, smi);
@@ -274,7 +280,7 @@ __global__ void __launch_bounds__(BS, 1) cg_mixed_kernel(MixedArgs a) {
         acc_add<NR>(acc, k, st);
       }
     });
-    ok = end_phase<NR>(acc, sh, part0, a.bar, nph++, a.err);
+    ok = end_phase<NR>(acc, sh, team);
     if (!ok) break;
     if (threadIdx.x < kMaxRhs) {
       const int k = threadIdx.x;
@@ -283,7 +289,7 @@ __global__ void __launch_bounds__(BS, 1) cg_mixed_kernel(MixedArgs a) {
     __syncthreads();
     // B: x^ += alpha p^, r^ -= alpha M t^
     zero_acc();
-    for_units(NI, s_run, [&](int k, uint32_t j) {
+    for_units(NI, s_run, team, [&](int k, uint32_t j) {
       const RowItem ri = make_item<W>(g, j);
       float smi[W];
       vload<float, W>(a.sm32 + ri.own, smi);
@@ -314,7 +320,7 @@ __global__ void __launch_bounds__(BS, 1) cg_mixed_kernel(MixedArgs a) {
         vstore<float, W>(rk + off, rv);
       }
     });
-    ok = end_phase<NR>(acc, sh, part1, a.bar, nph++, a.err, abort_req);
+    ok = end_phase<NR>(acc, sh, team, abort_req);
     if (!ok) break;
     const int abort_seen = sh.flag;  // block 0's abort flag (the next phase ends overwrite sh.flag)
     if (threadIdx.x < kMaxRhs) {
@@ -340,7 +346,7 @@ __global__ void __launch_bounds__(BS, 1) cg_mixed_kernel(MixedArgs a) {
     __syncthreads();
     if (s_upd.n > 0) {
       // C: t = M^T (x + x^) in FP64
-      for_units(NI64, s_upd, [&](int k, uint32_t j) {
+      for_units(NI64, s_upd, team, [&](int k, uint32_t j) {
         const RowItem it = make_item<W64>(g, j);
         double smi[W64];
         vload<double, W64>(sm + it.own, smi);
@@ -370,11 +376,11 @@ __global__ void __launch_bounds__(BS, 1) cg_mixed_kernel(MixedArgs a) {
         }
       });
       zero_acc();
-      ok = end_phase<1>(acc, sh, part0, a.bar, nph++, a.err);
+      ok = end_phase<1>(acc, sh, team);
       if (!ok) break;
       // D: x += x^, x^ = 0, r = b - M t, r^ = (float) r
       zero_acc();
-      for_units(NI64, s_upd, [&](int k, uint32_t j) {
+      for_units(NI64, s_upd, team, [&](int k, uint32_t j) {
         const RowItem it = make_item<W64>(g, j);
         double smi[W64];
         vload<double, W64>(sm + it.own, smi);
@@ -411,7 +417,7 @@ __global__ void __launch_bounds__(BS, 1) cg_mixed_kernel(MixedArgs a) {
           vstore<float, W64>(rhk + off, rf);
         }
       });
-      ok = end_phase<NR>(acc, sh, part1, a.bar, nph++, a.err);
+      ok = end_phase<NR>(acc, sh, team);
       if (!ok) break;
       if (threadIdx.x < kMaxRhs) {
         const int k = threadIdx.x;
@@ -436,14 +442,14 @@ __global__ void __launch_bounds__(BS, 1) cg_mixed_kernel(MixedArgs a) {
       __syncthreads();
     }
     if (abort_seen != 0) {  // block 0 saw the host's abort request at the end of phase B
-      if (threadIdx.x == 0 && blockIdx.x == 0) atomicExch(a.err, 2);
+      if (threadIdx.x == 0 && team.brank == 0) atomicExch(team.err, 2);
       ok = false;
       break;
     }
   }
   // ---------------------------------------------------------------- results
   // On the iteration cap x holds the solution of the last reliable update.
-  if (blockIdx.x == 0 && threadIdx.x < kMaxRhs) {
+  if (team.brank == 0 && threadIdx.x < kMaxRhs) {
     const int k = threadIdx.x;
     if (k < a.nrhs) {
       CgState st;
@@ -457,6 +463,15 @@ __global__ void __launch_bounds__(BS, 1) cg_mixed_kernel(MixedArgs a) {
       a.state[k] = st;
     }
   }
+}
+
+// The single-lattice solve: the whole cooperative grid is the team.
+template <int NC, int NR, int BS, int W>
+__global__ void __launch_bounds__(BS, 1) cg_mixed_kernel(MixedArgs a) {
+  __shared__ SyncShared sh;
+  __shared__ MixedShared ms;
+  Team team = grid_team(a.bar, a.partials, a.err);
+  mixed_solve<NC, NR, W>(a, team, sh, ms);
 }
 
 }  // namespace gn

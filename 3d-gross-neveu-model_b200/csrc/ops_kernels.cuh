@@ -50,30 +50,45 @@ __global__ void __launch_bounds__(kOpThreads) dirac_item_kernel(Geom g, const do
 // sigma_out = sigma_in + eps P, and sm is built from the updated values (every
 // thread forms sigma_in + eps P identically, so the neighbour values agree bit
 // for bit with the stored ones).  sigma_out must not alias sigma_in.
+// Loads of the per-site helpers: through the read-only cache (RO) when the
+// data is constant for the kernel's lifetime (separate launches), plain when
+// the same kernel writes it in an earlier phase (the batched kernel).
+template <bool RO, typename T>
+__device__ __forceinline__ T ld_site(const T *p) {
+  if constexpr (RO) return __ldg(p);
+  else return *p;
+}
+
+template <typename T, bool RO = true>
+__device__ __forceinline__ void sigma_mass_site(const Geom &g, uint32_t i, const T *__restrict__ sigma_in,
+                                                const T *__restrict__ P, T eps, T *__restrict__ sigma_out,
+                                                T *__restrict__ sm) {
+  const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1}, {1, 1, 1}};
+  uint32_t x0, x1, x2, par, row, k;
+  site_coords(g, i, x0, x1, x2, par, row, k);
+  T s = T(0);
+#pragma unroll
+  for (int c = 0; c < 8; c++) {
+    const uint32_t j = site_index(g, int(x0) - off[c][0], int(x1) - off[c][1], int(x2) - off[c][2]);
+    T v = ld_site<RO>(sigma_in + j);
+    if (P != nullptr) v = v + eps * ld_site<RO>(P + j);
+    s = (c == 0) ? v : s + v;
+  }
+  sm[i] = s / T(8);
+  if (sigma_out != nullptr) {
+    T v = ld_site<RO>(sigma_in + i);
+    if (P != nullptr) v = v + eps * ld_site<RO>(P + i);
+    sigma_out[i] = v;
+  }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kOpThreads) sigma_mass_kernel(Geom g, const T *__restrict__ sigma_in,
                                                                const T *__restrict__ P, T eps,
                                                                T *__restrict__ sigma_out, T *__restrict__ sm) {
   const uint32_t V = uint32_t(g.V);
-  const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1}, {1, 1, 1}};
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x) {
-    uint32_t x0, x1, x2, par, row, k;
-    site_coords(g, i, x0, x1, x2, par, row, k);
-    T s = T(0);
-#pragma unroll
-    for (int c = 0; c < 8; c++) {
-      const uint32_t j = site_index(g, int(x0) - off[c][0], int(x1) - off[c][1], int(x2) - off[c][2]);
-      T v = __ldg(sigma_in + j);
-      if (P != nullptr) v = v + eps * __ldg(P + j);
-      s = (c == 0) ? v : s + v;
-    }
-    sm[i] = s / T(8);
-    if (sigma_out != nullptr) {
-      T v = __ldg(sigma_in + i);
-      if (P != nullptr) v = v + eps * __ldg(P + i);
-      sigma_out[i] = v;
-    }
-  }
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x)
+    sigma_mass_site<T>(g, i, sigma_in, P, eps, sigma_out, sm);
 }
 
 // P += eps F (EvolveMomentaSigma, moleculardynamics.c:843-848)
@@ -88,30 +103,36 @@ __global__ void __launch_bounds__(kOpThreads) momenta_kernel(uint32_t V, T *P, c
 // x+2^, x+0^+1^+2^; flavour 0 first.  X_f = (M M^T)^-1 phi_f, Y_f = M^T X_f.
 // If P != null the momentum step P += pcoef F is fused (the integrators always
 // follow a force by one).
+template <typename T, bool RO = true>
+__device__ __forceinline__ void force_site(const Geom &g, uint32_t i, const T *__restrict__ X, const T *__restrict__ Y,
+                                           const T *__restrict__ sigma, T gcoef, T *__restrict__ F, T *P, T pcoef) {
+  const uint32_t V = uint32_t(g.V);
+  const int off[8][3] = {{0, 0, 0}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 1, 1}};
+  uint32_t x0, x1, x2, par, row, k;
+  site_coords(g, i, x0, x1, x2, par, row, k);
+  uint32_t cj[8];
+#pragma unroll
+  for (int c = 0; c < 8; c++) cj[c] = site_index(g, int(x0) + off[c][0], int(x1) + off[c][1], int(x2) + off[c][2]);
+  T f = T(0);
+#pragma unroll
+  for (int fl = 0; fl < 2; fl++) {
+    const T *Xf = X + size_t(fl) * V;
+    const T *Yf = Y + size_t(fl) * V;
+#pragma unroll
+    for (int c = 0; c < 8; c++) f = f + T(0.125) * (ld_site<RO>(Xf + cj[c]) * ld_site<RO>(Yf + cj[c]));
+  }
+  f = f - gcoef * ld_site<RO>(sigma + i);
+  F[i] = f;
+  if (P != nullptr) P[i] = P[i] + f * pcoef;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kOpThreads) force_kernel(Geom g, const T *__restrict__ X, const T *__restrict__ Y,
                                                           const T *__restrict__ sigma, T gcoef, T *__restrict__ F,
                                                           T *P, T pcoef) {
   const uint32_t V = uint32_t(g.V);
-  const int off[8][3] = {{0, 0, 0}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 1, 1}};
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x) {
-    uint32_t x0, x1, x2, par, row, k;
-    site_coords(g, i, x0, x1, x2, par, row, k);
-    uint32_t cj[8];
-#pragma unroll
-    for (int c = 0; c < 8; c++) cj[c] = site_index(g, int(x0) + off[c][0], int(x1) + off[c][1], int(x2) + off[c][2]);
-    T f = T(0);
-#pragma unroll
-    for (int fl = 0; fl < 2; fl++) {
-      const T *Xf = X + size_t(fl) * V;
-      const T *Yf = Y + size_t(fl) * V;
-#pragma unroll
-      for (int c = 0; c < 8; c++) f = f + T(0.125) * (__ldg(Xf + cj[c]) * __ldg(Yf + cj[c]));
-    }
-    f = f - gcoef * __ldg(sigma + i);
-    F[i] = f;
-    if (P != nullptr) P[i] = P[i] + f * pcoef;
-  }
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x)
+    force_site<T>(g, i, X, Y, sigma, gcoef, F, P, pcoef);
 }
 
 // Compensated block sums of up to 4 quantities: per thread a Neumaier sum,
@@ -174,7 +195,7 @@ __global__ void __launch_bounds__(kOpThreads) energy_kernel(uint32_t V, const T 
 // Condensate dot products (condensate.c:142-145, :172, :194, :209, :227) of a
 // complex vector v = (vr, vi) with D = (Dr, Di), both as two planes:
 //   q0 = sum Re(conj v D) / V, q1 = sum Re(conj v D), q2 = sum Im(conj v D)
-__global__ void __launch_bounds__(kOpThreads) cond_dot_kernel(uint32_t V, const double *__restrict__ v,
+static __global__ void __launch_bounds__(kOpThreads) cond_dot_kernel(uint32_t V, const double *__restrict__ v,
                                                              const double *__restrict__ D, double *part) {
   double hi[3] = {0, 0, 0}, lo[3] = {0, 0, 0};
   const double Vd = double(V);
@@ -193,7 +214,7 @@ __global__ void __launch_bounds__(kOpThreads) cond_dot_kernel(uint32_t V, const 
 //   mode 1: 1/V everywhere
 //   mode 2: phase table[x2] (re, im) indexed by the time coordinate
 //   mode 3: v *= sm (pointwise, both planes)
-__global__ void __launch_bounds__(kOpThreads) cond_fill_kernel(Geom g, int mode, const signed char *__restrict__ signs,
+static __global__ void __launch_bounds__(kOpThreads) cond_fill_kernel(Geom g, int mode, const signed char *__restrict__ signs,
                                                               const double *__restrict__ table,
                                                               const double *__restrict__ sm, double *v) {
   const uint32_t V = uint32_t(g.V);

@@ -35,6 +35,11 @@ __device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long l
   asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
+__device__ __forceinline__ int ld_relaxed_int(const int *p) {
+  int v;
+  asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
 __device__ __forceinline__ void fence_acquire() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 
 struct SyncShared {
@@ -44,16 +49,43 @@ struct SyncShared {
   int flag;                 // block 0's flag word of the last phase
 };
 
-// End of phase number `phase` (counted from 0 in every block alike), first
-// half: publishes this block's partial sums of NQ quantities (acc[]) and the
-// flag word, and waits until every block has done the same.  The grid's
-// writes of the phase are visible to this block on return.  Returns false if
-// this block's wait timed out (it then sets *err; the other blocks time out at
-// their next wait).  part_slot: [NQ][gridDim.x] partials followed by one flag
-// word.
+// A team: the blocks that sweep one lattice together and synchronise among
+// themselves -- the whole grid of a single-lattice solve, or a group of
+// blocks of the batched kernel.  A one-block team needs no global memory.
+struct Team {
+  uint32_t tid;       // thread index within the team
+  uint32_t nthreads;  // threads in the team
+  int brank;          // this block's index within the team
+  int nblocks;        // blocks in the team
+  PhaseBar *bar;      // arrival counter (nblocks > 1)
+  double *partials;   // [2][kSyncQ + 1][nblocks] partial sums (nblocks > 1)
+  int *err;           // set to 1 by a wait that timed out
+  unsigned long long nph;  // phases ended so far (the same count in every block of the team)
+};
+
+// The whole grid as one team.
+__device__ __forceinline__ Team grid_team(PhaseBar *bar, double *partials, int *err) {
+  Team t;
+  t.tid = blockIdx.x * blockDim.x + threadIdx.x;
+  t.nthreads = gridDim.x * blockDim.x;
+  t.brank = int(blockIdx.x);
+  t.nblocks = int(gridDim.x);
+  t.bar = bar;
+  t.partials = partials;
+  t.err = err;
+  t.nph = 0;
+  return t;
+}
+
+// End of the team's next phase, first half: publishes this block's partial
+// sums of NQ quantities (acc[]) and the flag word, and waits until every block
+// of the team has done the same.  The team's writes of the phase are visible
+// to this block on return.  Returns false if this block's wait timed out (it
+// then sets *err; the other blocks time out at their next wait).  Slots
+// alternate between two banks: [NQ][nblocks] partials, then one flag word.
 template <int NQ>
-__device__ __forceinline__ bool phase_arrive_wait(double (&acc)[kSyncQ], SyncShared &sh, double *part_slot,
-                                                  PhaseBar *bar, unsigned long long phase, int *err, int flag = 0) {
+__device__ __forceinline__ bool phase_arrive_wait(double (&acc)[kSyncQ], SyncShared &sh, const Team &t,
+                                                  int flag = 0) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
   for (int q = 0; q < NQ; q++) {
@@ -62,61 +94,71 @@ __device__ __forceinline__ bool phase_arrive_wait(double (&acc)[kSyncQ], SyncSha
   }
   __syncthreads();
   if (w == 0) {
-    double tot[NQ];
+    double tot[NQ > 0 ? NQ : 1];
 #pragma unroll
     for (int q = 0; q < NQ; q++) tot[q] = warp_sum(lane < nw ? sh.red[q * 32 + lane] : 0.0);
     if (lane == 0) {
+      if (t.nblocks == 1) {  // the block is the team: its sums are the totals
 #pragma unroll
-      for (int q = 0; q < NQ; q++) part_slot[size_t(q) * gridDim.x + blockIdx.x] = tot[q];
-      if (blockIdx.x == 0) reinterpret_cast<int *>(part_slot + size_t(NQ) * gridDim.x)[0] = flag;
-      // arrive (release: the block's writes of this phase, ordered before by the
-      // block barrier, become visible with it), poll with relaxed loads, and
-      // acquire once the count is complete
-      red_release_add64(&bar->arrived, 1ull);
-      const unsigned long long target = (phase + 1ull) * gridDim.x;
-      unsigned spins = 0;
-      int ok = 1;
-      while (ld_relaxed64(&bar->arrived) < target) {
-        if (++spins > (1u << 22)) {  // ~ a second: give up, report, return
-          atomicExch(err, 1);
-          ok = 0;
-          break;
+        for (int q = 0; q < NQ; q++) sh.val[q] = tot[q];
+        sh.flag = flag;
+        sh.ok = 1;
+      } else {
+        double *slot = t.partials + (t.nph & 1ull) * size_t(kSyncQ + 1) * t.nblocks;
+#pragma unroll
+        for (int q = 0; q < NQ; q++) slot[size_t(q) * t.nblocks + t.brank] = tot[q];
+        if (t.brank == 0) reinterpret_cast<int *>(slot + size_t(NQ) * t.nblocks)[0] = flag;
+        // arrive (release: the block's writes of this phase, ordered before by
+        // the block barrier, become visible with it), poll with relaxed loads,
+        // and acquire once the count is complete
+        red_release_add64(&t.bar->arrived, 1ull);
+        const unsigned long long target = (t.nph + 1ull) * t.nblocks;
+        unsigned spins = 0;
+        int ok = 1;
+        while (ld_relaxed64(&t.bar->arrived) < target) {
+          if (++spins > (1u << 22)) {  // ~ a second: give up, report, return
+            atomicExch(t.err, 1);
+            ok = 0;
+            break;
+          }
         }
+        fence_acquire();
+        sh.ok = ok;
       }
-      fence_acquire();
-      sh.ok = ok;
     }
   }
   __syncthreads();
   return sh.ok != 0;
 }
 
-// Second half: the grid totals into sh.val[0..NQ) and block 0's flag word into
-// sh.flag, summed by every block in the same order (so every block holds the
-// same bits).  Any work that does not need the totals may run between the two
-// halves: the partials' round trip then overlaps it.
+// Second half: the team totals into sh.val[0..NQ) and the flag word of the
+// team's block 0 into sh.flag, summed by every block in the same order (so
+// every block holds the same bits).  Advances the team's phase count.
 template <int NQ>
-__device__ __forceinline__ void phase_totals(SyncShared &sh, const double *part_slot) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  if (w < NQ) {
-    const double *p = part_slot + size_t(w) * gridDim.x;
-    double s = 0.0;
-    for (int b = lane; b < int(gridDim.x); b += 32) s += p[b];
-    s = warp_sum(s);
-    if (lane == 0) sh.val[w] = s;
-  } else if (threadIdx.x == blockDim.x - 1) {
-    sh.flag = reinterpret_cast<const int *>(part_slot + size_t(NQ) * gridDim.x)[0];
+__device__ __forceinline__ void phase_totals(SyncShared &sh, Team &t) {
+  if (t.nblocks > 1) {
+    const double *slot = t.partials + (t.nph & 1ull) * size_t(kSyncQ + 1) * t.nblocks;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (w < NQ) {
+      const double *p = slot + size_t(w) * t.nblocks;
+      double s = 0.0;
+      for (int b = lane; b < t.nblocks; b += 32) s += p[b];
+      s = warp_sum(s);
+      if (lane == 0) sh.val[w] = s;
+    } else if (threadIdx.x == blockDim.x - 1) {
+      sh.flag = reinterpret_cast<const int *>(slot + size_t(NQ) * t.nblocks)[0];
+    }
+    __syncthreads();
   }
-  __syncthreads();
+  t.nph++;
 }
 
-// Both halves: on return sh.val[0..NQ) holds the grid totals in every block and
-// sh.flag the word block 0 put in `flag`.
+// Both halves: on return sh.val[0..NQ) holds the team totals in every block
+// and sh.flag the word the team's block 0 put in `flag`.
 template <int NQ>
-__device__ __forceinline__ bool end_phase(double (&acc)[kSyncQ], SyncShared &sh, double *part_slot, PhaseBar *bar,
-                                          unsigned long long phase, int *err, int flag = 0) {
-  const bool ok = phase_arrive_wait<NQ>(acc, sh, part_slot, bar, phase, err, flag);
-  phase_totals<NQ>(sh, part_slot);
+__device__ __forceinline__ bool end_phase(double (&acc)[kSyncQ], SyncShared &sh, Team &t, int flag = 0) {
+  const bool ok = phase_arrive_wait<NQ>(acc, sh, t, flag);
+  phase_totals<NQ>(sh, t);
   return ok;
 }
 
