@@ -31,6 +31,7 @@ UNITS = {
     "capi.cu": [],
     "noalloc.cu": ["--fmad=false"],
     "exact.cu": ["--fmad=false"],
+    "ensemble.cu": ["--fmad=false"],
 }
 CORE_LIB = LIB / "libgn_b200.so"
 DROPIN_LIB = LIB / "libgn_dropin.so"

@@ -1,0 +1,311 @@
+// ensemble_kernel.cuh -- many independent sigma-HMC chains of mixed lattice
+// sizes in one persistent kernel per slice of a trajectory.
+//
+// A launch runs one slice of the trajectory's op list (an MD step, or the
+// refresh / initial solve / energy at either end) for every chain.  Chains are
+// taken from a work queue in order of decreasing volume: the big ones by
+// groups of gs blocks that synchronise with a team barrier (phase_sync.cuh),
+// the small ones by single blocks that need only __syncthreads.  Every chain's
+// work is a fixed sequence of team phases, so every block of a team takes the
+// same branches.  Momenta, pseudofermion sources and the Metropolis uniform
+// come from the chain's own Philox stream (philox.cuh) with the trajectory
+// number as the counter, so a chain's results do not depend on the chains
+// beside it or on which team ran it (for a fixed team size).
+#pragma once
+#include "mixed_kernel.cuh"
+#include "ops_kernels.cuh"
+#include "philox.cuh"
+
+namespace gn {
+
+constexpr int kEnsThreads = 1024;
+
+// Ops of the batched trajectory (the schedule of schedule.h, translated).
+enum EnsOpCode : int {
+  E_REFRESH = 1,  // save sigma; P, chi_0, chi_1 ~ N(0, 1) from the chain's stream
+  E_PHI,          // phi_f = M chi_f
+  E_SOLVE,        // X_f = (M M^T)^-1 phi_f, both flavours, mixed precision
+  E_FORCE,        // Y_f = M^T X_f; F = sigma force; P += c F
+  E_P,            // P += c F
+  E_Q,            // sigma += c P, sm recomputed
+  E_ENERGY0,      // H0
+  E_ENERGY1,      // H1
+  E_METROPOLIS    // accept if u <= exp(-(H1 - H0)), else restore sigma; statistics
+};
+
+struct EnsOp {
+  int code;
+  double c;
+};
+
+// One chain's arrays (device pointers, 256-byte aligned) and constants.
+struct EnsChain {
+  Geom g;
+  int w;  // sites per FP32 item (4, 2 or 1); the FP64 sweeps use min(w, 2)
+  double beta_s;
+  unsigned long long stream;  // Philox key word of the chain
+  double *sigma[2];           // current / other (ping-pong of the sigma steps)
+  double *sm, *P, *F, *sigma_save;
+  double *chi, *phi, *X, *Y;  // two flavour planes each
+  double *t64;                // solver FP64 scratch, two planes
+  float *sm32, *rh, *ph, *th, *xh;  // solver FP32 vectors, two planes each
+};
+
+// One chain's mutable state (device).
+struct EnsState {
+  int cur;     // which sigma buffer is current
+  int failed;  // a solve of the current trajectory did not converge
+  double H0, H1;
+  long long ntraj;  // trajectories done: the Philox counter of the next one
+  // accumulated since the last reset
+  long long n, nacc, iters, reliable, fails;
+  double sum_dH, sum_exp_mdH, sum_sigma2, last_dH;
+  int last_acc;
+};
+
+struct EnsLaunch {
+  const EnsChain *chains;
+  EnsState *states;
+  int nchains;
+  const int *order;  // chain indices: the nbig big chains first, all by decreasing volume
+  int nbig;
+  const EnsOp *ops;
+  int op_begin, op_end;
+  int gs;             // blocks per group (big chains)
+  int *queue;         // [2] next big / next small task; zero before the launch
+  PhaseBar *bars;     // [groups] team barrier counters; zero before the launch
+  double *partials;   // [groups][2][kSyncQ + 1][gs]
+  CgState *cg_state;  // [gridDim.x][kMaxRhs] solver status scratch
+  int *err;
+  unsigned long long seed;
+  double tol;     // relative tolerance of every solve
+  double delta;   // reliable-update threshold
+  int n_ru;       // reliable update at least every n_ru iterations
+};
+
+// Sweep of (plane, item) units of W sites over the team: M or M^T of two planes.
+template <int W, int OP>
+__device__ __forceinline__ void team_dirac2(const Geom &g, const Team &t, const double *sm, const double *in,
+                                            double *out) {
+  const uint32_t NI = row_items<W>(g), V = uint32_t(g.V);
+  for (uint32_t u = t.tid; u < 2u * NI; u += t.nthreads) {
+    const uint32_t f = u >= NI ? 1u : 0u, j = u - f * NI;
+    const RowItem it = make_item<W>(g, j);
+    Nb<double> n[W];
+    double smv[W], o[W];
+    gather_item<double, W>(it, in + size_t(f) * V, n);
+    vload<double, W>(sm + it.own, smv);
+    if (OP == 0) item_M<double, W>(it, smv, n, o);
+    else item_Mt<double, W>(it, smv, n, o);
+    vstore<double, W>(out + size_t(f) * V + it.own, o);
+  }
+}
+
+// The solver of one chain, one function per item width (each gets its own
+// register allocation instead of sharing the caller's).
+template <int W>
+__device__ __noinline__ void ens_solve(const MixedArgs &a, Team &t, SyncShared &sh, MixedShared &ms) {
+  mixed_solve<1, 2, W>(a, t, sh, ms);
+}
+
+// Box-Muller on two uniforms: two N(0, 1) values.
+__device__ __forceinline__ void box_muller(uint64_t a, uint64_t b, double &z0, double &z1) {
+  const double r = sqrt(-2.0 * log(phx_unit_open0(a)));
+  double s, c;
+  sincospi(2.0 * phx_unit(b), &s, &c);
+  z0 = r * c;
+  z1 = r * s;
+}
+
+// The chain's ops [op_begin, op_end) by team t.  Returns false on a barrier timeout.
+__device__ __noinline__ bool ens_run_chain(const EnsLaunch &L, int c, Team &t, SyncShared &sh, MixedShared &ms) {
+  const EnsChain &ch = L.chains[c];
+  EnsState *st = L.states + c;
+  const Geom g = ch.g;
+  const uint32_t V = uint32_t(g.V);
+  const bool leader = t.brank == 0 && threadIdx.x == 0;
+  int cur = st->cur;  // every thread tracks the ping-pong index itself
+  double acc[kSyncQ];
+  auto zero_acc = [&]() {
+#pragma unroll
+    for (int q = 0; q < kSyncQ; q++) acc[q] = 0.0;
+  };
+  for (int o = L.op_begin; o < L.op_end; o++) {
+    const EnsOp op = L.ops[o];
+    double *const sig = ch.sigma[cur];
+    double *const sig_o = ch.sigma[cur ^ 1];
+    zero_acc();
+    bool ok = true;
+    if (op.code == E_REFRESH) {
+      const unsigned long long traj = (unsigned long long)st->ntraj;
+      for (uint32_t i = t.tid; i < V; i += t.nthreads) ch.sigma_save[i] = sig[i];
+      // four sites per Philox block: P, chi_0, chi_1
+      for (uint32_t u = t.tid; u < 3u * (V / 4u); u += t.nthreads) {
+        const uint32_t f = u / (V / 4u), q = u - f * (V / 4u);
+        const Philox4x64 r = phx_draw(L.seed, ch.stream, traj, f, q);
+        double z[4];
+        box_muller(r.v[0], r.v[1], z[0], z[1]);
+        box_muller(r.v[2], r.v[3], z[2], z[3]);
+        double *dst = f == 0 ? ch.P : ch.chi + size_t(f - 1) * V;
+#pragma unroll
+        for (int e = 0; e < 4; e++) dst[4 * q + e] = z[e];
+      }
+      if (leader) st->failed = 0;
+      ok = end_phase<0>(acc, sh, t);
+    } else if (op.code == E_PHI) {
+      if (ch.w >= 2) team_dirac2<2, 0>(g, t, ch.sm, ch.chi, ch.phi);
+      else team_dirac2<1, 0>(g, t, ch.sm, ch.chi, ch.phi);
+      ok = end_phase<0>(acc, sh, t);
+    } else if (op.code == E_SOLVE) {
+      MixedArgs a;
+      a.g = g;
+      a.sm = ch.sm;
+      a.sm32 = ch.sm32;
+      for (int k = 0; k < kMaxRhs; k++) {
+        const int kk = k < 2 ? k : 1;
+        a.b[k] = ch.phi + size_t(kk) * V;
+        a.x[k] = ch.X + size_t(kk) * V;
+        a.t64[k] = ch.t64 + size_t(kk) * V;
+        a.rh[k] = ch.rh + size_t(kk) * V;
+        a.ph[k] = ch.ph + size_t(kk) * V;
+        a.th[k] = ch.th + size_t(kk) * V;
+        a.xh[k] = ch.xh + size_t(kk) * V;
+      }
+      a.nrhs = 2;
+      a.variant = 1;
+      a.rel = 1;
+      a.tol = L.tol;
+      a.max_iter = (long long)V + 1;
+      a.delta = L.delta;
+      a.n_ru = L.n_ru;
+      a.partials = nullptr;
+      a.bar = nullptr;
+      a.err = t.err;
+      a.abort_flag = nullptr;
+      a.state = L.cg_state + size_t(blockIdx.x) * kMaxRhs;
+      if (ch.w == 4) ens_solve<4>(a, t, sh, ms);
+      else if (ch.w == 2) ens_solve<2>(a, t, sh, ms);
+      else ens_solve<1>(a, t, sh, ms);
+      if (leader) {
+        for (int k = 0; k < 2; k++) {
+          const int s = ms.status[k];
+          if (s != kCgConverged && s != kCgConvergedStart) st->failed = 1;
+          st->iters += (s == kCgConverged) ? ms.iters[k] : 0;
+          st->reliable += ms.nru[k];
+        }
+      }
+      ok = ld_relaxed_int(t.err) == 0;
+    } else if (op.code == E_FORCE) {
+      if (ch.w >= 2) team_dirac2<2, 1>(g, t, ch.sm, ch.X, ch.Y);
+      else team_dirac2<1, 1>(g, t, ch.sm, ch.X, ch.Y);
+      ok = end_phase<0>(acc, sh, t);
+      const double gcoef = (4 * ch.beta_s / 2.0);  // (NFLAV * beta_scalar / 2.0), moleculardynamics.c:580
+      for (uint32_t i = t.tid; i < V && ok; i += t.nthreads)
+        force_site<double, false>(g, i, ch.X, ch.Y, sig, gcoef, ch.F, ch.P, op.c);
+      ok = end_phase<0>(acc, sh, t) && ok;
+    } else if (op.code == E_P) {
+      for (uint32_t i = t.tid; i < V; i += t.nthreads) ch.P[i] = ch.P[i] + ch.F[i] * op.c;
+      ok = end_phase<0>(acc, sh, t);
+    } else if (op.code == E_Q) {
+      for (uint32_t i = t.tid; i < V; i += t.nthreads)
+        sigma_mass_site<double, false>(g, i, sig, ch.P, op.c, sig_o, ch.sm);
+      cur ^= 1;
+      ok = end_phase<0>(acc, sh, t);
+    } else if (op.code == E_ENERGY0 || op.code == E_ENERGY1) {
+      // ComputeFullEnergyForSigma, moleculardynamics.c:299-319
+      for (uint32_t i = t.tid; i < V; i += t.nthreads) {
+        const double p = ch.P[i];
+        acc[0] += p * p / 2.0;
+        acc[1] += 0.5 * (ch.phi[i] * ch.X[i]) + 0.5 * (ch.phi[V + i] * ch.X[V + i]);
+        acc[2] += sig[i] * sig[i];
+      }
+      ok = end_phase<3>(acc, sh, t);
+      const double h = (sh.val[0] + sh.val[1]) + (4 * ch.beta_s / 4.0) * sh.val[2];
+      if (leader) {
+        if (op.code == E_ENERGY0) st->H0 = h;
+        else st->H1 = h;
+      }
+      ok = end_phase<0>(acc, sh, t) && ok;  // H stored before anyone reads it
+    } else if (op.code == E_METROPOLIS) {
+      const double dH = st->H1 - st->H0;
+      const Philox4x64 r = phx_draw(L.seed, ch.stream, (unsigned long long)st->ntraj, kPhxMetropolis, 0);
+      const int failed = st->failed;
+      const int accept = !failed && (phx_unit(r.v[0]) <= exp(-dH));
+      if (!accept) {  // restore sigma and its mass (moleculardynamics.c:1404-1416)
+        for (uint32_t i = t.tid; i < V; i += t.nthreads)
+          sigma_mass_site<double, false>(g, i, ch.sigma_save, (const double *)nullptr, 0.0, sig_o, ch.sm);
+        cur ^= 1;
+      }
+      ok = end_phase<0>(acc, sh, t);
+      const double *fin = ch.sigma[cur];
+      for (uint32_t i = t.tid; i < V; i += t.nthreads) acc[0] += fin[i] * fin[i];
+      ok = end_phase<1>(acc, sh, t) && ok;
+      if (leader) {
+        st->n++;
+        st->nacc += accept;
+        st->fails += failed;
+        st->sum_dH += dH;
+        st->sum_exp_mdH += exp(-dH);
+        st->sum_sigma2 += sh.val[0] / double(V);
+        st->last_dH = dH;
+        st->last_acc = accept;
+        st->ntraj++;
+      }
+    }
+    if (!ok) return false;
+  }
+  // every block of the team has passed the last barrier (after reading st->cur)
+  if (leader) st->cur = cur;
+  return true;
+}
+
+__global__ void __launch_bounds__(kEnsThreads, 1) ens_node_kernel(EnsLaunch L) {
+  __shared__ SyncShared sh;
+  __shared__ MixedShared ms;
+  __shared__ int s_task;
+  const int gs = L.gs;
+  const int group = int(blockIdx.x) / gs, grank = int(blockIdx.x) % gs;
+  // ---- big chains: a group of gs blocks each
+  if (gs > 1 && L.nbig > 0) {
+    Team gt;
+    gt.tid = uint32_t(grank) * blockDim.x + threadIdx.x;
+    gt.nthreads = uint32_t(gs) * blockDim.x;
+    gt.brank = grank;
+    gt.nblocks = gs;
+    gt.bar = L.bars + group;
+    gt.partials = L.partials + size_t(group) * 2 * (kSyncQ + 1) * gs;
+    gt.err = L.err;
+    gt.nph = 0;
+    for (;;) {
+      int task = 0;
+      if (grank == 0 && threadIdx.x == 0) task = atomicAdd(&L.queue[0], 1);
+      double acc[kSyncQ];
+#pragma unroll
+      for (int q = 0; q < kSyncQ; q++) acc[q] = 0.0;
+      if (!end_phase<0>(acc, sh, gt, task)) return;  // the group leader's task, to every block
+      task = sh.flag;
+      if (task >= L.nbig) break;
+      if (!ens_run_chain(L, L.order[task], gt, sh, ms)) return;
+    }
+  }
+  // ---- small chains: one block each
+  Team bt;
+  bt.tid = threadIdx.x;
+  bt.nthreads = blockDim.x;
+  bt.brank = 0;
+  bt.nblocks = 1;
+  bt.bar = nullptr;
+  bt.partials = nullptr;
+  bt.err = L.err;
+  bt.nph = 0;
+  for (;;) {
+    if (threadIdx.x == 0) s_task = L.nbig + atomicAdd(&L.queue[1], 1);
+    __syncthreads();
+    const int task = s_task;
+    __syncthreads();
+    if (task >= L.nchains) break;
+    if (!ens_run_chain(L, L.order[task], bt, sh, ms)) return;
+  }
+}
+
+}  // namespace gn

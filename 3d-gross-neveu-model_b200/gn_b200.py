@@ -58,6 +58,20 @@ class TrajResult(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class EnsParams(C.Structure):
+    _fields_ = [("eps", C.c_double), ("steps", C.c_int), ("integrator", C.c_int), ("tol", C.c_double)]
+
+
+class ChainStats(C.Structure):
+    _fields_ = [("trajectories", C.c_longlong), ("accepted", C.c_longlong), ("failed", C.c_longlong),
+                ("cg_iterations", C.c_longlong), ("reliable_updates", C.c_longlong), ("sum_dH", C.c_double),
+                ("sum_exp_mdH", C.c_double), ("sum_sigma2", C.c_double), ("last_dH", C.c_double),
+                ("last_accepted", C.c_int), ("total_trajectories", C.c_longlong)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _dp = C.POINTER(C.c_double)
 _lib = None
 
@@ -107,6 +121,18 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
         "gn_launch_count": ([v], C.c_longlong),
         "gn_flush_l2": ([v], C.c_int),
         "gn_set_parity_mode": ([v, C.c_int], C.c_int),
+        "gn_ensemble_create": ([C.POINTER(v), C.c_int, C.POINTER(C.c_int), _dp, C.POINTER(C.c_ulonglong),
+                                C.c_ulonglong, C.c_int], C.c_int),
+        "gn_ensemble_destroy": ([v], None),
+        "gn_ensemble_load_sigma": ([v, C.c_int, _dp], C.c_int),
+        "gn_ensemble_store_sigma": ([v, C.c_int, _dp, _dp], C.c_int),
+        "gn_ensemble_set_layout": ([v, C.c_int, C.c_longlong], C.c_int),
+        "gn_ensemble_tune": ([v, C.POINTER(EnsParams), C.POINTER(C.c_int), C.POINTER(C.c_longlong)], C.c_int),
+        "gn_ensemble_run": ([v, C.POINTER(EnsParams), C.c_int, C.c_int], C.c_int),
+        "gn_ensemble_stats": ([v, C.POINTER(ChainStats), C.c_int], C.c_int),
+        "gn_ensemble_stream": ([v], C.c_void_p),
+        "gn_ensemble_info": ([v, C.POINTER(C.c_int), C.POINTER(C.c_longlong), C.POINTER(C.c_int),
+                              C.POINTER(C.c_int)], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -336,3 +362,75 @@ class Lattice:
 
     def flush_l2(self):
         self._check(self.lib.gn_flush_l2(self.ctx))
+
+
+class Ensemble:
+    """Many independent sigma-HMC chains (gn_ensemble_* of gn_b200.h)."""
+
+    def __init__(self, Ls, betas, seed=1231, stream_ids=None, device=0):
+        self.lib = load_library()
+        self.Ls = [int(x) for x in Ls]
+        self.n = len(self.Ls)
+        Larr = (C.c_int * self.n)(*self.Ls)
+        barr = np.ascontiguousarray(betas, np.float64)
+        ids = None if stream_ids is None else (C.c_ulonglong * self.n)(*[int(x) for x in stream_ids])
+        self.ens = C.c_void_p()
+        self._check(self.lib.gn_ensemble_create(C.byref(self.ens), self.n, Larr, _p(barr), ids, int(seed), device))
+
+    def _check(self, st, allow=(GN_OK,)):
+        if st not in allow:
+            raise GnError(st, self.lib.gn_last_error().decode())
+        return st
+
+    def close(self):
+        if self.ens:
+            self.lib.gn_ensemble_destroy(self.ens)
+            self.ens = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def load_sigma(self, c, sigma):
+        s = np.ascontiguousarray(sigma, np.float64)
+        assert s.size == self.Ls[c] ** 3
+        self._check(self.lib.gn_ensemble_load_sigma(self.ens, c, _p(s)))
+
+    def store_sigma(self, c):
+        V = self.Ls[c] ** 3
+        s, sm = np.empty(V), np.empty(V)
+        self._check(self.lib.gn_ensemble_store_sigma(self.ens, c, _p(s), _p(sm)))
+        return s, sm
+
+    @staticmethod
+    def params(eps, steps, integrator=GN_LFMN2VF, tol=1e-10):
+        return EnsParams(eps, steps, integrator, tol)
+
+    def set_layout(self, group_blocks, big_min_volume):
+        self._check(self.lib.gn_ensemble_set_layout(self.ens, group_blocks, big_min_volume))
+
+    def tune(self, p):
+        gs, vmin = C.c_int(), C.c_longlong()
+        self._check(self.lib.gn_ensemble_tune(self.ens, C.byref(p), C.byref(gs), C.byref(vmin)))
+        return gs.value, vmin.value
+
+    def run(self, p, ntraj, graph=True):
+        self._check(self.lib.gn_ensemble_run(self.ens, C.byref(p), int(ntraj), int(graph)))
+
+    def stats(self, reset=False):
+        out = (ChainStats * self.n)()
+        self._check(self.lib.gn_ensemble_stats(self.ens, out, int(reset)))
+        return [o.as_dict() for o in out]
+
+    @property
+    def stream(self):
+        """The cudaStream_t (as an int) the ensemble runs on."""
+        return self.lib.gn_ensemble_stream(self.ens)
+
+    def info(self):
+        gs, vmin, g, nl = C.c_int(), C.c_longlong(), C.c_int(), C.c_int()
+        self._check(self.lib.gn_ensemble_info(self.ens, C.byref(gs), C.byref(vmin), C.byref(g), C.byref(nl)))
+        return {"group_blocks": gs.value, "big_min_volume": vmin.value, "graph": g.value,
+                "launches_per_trajectory": nl.value}

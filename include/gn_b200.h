@@ -237,6 +237,71 @@ GN_API const char *gn_cg_noalloc_error(void);
 /* The largest V = L^3 gn_cg_noalloc accepts. */
 GN_API long long gn_cg_noalloc_max_volume(void);
 
+/* ---- batched chains ------------------------------------------------------ */
+
+/* No counterpart in the reference, which runs one chain per process
+ * (observables.c:178 drives one lattice).  An ensemble holds many independent
+ * sigma-HMC chains, each with its own lattice size L (even, 4..256) and
+ * beta_s, on one GPU.  Every trajectory is the reference's (the integrators of
+ * moleculardynamics.c:859 / :1018 / :1234, energy of :299, Metropolis test
+ * u <= exp(-dH) with sigma restored on reject); every solve is the
+ * mixed-precision CG to a true relative residual `tol`, from x = 0.  The
+ * random numbers (momenta, pseudofermion sources, the Metropolis uniform) come
+ * from the chain's own Philox4x64-10 stream, key (seed, stream id), counter
+ * (trajectory number, field, site block): a chain's trajectory depends only on
+ * its own state, L, beta_s, stream id and the team layout, not on the chains
+ * beside it.  All chains advance together: one persistent kernel per MD step,
+ * the trajectory replayed as a CUDA graph. */
+typedef struct gn_ensemble gn_ensemble;
+
+typedef struct {
+  double eps;     /* MD step size */
+  int steps;      /* MD steps per trajectory (>= 1) */
+  int integrator; /* GN_LFMN2VF, GN_LF2 or GN_LFMN2 */
+  double tol;     /* relative tolerance of every solve, true residual (> 0) */
+} gn_ens_params;
+
+typedef struct {
+  long long trajectories;       /* since the last reset */
+  long long accepted;
+  long long failed;             /* trajectories rejected because a solve did not converge */
+  long long cg_iterations;      /* inner (FP32) iterations of the counted solves */
+  long long reliable_updates;
+  double sum_dH, sum_exp_mdH;   /* sums of dH and exp(-dH) */
+  double sum_sigma2;            /* sum over trajectories of (1/V) sum_x sigma(x)^2 after the trajectory */
+  double last_dH;
+  int last_accepted;
+  long long total_trajectories; /* since creation (the Philox counter of the next one) */
+} gn_chain_stats;
+
+/* nchains chains: L[c], beta_s[c]; stream_ids[c] (NULL: c) keys each chain's
+ * Philox stream together with seed.  sigma starts at 0: load it per chain. */
+GN_API int gn_ensemble_create(gn_ensemble **ens, int nchains, const int *L, const double *beta_s,
+                              const unsigned long long *stream_ids, unsigned long long seed, int device);
+GN_API void gn_ensemble_destroy(gn_ensemble *ens);
+/* sigma of chain c (V doubles, fermion order) in and out; sm optional on output. */
+GN_API int gn_ensemble_load_sigma(gn_ensemble *ens, int chain, const double *sigma);
+GN_API int gn_ensemble_store_sigma(gn_ensemble *ens, int chain, double *sigma, double *sigmamass);
+/* Team layout: chains with V >= big_min_volume run on groups of group_blocks
+ * blocks, the others on single blocks (group_blocks = 1: all on single blocks).
+ * The layout fixes the order of the reductions, hence the last bits. */
+GN_API int gn_ensemble_set_layout(gn_ensemble *ens, int group_blocks, long long big_min_volume);
+/* Autotuner: times the refresh-and-solve slice (no effect on any chain's
+ * results) for every candidate layout, keeps the fastest and returns it. */
+GN_API int gn_ensemble_tune(gn_ensemble *ens, const gn_ens_params *p, int *group_blocks, long long *big_min_volume);
+/* ntraj trajectories of every chain; use_graph = 1 replays a captured CUDA
+ * graph (falls back to direct launches where capture is not possible).
+ * GN_ERR_TIMEOUT if a team barrier timed out. */
+GN_API int gn_ensemble_run(gn_ensemble *ens, const gn_ens_params *p, int ntraj, int use_graph);
+/* Per-chain statistics into out[nchains] (may be NULL); reset = 1 zeroes the
+ * accumulators afterwards. */
+GN_API int gn_ensemble_stats(gn_ensemble *ens, gn_chain_stats *out, int reset);
+/* The CUDA stream (cudaStream_t) the ensemble's work runs on. */
+GN_API void *gn_ensemble_stream(gn_ensemble *ens);
+/* The layout in use, whether the last run used the graph, kernel launches per trajectory. */
+GN_API int gn_ensemble_info(gn_ensemble *ens, int *group_blocks, long long *big_min_volume, int *graph_used,
+                            int *launches_per_trajectory);
+
 #ifdef __cplusplus
 }
 #endif
