@@ -66,7 +66,7 @@ def parse():
     ap.add_argument("--eps", type=float, default=0.05)
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--case", choices=["cg64", "dirac128", "dirac256", "traj64", "cgscan"], default=None,
+    ap.add_argument("--case", choices=["cg64", "dirac128", "dirac256", "traj64", "cgscan", "batched"], default=None,
                     help="run one small case for a profiler instead of the benchmark")
     return ap.parse_args()
 
@@ -439,6 +439,48 @@ def kernel_roofline(lat, stream, a, G):
                     f"{(2 * 5 * 4 + 8 * 3) * V / 1e6:.0f} MB is L2-resident within the solve"}
 
 
+def batched_bench(G, dev, nchains=256, ntraj=2, warmup=1, tune=True):
+    """The batched ensemble: nchains chains with L uniform in {8, 12, 16, 24, 32,
+    48} (seeded), beta_s on a uniform grid over [0.5, 1.2], LFMN2VF 8 x eps 0.08,
+    every solve mixed precision to 1e-10 (true relative residual), device
+    Philox draws, one persistent kernel per MD step replayed as a CUDA graph.
+    Timed with CUDA events on the ensemble's stream over `ntraj` trajectories
+    of every chain after `warmup`.  Algorithmic bytes: 96 per site per pair of
+    solver iterations (the two flavours' FP32 sweeps, 8 + 2 x 44 B)."""
+    import torch
+    rng = np.random.default_rng(4242)
+    Ls = [int(x) for x in rng.choice([8, 12, 16, 24, 32, 48], size=nchains)]
+    betas = list(np.linspace(0.5, 1.2, nchains))
+    p = G.Ensemble.params(0.08, 8)
+    with G.Ensemble(Ls, betas, seed=1231) as e:
+        for c, (L, b) in enumerate(zip(Ls, betas)):
+            e.load_sigma(c, rng.normal(0.0, np.sqrt(2.0 / (NFLAV * b)), L ** 3))
+        layout = e.tune(p) if tune else (1, 0)
+        e.run(p, warmup)
+        e.stats(reset=True)
+        st = torch.cuda.ExternalStream(e.stream, device=dev)
+        e0, e1 = cuda_events()
+        e0.record(st)
+        e.run(p, ntraj)
+        e1.record(st)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        stats = e.stats()
+        info = e.info()
+    sites = sum(L ** 3 for L in Ls)
+    iters = sum(s["cg_iterations"] for s in stats)
+    acc = sum(s["accepted"] for s in stats) / (nchains * ntraj)
+    nbytes = sum(L ** 3 * s["cg_iterations"] / 2 * 96 for L, s in zip(Ls, stats))
+    return {"metric": "chain trajectories/s, 256 chains L in {8..48}, LFMN2VF 8 x eps 0.08, mixed CG to 1e-10",
+            "value": nchains * ntraj / (ms / 1e3), "unit": "traj/s",
+            "site_trajectories_per_s": sites * ntraj / (ms / 1e3), "ms_per_ensemble_trajectory": ms / ntraj,
+            "chains": nchains, "sites": sites, "acceptance": acc,
+            "cg_iterations_per_chain_trajectory": iters / (nchains * ntraj),
+            "solver_gbs": nbytes / (ms / 1e3) / 1e9,
+            "layout": {"group_blocks": layout[0], "big_min_volume": layout[1]},
+            "graph": info["graph"], "launches_per_trajectory": info["launches_per_trajectory"] + 2}
+
+
 def dirac_roofline(G, stream, dev, reps=20, L=256):
     """Dirac M on one FP64 plane at L = 256 (V = 16,777,216): psi, sm and the
     output are 384 MB, three times the L2, so back-to-back launches run from
@@ -485,6 +527,9 @@ def run_case(a):
         return
     if a.case == "cgscan":
         cg_scan(G, dev)
+        return
+    if a.case == "batched":
+        print(json.dumps(batched_bench(G, dev)))
         return
     L, V = 64, 64 ** 3
     lat = G.Lattice(L, 0)

@@ -210,11 +210,12 @@ class Port:
 class Ref:
     """The reference's own code at one lattice size (oracle/_ref/libgnref_L{L}_i{I}.so)."""
 
-    def __init__(self, L: int, integrator: int = 0, build: bool = True):
+    def __init__(self, L: int, integrator: int = 0, build: bool = True, extra_defs: tuple = (), tag: str = ""):
+        """extra_defs / tag: a variant build (e.g. other CG tolerances) under its own name."""
         from . import build_ref  # noqa: F401  (package-relative when imported as oracle.oracle)
-        path = build_ref.lib_path(L, integrator)
+        path = build_ref.lib_path(L, integrator, tag)
         if build and build_ref.available():
-            path = build_ref.build(L, integrator)
+            path = build_ref.build(L, integrator, tuple(extra_defs), tag)
         if not path.exists():
             raise FileNotFoundError(f"{path} not built (the reference tree is needed to build it)")
         # RTLD_LOCAL: several L's can be loaded side by side

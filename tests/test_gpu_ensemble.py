@@ -1,0 +1,127 @@
+"""Batched chains (gn_ensemble_*): many independent sigma-HMC chains of mixed
+lattice sizes in persistent kernels per MD step, replayed as a CUDA graph,
+with device Philox random numbers.
+
+- Statistics agree with the reference's own chains within statistical errors
+  (tests/golden/ensemble_reference_L8.json, made by
+  tests/golden/make_ensemble_stats.py) for three beta_s: acceptance,
+  <sigma^2>, <|sigma_bar|> and the condensate oriented by the sign of
+  sigma_bar (the Z2 symmetry sigma -> -sigma flips tr1 with it; a chain in the
+  broken phase stays in one vacuum, so the GPU chains, started independently,
+  populate both).  <exp(-dH)> = 1, the identity of a reversible
+  area-preserving integrator, holds within the GPU chains' error.
+- A chain's trajectory does not depend on the chains beside it: the same chain
+  alone and in a mixed ensemble ends bit for bit the same, with and without
+  the CUDA graph.
+- The autotuner returns a layout and the benchmark's mix of sizes runs.
+"""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GOLD = Path(__file__).resolve().parent / "golden"
+
+
+def _sigma0(L, beta, seed):
+    return np.random.default_rng(seed).normal(0.0, np.sqrt(2.0 / (4 * beta)), L ** 3)
+
+
+def test_chain_alone_equals_chain_in_mix():
+    import gn_b200 as G
+    p = G.Ensemble.params(0.08, 8)
+    L0, b0 = 12, 0.85
+    s0 = _sigma0(L0, b0, 1)
+    with G.Ensemble([L0], [b0], seed=99, stream_ids=[7]) as e:
+        e.load_sigma(0, s0)
+        e.run(p, 5)
+        alone, _ = e.store_sigma(0)
+        st_alone = e.stats()[0]
+    Ls = [8, 16, L0, 24, 8, 12]
+    betas = [0.6, 1.0, b0, 0.7, 1.1, 0.9]
+    ids = [3, 4, 7, 5, 6, 8]
+    for graph in (True, False):
+        with G.Ensemble(Ls, betas, seed=99, stream_ids=ids) as e:
+            for c, (L, b) in enumerate(zip(Ls, betas)):
+                e.load_sigma(c, s0 if c == 2 else _sigma0(L, b, 10 + c))
+            e.run(p, 5, graph=graph)
+            mixed, _ = e.store_sigma(2)
+            st = e.stats()[2]
+            if graph:
+                assert e.info()["graph"] == 1
+        assert np.array_equal(mixed, alone)
+        assert st["accepted"] == st_alone["accepted"] and st["sum_dH"] == st_alone["sum_dH"]
+
+
+def test_ensemble_statistics_vs_reference():
+    import gn_b200 as G
+    ref = json.loads((GOLD / "ensemble_reference_L8.json").read_text())
+    L, nper = ref["L"], 32
+    betas = [float(b) for b in ref["betas"]]
+    Ls = [L] * (nper * len(betas))
+    bet = [b for b in betas for _ in range(nper)]
+    p = G.Ensemble.params(ref["eps"], ref["steps"])
+    n = len(Ls)
+    nchunk, per = 15, 10
+    s2 = np.zeros((n, nchunk))
+    sbar = np.zeros((n, nchunk))
+    acc, emdh = np.zeros(n), np.zeros(n)
+    with G.Ensemble(Ls, bet, seed=2024) as e:
+        for c, b in enumerate(bet):
+            e.load_sigma(c, _sigma0(L, b, 1000 + c))
+        e.run(p, 100)  # thermalisation
+        e.stats(reset=True)
+        for k in range(nchunk):
+            e.run(p, per)
+            st = e.stats(reset=True)
+            assert all(s["failed"] == 0 for s in st)
+            s2[:, k] = [s["sum_sigma2"] / per for s in st]
+            acc += [s["accepted"] for s in st]
+            emdh += [s["sum_exp_mdH"] for s in st]
+            sbar[:, k] = [abs(np.mean(e.store_sigma(c)[0])) for c in range(n)]
+        ntot = nchunk * per
+        sigmas = [e.store_sigma(c)[0] for c in range(n)]
+    # condensate tr1 on each chain's final configuration (single-lattice path,
+    # Z2 noise), oriented by the sign of that configuration's sigma_bar
+    rng = np.random.default_rng(5)
+    cond = []
+    with G.Lattice(L) as lat:
+        for s in sigmas:
+            out, *_ = lat.condensate(lat.sigma_mass(s), 1e-9, np.zeros(L ** 3, complex),
+                                     lambda: float(rng.uniform()))
+            cond.append(out[0] * np.sign(np.mean(s)))
+    cond = np.array(cond)
+    for i, b in enumerate(betas):
+        r = ref["betas"][str(b)]
+        sl = slice(i * nper, (i + 1) * nper)
+        for name, per_chain in (("acceptance", acc[sl] / ntot), ("sigma2", s2[sl].mean(axis=1)),
+                                ("abs_sigma_bar", sbar[sl].mean(axis=1)), ("cond_tr1_oriented", cond[sl])):
+            m, err = per_chain.mean(), per_chain.std(ddof=1) / np.sqrt(nper)
+            tol = 4.0 * np.hypot(err, r[name + "_err"]) + 1e-12
+            assert abs(m - r[name]) <= tol, (b, name, m, err, r[name], r[name + "_err"])
+        m = (emdh[sl] / ntot).mean()
+        err = (emdh[sl] / ntot).std(ddof=1) / np.sqrt(nper)
+        assert abs(m - 1.0) <= 5.0 * err + 1e-5, (b, m, err)
+
+
+def test_autotuner_and_mixed_sizes():
+    """The benchmark's mix of lattice sizes: the tuner returns a valid layout,
+    every chain runs, dH stays small."""
+    import gn_b200 as G
+    rng = np.random.default_rng(3)
+    Ls = [int(x) for x in rng.choice([8, 12, 16, 24, 32, 48], size=24)]
+    bet = list(np.linspace(0.5, 1.2, 24))
+    p = G.Ensemble.params(0.08, 8)
+    with G.Ensemble(Ls, bet, seed=11) as e:
+        for c, (L, b) in enumerate(zip(Ls, bet)):
+            e.load_sigma(c, _sigma0(L, b, c))
+        gs, vmin = e.tune(p)
+        assert gs >= 1
+        e.run(p, 3)
+        st = e.stats()
+    assert all(s["trajectories"] == 3 and s["failed"] == 0 for s in st)
+    assert max(abs(s["last_dH"]) for s in st) < 5.0
+    assert all(s["cg_iterations"] > 0 for s in st)
