@@ -351,6 +351,7 @@ def run_ours(a, world, rank, local):
     # dominant kernel: one two-flavour mixed CG solve, events around the kernel
     roof = kernel_roofline(lat, stream, a, G)
     dirac = dirac_roofline(G, stream, dev)
+    batched = batched_bench(G, dev) if world == 1 else None
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -382,7 +383,8 @@ def run_ours(a, world, rank, local):
             "dirac_roofline": roof_json(dirac, peaks),
             "cpu_baseline": cpu,
             "clocks": mixed["clocks"],
-            "gpu_launches": int(round(mixed["launches"] * a.steps))}
+            "gpu_launches": int(round(mixed["launches"] * a.steps)),
+            "batched": batched}
     if rank == 0:
         print(json.dumps(line), flush=True)
     lat.close()
