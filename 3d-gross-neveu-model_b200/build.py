@@ -32,6 +32,7 @@ UNITS = {
     "noalloc.cu": ["--fmad=false"],
     "exact.cu": ["--fmad=false"],
     "ensemble.cu": ["--fmad=false"],
+    "serve.cu": ["--fmad=false"],
 }
 CORE_LIB = LIB / "libgn_b200.so"
 DROPIN_LIB = LIB / "libgn_dropin.so"

@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "../../include/gn_b200.h"
+#define GN_DEFINE_ENSEMBLE_KERNEL
 #include "ensemble_kernel.cuh"
 #include "errors.h"
 #include "launch.h"
@@ -156,9 +157,13 @@ Ensemble::Ensemble(int n, const int *L, const double *beta_s, const unsigned lon
   check(cudaMemsetAsync(arena_, 0, total, stream_), "memset arena");
   chains_.resize(n);
   for (int c = 0; c < n; c++) carve(static_cast<char *>(arena_) + off[c], c, &chains_[c]);
+  check(cudaMalloc(&d_states_, n * sizeof(EnsState)), "cudaMalloc states");
+  for (int c = 0; c < n; c++) {
+    chains_[c].state = d_states_ + c;
+    chains_[c].op_begin = chains_[c].op_end = 0;
+  }
   check(cudaMalloc(&d_chains_, n * sizeof(EnsChain)), "cudaMalloc chains");
   check(cudaMemcpyAsync(d_chains_, chains_.data(), n * sizeof(EnsChain), cudaMemcpyHostToDevice, stream_), "copy");
-  check(cudaMalloc(&d_states_, n * sizeof(EnsState)), "cudaMalloc states");
   check(cudaMemsetAsync(d_states_, 0, n * sizeof(EnsState), stream_), "memset states");
   check(cudaMalloc(&d_order_, n * sizeof(int)), "cudaMalloc order");
   check(cudaMalloc(&d_queue_, kMaxNodes * 2 * sizeof(int)), "cudaMalloc queue");
@@ -298,7 +303,6 @@ Ensemble::Plan &Ensemble::plan_for(const gn_ens_params &p) {
 void Ensemble::launch_node(const Plan &pl, int k, double tol) {
   EnsLaunch a;
   a.chains = d_chains_;
-  a.states = d_states_;
   a.nchains = n_;
   a.order = d_order_;
   a.nbig = nbig_;

@@ -30,7 +30,10 @@ enum EnsOpCode : int {
   E_Q,            // sigma += c P, sm recomputed
   E_ENERGY0,      // H0
   E_ENERGY1,      // H1
-  E_METROPOLIS    // accept if u <= exp(-(H1 - H0)), else restore sigma; statistics
+  E_METROPOLIS,   // accept if u <= exp(-(H1 - H0)), else restore sigma; statistics
+  E_RHS,          // phi_0 ~ N(0, 1), phi_1 = 0 (a solve request's right-hand side)
+  E_Z2,           // phi_0, phi_1 = Z2 noise vectors 2c, 2c+1 of the request
+  E_TRACE         // Y_f = M^T X_f; result += sum_f phi_f . Y_f / V (condensate estimate)
 };
 
 struct EnsOp {
@@ -38,8 +41,12 @@ struct EnsOp {
   double c;
 };
 
+struct EnsState;
+
 // One chain's arrays (device pointers, 256-byte aligned) and constants.
 struct EnsChain {
+  struct EnsState *state;     // the chain's mutable state
+  int op_begin, op_end;       // the chain's own op range (used when the launch gives none)
   Geom g;
   int w;  // sites per FP32 item (4, 2 or 1); the FP64 sweeps use min(w, 2)
   double beta_s;
@@ -61,16 +68,18 @@ struct EnsState {
   long long n, nacc, iters, reliable, fails;
   double sum_dH, sum_exp_mdH, sum_sigma2, last_dH;
   int last_acc;
+  // the current request of a served chain
+  unsigned long long serial;  // Philox counter of the request's draws
+  double result;              // E_TRACE accumulator
 };
 
 struct EnsLaunch {
   const EnsChain *chains;
-  EnsState *states;
   int nchains;
   const int *order;  // chain indices: the nbig big chains first, all by decreasing volume
   int nbig;
   const EnsOp *ops;
-  int op_begin, op_end;
+  int op_begin, op_end;  // op range of every chain; op_begin < 0: each chain's own
   int gs;             // blocks per group (big chains)
   int *queue;         // [2] next big / next small task; zero before the launch
   PhaseBar *bars;     // [groups] team barrier counters; zero before the launch
@@ -118,9 +127,11 @@ __device__ __forceinline__ void box_muller(uint64_t a, uint64_t b, double &z0, d
 }
 
 // The chain's ops [op_begin, op_end) by team t.  Returns false on a barrier timeout.
-__device__ __noinline__ bool ens_run_chain(const EnsLaunch &L, int c, Team &t, SyncShared &sh, MixedShared &ms) {
+static __device__ __noinline__ bool ens_run_chain(const EnsLaunch &L, int c, Team &t, SyncShared &sh, MixedShared &ms) {
   const EnsChain &ch = L.chains[c];
-  EnsState *st = L.states + c;
+  EnsState *st = ch.state;
+  const int op_begin = L.op_begin >= 0 ? L.op_begin : ch.op_begin;
+  const int op_end = L.op_begin >= 0 ? L.op_end : ch.op_end;
   const Geom g = ch.g;
   const uint32_t V = uint32_t(g.V);
   const bool leader = t.brank == 0 && threadIdx.x == 0;
@@ -130,7 +141,7 @@ __device__ __noinline__ bool ens_run_chain(const EnsLaunch &L, int c, Team &t, S
 #pragma unroll
     for (int q = 0; q < kSyncQ; q++) acc[q] = 0.0;
   };
-  for (int o = L.op_begin; o < L.op_end; o++) {
+  for (int o = op_begin; o < op_end; o++) {
     const EnsOp op = L.ops[o];
     double *const sig = ch.sigma[cur];
     double *const sig_o = ch.sigma[cur ^ 1];
@@ -171,7 +182,7 @@ __device__ __noinline__ bool ens_run_chain(const EnsLaunch &L, int c, Team &t, S
         a.th[k] = ch.th + size_t(kk) * V;
         a.xh[k] = ch.xh + size_t(kk) * V;
       }
-      a.nrhs = 2;
+      a.nrhs = op.c > 0.0 ? int(op.c) : 2;
       a.variant = 1;
       a.rel = 1;
       a.tol = L.tol;
@@ -187,7 +198,7 @@ __device__ __noinline__ bool ens_run_chain(const EnsLaunch &L, int c, Team &t, S
       else if (ch.w == 2) ens_solve<2>(a, t, sh, ms);
       else ens_solve<1>(a, t, sh, ms);
       if (leader) {
-        for (int k = 0; k < 2; k++) {
+        for (int k = 0; k < a.nrhs; k++) {
           const int s = ms.status[k];
           if (s != kCgConverged && s != kCgConvergedStart) st->failed = 1;
           st->iters += (s == kCgConverged) ? ms.iters[k] : 0;
@@ -251,6 +262,42 @@ __device__ __noinline__ bool ens_run_chain(const EnsLaunch &L, int c, Team &t, S
         st->last_acc = accept;
         st->ntraj++;
       }
+    } else if (op.code == E_RHS) {
+      const unsigned long long serial = st->serial;
+      for (uint32_t q = t.tid; q < V / 4u; q += t.nthreads) {
+        const Philox4x64 r = phx_draw(L.seed, ch.stream, serial, kPhxRhs, q);
+        double z[4];
+        box_muller(r.v[0], r.v[1], z[0], z[1]);
+        box_muller(r.v[2], r.v[3], z[2], z[3]);
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          ch.phi[4 * q + e] = z[e];
+          ch.phi[V + 4 * q + e] = 0.0;
+        }
+      }
+      if (leader) st->failed = 0;
+      ok = end_phase<0>(acc, sh, t);
+    } else if (op.code == E_Z2) {
+      // one Philox block gives the signs of 256 sites: noise vector n, block q
+      const unsigned long long serial = st->serial;
+      const int n0 = 2 * int(op.c);
+      for (uint32_t u = t.tid; u < 2u * V; u += t.nthreads) {
+        const uint32_t f = u >= V ? 1u : 0u, i = u - f * V;
+        const Philox4x64 r = phx_draw(L.seed, ch.stream, serial, kPhxZ2 + uint64_t(n0 + int(f)), i >> 8);
+        const uint64_t bits = r.v[(i >> 6) & 3u];
+        ch.phi[u] = ((bits >> (i & 63u)) & 1ull) ? 1.0 : -1.0;
+      }
+      if (leader) st->failed = 0;
+      ok = end_phase<0>(acc, sh, t);
+    } else if (op.code == E_TRACE) {
+      // tr M^{-1} estimate of condensate.c:142-145 for two real noise vectors:
+      // xi . M^T (M M^T)^-1 xi / V
+      if (ch.w >= 2) team_dirac2<2, 1>(g, t, ch.sm, ch.X, ch.Y);
+      else team_dirac2<1, 1>(g, t, ch.sm, ch.X, ch.Y);
+      ok = end_phase<0>(acc, sh, t);
+      for (uint32_t u = t.tid; u < 2u * V; u += t.nthreads) acc[0] += ch.phi[u] * ch.Y[u];
+      ok = end_phase<1>(acc, sh, t) && ok;
+      if (leader) st->result += sh.val[0] / double(V);
     }
     if (!ok) return false;
   }
@@ -259,6 +306,11 @@ __device__ __noinline__ bool ens_run_chain(const EnsLaunch &L, int c, Team &t, S
   return true;
 }
 
+// Defined in one translation unit (ensemble.cu, which sets
+// GN_DEFINE_ENSEMBLE_KERNEL); the others launch it through this declaration.
+__global__ void __launch_bounds__(kEnsThreads, 1) ens_node_kernel(EnsLaunch L);
+
+#ifdef GN_DEFINE_ENSEMBLE_KERNEL
 __global__ void __launch_bounds__(kEnsThreads, 1) ens_node_kernel(EnsLaunch L) {
   __shared__ SyncShared sh;
   __shared__ MixedShared ms;
@@ -307,5 +359,6 @@ __global__ void __launch_bounds__(kEnsThreads, 1) ens_node_kernel(EnsLaunch L) {
     if (!ens_run_chain(L, L.order[task], bt, sh, ms)) return;
   }
 }
+#endif
 
 }  // namespace gn

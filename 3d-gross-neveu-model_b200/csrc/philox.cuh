@@ -63,7 +63,17 @@ GN_PHX_HD double phx_unit_open0(uint64_t x) { return double((x >> 11) + 1ull) * 
 GN_PHX_HD double phx_unit(uint64_t x) { return double(x >> 11) * (1.0 / 9007199254740992.0); }
 
 // Streams of one chain: what a counter's words mean.
-enum PhxField : uint64_t { kPhxMomenta = 0, kPhxChi0 = 1, kPhxChi1 = 2, kPhxMetropolis = 3 };
+// (Trajectory draws take the chain's trajectory number as the counter word;
+// a served request's own draws take its serial number: a solve's right-hand
+// side, and Z2 noise vector n at kPhxZ2 + n.)
+enum PhxField : uint64_t {
+  kPhxMomenta = 0,
+  kPhxChi0 = 1,
+  kPhxChi1 = 2,
+  kPhxMetropolis = 3,
+  kPhxRhs = 4,
+  kPhxZ2 = 16
+};
 
 // Four random words for (field, block) of trajectory `traj` of the chain with
 // key (seed, chain).

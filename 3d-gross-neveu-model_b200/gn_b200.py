@@ -72,6 +72,18 @@ class ChainStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class ReqInfo(C.Structure):
+    _fields_ = [("id", C.c_longlong), ("type", C.c_int), ("status", C.c_int), ("chain", C.c_int),
+                ("noise_vectors", C.c_int), ("failed", C.c_int), ("accepted", C.c_int), ("t_arrival", C.c_double),
+                ("t_admit", C.c_double), ("t_done", C.c_double), ("dH", C.c_double), ("value", C.c_double),
+                ("cg_iterations", C.c_longlong)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+GN_REQ_TRAJECTORY, GN_REQ_SOLVE, GN_REQ_CONDENSATE = 0, 1, 2
+
 _dp = C.POINTER(C.c_double)
 _lib = None
 
@@ -131,6 +143,17 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
         "gn_ensemble_run": ([v, C.POINTER(EnsParams), C.c_int, C.c_int], C.c_int),
         "gn_ensemble_stats": ([v, C.POINTER(ChainStats), C.c_int], C.c_int),
         "gn_ensemble_stream": ([v], C.c_void_p),
+        "gn_server_create": ([C.POINTER(v), C.POINTER(EnsParams), C.c_double, C.c_ulonglong, C.c_int,
+                              C.c_longlong, C.c_int], C.c_int),
+        "gn_server_destroy": ([v], None),
+        "gn_server_add_chain": ([v, C.c_int, C.c_double, _dp, C.c_ulonglong], C.c_int),
+        "gn_server_clock": ([v], C.c_double),
+        "gn_server_submit": ([v, C.c_int, C.c_int, C.c_int, C.c_double], C.c_longlong),
+        "gn_server_step": ([v, C.POINTER(C.c_int)], C.c_int),
+        "gn_server_request": ([v, C.c_longlong, C.POINTER(ReqInfo)], C.c_int),
+        "gn_server_solution": ([v, C.c_longlong, _dp], C.c_int),
+        "gn_server_chain_sigma": ([v, C.c_int, _dp], C.c_int),
+        "gn_server_load": ([v, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_longlong)], C.c_int),
         "gn_ensemble_info": ([v, C.POINTER(C.c_int), C.POINTER(C.c_longlong), C.POINTER(C.c_int),
                               C.POINTER(C.c_int)], C.c_int),
     }
@@ -434,3 +457,83 @@ class Ensemble:
         self._check(self.lib.gn_ensemble_info(self.ens, C.byref(gs), C.byref(vmin), C.byref(g), C.byref(nl)))
         return {"group_blocks": gs.value, "big_min_volume": vmin.value, "graph": g.value,
                 "launches_per_trajectory": nl.value}
+
+
+class Server:
+    """Requests on resident chains with continuous batching (gn_server_* of gn_b200.h)."""
+
+    def __init__(self, traj_params, mem_budget_bytes=8e9, seed=1231, group_blocks=4, big_min_volume=4096, device=0):
+        self.lib = load_library()
+        self.srv = C.c_void_p()
+        self._check(self.lib.gn_server_create(C.byref(self.srv), C.byref(traj_params), float(mem_budget_bytes),
+                                              int(seed), group_blocks, big_min_volume, device))
+        self.Ls = []
+
+    def _check(self, st, allow=(GN_OK,)):
+        if st not in allow:
+            raise GnError(st, self.lib.gn_last_error().decode())
+        return st
+
+    def close(self):
+        if self.srv:
+            self.lib.gn_server_destroy(self.srv)
+            self.srv = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def add_chain(self, L, beta_s, sigma, stream_id):
+        s = np.ascontiguousarray(sigma, np.float64)
+        c = self.lib.gn_server_add_chain(self.srv, int(L), float(beta_s), _p(s), int(stream_id))
+        if c < 0:
+            raise GnError(c, self.lib.gn_last_error().decode())
+        self.Ls.append(int(L))
+        return c
+
+    def clock(self):
+        return self.lib.gn_server_clock(self.srv)
+
+    def submit(self, chain, rtype, noise_vectors=0, t_arrival=None):
+        t = self.clock() if t_arrival is None else float(t_arrival)
+        rid = self.lib.gn_server_submit(self.srv, int(chain), int(rtype), int(noise_vectors), t)
+        if rid < 0:
+            raise GnError(int(rid), self.lib.gn_last_error().decode())
+        return rid
+
+    def step(self):
+        n = C.c_int()
+        self._check(self.lib.gn_server_step(self.srv, C.byref(n)))
+        return n.value
+
+    def request(self, rid):
+        r = ReqInfo()
+        self._check(self.lib.gn_server_request(self.srv, int(rid), C.byref(r)))
+        return r.as_dict()
+
+    def solution(self, rid):
+        info = self.request(rid)
+        x = np.empty(self.Ls[info["chain"]] ** 3)
+        self._check(self.lib.gn_server_solution(self.srv, int(rid), _p(x)))
+        return x
+
+    def chain_sigma(self, c):
+        s = np.empty(self.Ls[c] ** 3)
+        self._check(self.lib.gn_server_chain_sigma(self.srv, int(c), _p(s)))
+        return s
+
+    def load(self):
+        r, q, b = C.c_int(), C.c_int(), C.c_longlong()
+        self._check(self.lib.gn_server_load(self.srv, C.byref(r), C.byref(q), C.byref(b)))
+        return {"running": r.value, "queued": q.value, "bytes_in_use": b.value}
+
+    def drain(self, max_steps=100000):
+        """Steps until nothing is running or queued."""
+        for _ in range(max_steps):
+            ld = self.load()
+            if ld["running"] == 0 and ld["queued"] == 0:
+                return
+            self.step()
+        raise RuntimeError("server did not drain")

@@ -302,6 +302,62 @@ GN_API void *gn_ensemble_stream(gn_ensemble *ens);
 GN_API int gn_ensemble_info(gn_ensemble *ens, int *group_blocks, long long *big_min_volume, int *graph_used,
                             int *launches_per_trajectory);
 
+/* ---- serving ------------------------------------------------------------- */
+
+/* No counterpart in the reference.  A server keeps chains resident on the GPU
+ * (sigma and its mass) and runs requests on them with continuous batching:
+ *   GN_REQ_TRAJECTORY  one HMC trajectory of the chain (the ensemble's: the
+ *                      parameters given at creation, mixed-precision solves);
+ *   GN_REQ_SOLVE       one solve of (M M^T) x = b at the chain's sigma, b ~ N(0, 1);
+ *   GN_REQ_CONDENSATE  the estimate (1/n) sum_k xi_k . M^T (M M^T)^-1 xi_k / V
+ *                      of tr M^-1 / V (condensate.c:142-145) from n Z2 vectors.
+ * gn_server_step launches the batched kernel once: every running request
+ * advances by one slice (a trajectory has one per MD step, a solve one, a
+ * condensate one per two noise vectors), finished requests retire, and queued
+ * ones are admitted in arrival order when their chain is free and their work
+ * arrays (about 148 bytes per site) fit the memory budget.  A request's draws
+ * come from its chain's Philox stream with its number among the chain's
+ * requests (trajectories: the chain's trajectory number) as the counter, so its
+ * result does not depend on the requests running beside it.  Times are seconds on the server's clock
+ * (gn_server_clock). */
+typedef struct gn_server gn_server;
+
+enum gn_request_type { GN_REQ_TRAJECTORY = 0, GN_REQ_SOLVE = 1, GN_REQ_CONDENSATE = 2 };
+
+typedef struct {
+  long long id;
+  int type;           /* gn_request_type */
+  int status;         /* 0 queued, 1 running, 2 done */
+  int chain;
+  int noise_vectors;  /* condensate requests */
+  int failed;         /* a solve did not converge (a trajectory is then rejected) */
+  int accepted;       /* trajectory */
+  double t_arrival, t_admit, t_done;
+  double dH;          /* trajectory */
+  double value;       /* condensate estimate */
+  long long cg_iterations;
+} gn_request_info;
+
+/* traj: the trajectories' integrator, steps, step size and the tolerance of
+ * every solve.  mem_budget_bytes bounds the running requests' work arrays.
+ * Chains with V >= big_min_volume run on groups of group_blocks blocks. */
+GN_API int gn_server_create(gn_server **srv, const gn_ens_params *traj, double mem_budget_bytes,
+                            unsigned long long seed, int group_blocks, long long big_min_volume, int device);
+GN_API void gn_server_destroy(gn_server *srv);
+/* A resident chain: returns its index (>= 0) or a negative status. */
+GN_API int gn_server_add_chain(gn_server *srv, int L, double beta_s, const double *sigma,
+                               unsigned long long stream_id);
+GN_API double gn_server_clock(gn_server *srv);
+/* Queues a request (noise_vectors: condensate only, even, 2..64); returns its id or a negative status. */
+GN_API long long gn_server_submit(gn_server *srv, int chain, int type, int noise_vectors, double t_arrival);
+/* One step of the server; *completed = requests finished in it. */
+GN_API int gn_server_step(gn_server *srv, int *completed);
+GN_API int gn_server_request(gn_server *srv, long long id, gn_request_info *out);
+/* A finished solve's x (V doubles). */
+GN_API int gn_server_solution(gn_server *srv, long long id, double *x);
+GN_API int gn_server_chain_sigma(gn_server *srv, int chain, double *sigma);
+GN_API int gn_server_load(gn_server *srv, int *running, int *queued, long long *bytes_in_use);
+
 #ifdef __cplusplus
 }
 #endif
