@@ -73,8 +73,8 @@ class Ensemble {
   EnsChain *d_chains_ = nullptr;
   EnsState *d_states_ = nullptr;
   int *d_order_ = nullptr;
-  int *d_queue_ = nullptr;      // [kMaxNodes][2]
-  PhaseBar *d_bars_ = nullptr;  // [kMaxNodes][capacity]
+  int *d_queue_ = nullptr;      // [kMaxNodes][kMaxTiers]
+  PhaseBar *d_bars_ = nullptr;  // [kMaxNodes][kMaxTiers][capacity]
   double *d_partials_ = nullptr;
   CgState *d_cg_state_ = nullptr;
   int *d_err_ = nullptr;
@@ -166,9 +166,10 @@ Ensemble::Ensemble(int n, const int *L, const double *beta_s, const unsigned lon
   check(cudaMemcpyAsync(d_chains_, chains_.data(), n * sizeof(EnsChain), cudaMemcpyHostToDevice, stream_), "copy");
   check(cudaMemsetAsync(d_states_, 0, n * sizeof(EnsState), stream_), "memset states");
   check(cudaMalloc(&d_order_, n * sizeof(int)), "cudaMalloc order");
-  check(cudaMalloc(&d_queue_, kMaxNodes * 2 * sizeof(int)), "cudaMalloc queue");
-  check(cudaMalloc(&d_bars_, size_t(kMaxNodes) * capacity_ * sizeof(PhaseBar)), "cudaMalloc bars");
-  check(cudaMalloc(&d_partials_, size_t(capacity_) * 2 * (kSyncQ + 1) * sizeof(double)), "cudaMalloc partials");
+  check(cudaMalloc(&d_queue_, kMaxNodes * kMaxTiers * sizeof(int)), "cudaMalloc queue");
+  check(cudaMalloc(&d_bars_, size_t(kMaxNodes) * kMaxTiers * capacity_ * sizeof(PhaseBar)), "cudaMalloc bars");
+  check(cudaMalloc(&d_partials_, size_t(kMaxTiers) * capacity_ * 2 * (kSyncQ + 1) * sizeof(double)),
+        "cudaMalloc partials");
   check(cudaMalloc(&d_cg_state_, size_t(capacity_) * kMaxRhs * sizeof(CgState)), "cudaMalloc cg state");
   check(cudaMalloc(&d_err_, sizeof(int)), "cudaMalloc err");
   check(cudaMemsetAsync(d_err_, 0, sizeof(int), stream_), "memset err");
@@ -305,13 +306,22 @@ void Ensemble::launch_node(const Plan &pl, int k, double tol) {
   a.chains = d_chains_;
   a.nchains = n_;
   a.order = d_order_;
-  a.nbig = nbig_;
+  if (gs_ > 1 && nbig_ > 0) {  // the big chains on teams of gs_ blocks, the rest on single blocks
+    a.ntier = 2;
+    a.tier_gs[0] = gs_;
+    a.tier_end[0] = nbig_;
+    a.tier_gs[1] = 1;
+    a.tier_end[1] = n_;
+  } else {
+    a.ntier = 1;
+    a.tier_gs[0] = 1;
+    a.tier_end[0] = n_;
+  }
   a.ops = pl.d_ops;
   a.op_begin = pl.node_begin[k];
   a.op_end = pl.node_begin[k + 1];
-  a.gs = gs_;
-  a.queue = d_queue_ + 2 * k;
-  a.bars = d_bars_ + size_t(k) * capacity_;
+  a.queue = d_queue_ + kMaxTiers * k;
+  a.bars = d_bars_ + size_t(k) * kMaxTiers * capacity_;
   a.partials = d_partials_;
   a.cg_state = d_cg_state_;
   a.err = d_err_;
@@ -319,9 +329,8 @@ void Ensemble::launch_node(const Plan &pl, int k, double tol) {
   a.tol = tol;
   a.delta = kEnsDelta;
   a.n_ru = kEnsReliableEvery;
-  const int groups = capacity_ / gs_;
   void *args[] = {(void *)&a};
-  check(cudaLaunchCooperativeKernel((const void *)ens_node_kernel, dim3(groups * gs_), dim3(kEnsThreads), args, 0,
+  check(cudaLaunchCooperativeKernel((const void *)ens_node_kernel, dim3(capacity_), dim3(kEnsThreads), args, 0,
                                     stream_),
         "ens_node_kernel launch");
 }
@@ -329,8 +338,9 @@ void Ensemble::launch_node(const Plan &pl, int k, double tol) {
 // One trajectory of every chain: zero the slices' queues and barriers, then the slices.
 void Ensemble::enqueue_trajectory(const Plan &pl, double tol) {
   const int nodes = int(pl.node_begin.size()) - 1;
-  check(cudaMemsetAsync(d_queue_, 0, size_t(nodes) * 2 * sizeof(int), stream_), "memset queue");
-  check(cudaMemsetAsync(d_bars_, 0, size_t(nodes) * capacity_ * sizeof(PhaseBar), stream_), "memset bars");
+  check(cudaMemsetAsync(d_queue_, 0, size_t(nodes) * kMaxTiers * sizeof(int), stream_), "memset queue");
+  check(cudaMemsetAsync(d_bars_, 0, size_t(nodes) * kMaxTiers * capacity_ * sizeof(PhaseBar), stream_),
+        "memset bars");
   for (int k = 0; k < nodes; k++) launch_node(pl, k, tol);
 }
 
@@ -401,8 +411,8 @@ void Ensemble::tune(const gn_ens_params &p, int *gs_out, long long *big_out) {
     set_layout(cd.first, cd.second);
     float ms = 0.f;
     for (int rep = 0; rep < 2; rep++) {  // the first launch warms up; the second is timed
-      check(cudaMemsetAsync(d_queue_, 0, 2 * sizeof(int), stream_), "memset queue");
-      check(cudaMemsetAsync(d_bars_, 0, size_t(capacity_) * sizeof(PhaseBar), stream_), "memset bars");
+      check(cudaMemsetAsync(d_queue_, 0, kMaxTiers * sizeof(int), stream_), "memset queue");
+      check(cudaMemsetAsync(d_bars_, 0, size_t(kMaxTiers) * capacity_ * sizeof(PhaseBar), stream_), "memset bars");
       check(cudaEventRecord(e0, stream_), "record");
       launch_node(pl, 0, p.tol);
       check(cudaEventRecord(e1, stream_), "record");

@@ -2,10 +2,13 @@
 // sizes in one persistent kernel per slice of a trajectory.
 //
 // A launch runs one slice of the trajectory's op list (an MD step, or the
-// refresh / initial solve / energy at either end) for every chain.  Chains are
-// taken from a work queue in order of decreasing volume: the big ones by
-// groups of gs blocks that synchronise with a team barrier (phase_sync.cuh),
-// the small ones by single blocks that need only __syncthreads.  Every chain's
+// refresh / initial solve / energy at either end) for every chain.  Chains
+// come in tiers, each taken from its own work queue, largest first: a tier's
+// chains run on teams of that tier's size, groups of blocks that synchronise
+// with a team barrier (phase_sync.cuh); the last tier's on single blocks that
+// need only __syncthreads.  Tier sizes divide each other (e.g. 16, 4, 1), so a
+// block's team in a later tier lies inside its team of the earlier one and no
+// block waits on a block outside its current team.  Every chain's
 // work is a fixed sequence of team phases, so every block of a team takes the
 // same branches.  Momenta, pseudofermion sources and the Metropolis uniform
 // come from the chain's own Philox stream (philox.cuh) with the trajectory
@@ -19,6 +22,7 @@
 namespace gn {
 
 constexpr int kEnsThreads = 1024;
+constexpr int kMaxTiers = 4;
 
 // Ops of the batched trajectory (the schedule of schedule.h, translated).
 enum EnsOpCode : int {
@@ -76,14 +80,15 @@ struct EnsState {
 struct EnsLaunch {
   const EnsChain *chains;
   int nchains;
-  const int *order;  // chain indices: the nbig big chains first, all by decreasing volume
-  int nbig;
+  const int *order;  // chain indices, tier by tier
+  int ntier;
+  int tier_gs[kMaxTiers];   // blocks per team of tier t (decreasing; each divides the previous)
+  int tier_end[kMaxTiers];  // tier t runs order[tier_end[t-1] .. tier_end[t])
   const EnsOp *ops;
   int op_begin, op_end;  // op range of every chain; op_begin < 0: each chain's own
-  int gs;             // blocks per group (big chains)
-  int *queue;         // [2] next big / next small task; zero before the launch
-  PhaseBar *bars;     // [groups] team barrier counters; zero before the launch
-  double *partials;   // [groups][2][kSyncQ + 1][gs]
+  int *queue;         // [kMaxTiers] next task of each tier; zero before the launch
+  PhaseBar *bars;     // [kMaxTiers][gridDim.x] team barrier counters; zero before the launch
+  double *partials;   // [kMaxTiers][gridDim.x][2][kSyncQ + 1]
   CgState *cg_state;  // [gridDim.x][kMaxRhs] solver status scratch
   int *err;
   unsigned long long seed;
@@ -315,48 +320,54 @@ __global__ void __launch_bounds__(kEnsThreads, 1) ens_node_kernel(EnsLaunch L) {
   __shared__ SyncShared sh;
   __shared__ MixedShared ms;
   __shared__ int s_task;
-  const int gs = L.gs;
-  const int group = int(blockIdx.x) / gs, grank = int(blockIdx.x) % gs;
-  // ---- big chains: a group of gs blocks each
-  if (gs > 1 && L.nbig > 0) {
-    Team gt;
-    gt.tid = uint32_t(grank) * blockDim.x + threadIdx.x;
-    gt.nthreads = uint32_t(gs) * blockDim.x;
-    gt.brank = grank;
-    gt.nblocks = gs;
-    gt.bar = L.bars + group;
-    gt.partials = L.partials + size_t(group) * 2 * (kSyncQ + 1) * gs;
-    gt.err = L.err;
-    gt.nph = 0;
-    for (;;) {
-      int task = 0;
-      if (grank == 0 && threadIdx.x == 0) task = atomicAdd(&L.queue[0], 1);
-      double acc[kSyncQ];
+  int tb = 0;  // first order index of the tier
+  for (int tier = 0; tier < L.ntier; tier++) {
+    const int gs = L.tier_gs[tier], te = L.tier_end[tier];
+    if (gs > 1) {
+      // teams of gs blocks; blocks beyond the last whole team go straight on
+      const int group = int(blockIdx.x) / gs, grank = int(blockIdx.x) % gs;
+      if (group < int(gridDim.x) / gs && te > tb) {
+        Team gt;
+        gt.tid = uint32_t(grank) * blockDim.x + threadIdx.x;
+        gt.nthreads = uint32_t(gs) * blockDim.x;
+        gt.brank = grank;
+        gt.nblocks = gs;
+        gt.bar = L.bars + size_t(tier) * gridDim.x + group;
+        gt.partials = L.partials + (size_t(tier) * gridDim.x + size_t(group) * gs) * 2 * (kSyncQ + 1);
+        gt.err = L.err;
+        gt.nph = 0;
+        for (;;) {
+          int task = 0;
+          if (grank == 0 && threadIdx.x == 0) task = tb + atomicAdd(&L.queue[tier], 1);
+          double acc[kSyncQ];
 #pragma unroll
-      for (int q = 0; q < kSyncQ; q++) acc[q] = 0.0;
-      if (!end_phase<0>(acc, sh, gt, task)) return;  // the group leader's task, to every block
-      task = sh.flag;
-      if (task >= L.nbig) break;
-      if (!ens_run_chain(L, L.order[task], gt, sh, ms)) return;
+          for (int q = 0; q < kSyncQ; q++) acc[q] = 0.0;
+          if (!end_phase<0>(acc, sh, gt, task)) return;  // the team leader's task, to every block
+          task = sh.flag;
+          if (task >= te) break;
+          if (!ens_run_chain(L, L.order[task], gt, sh, ms)) return;
+        }
+      }
+    } else {
+      Team bt;
+      bt.tid = threadIdx.x;
+      bt.nthreads = blockDim.x;
+      bt.brank = 0;
+      bt.nblocks = 1;
+      bt.bar = nullptr;
+      bt.partials = nullptr;
+      bt.err = L.err;
+      bt.nph = 0;
+      for (;;) {
+        if (threadIdx.x == 0) s_task = tb + atomicAdd(&L.queue[tier], 1);
+        __syncthreads();
+        const int task = s_task;
+        __syncthreads();
+        if (task >= te) break;
+        if (!ens_run_chain(L, L.order[task], bt, sh, ms)) return;
+      }
     }
-  }
-  // ---- small chains: one block each
-  Team bt;
-  bt.tid = threadIdx.x;
-  bt.nthreads = blockDim.x;
-  bt.brank = 0;
-  bt.nblocks = 1;
-  bt.bar = nullptr;
-  bt.partials = nullptr;
-  bt.err = L.err;
-  bt.nph = 0;
-  for (;;) {
-    if (threadIdx.x == 0) s_task = L.nbig + atomicAdd(&L.queue[1], 1);
-    __syncthreads();
-    const int task = s_task;
-    __syncthreads();
-    if (task >= L.nchains) break;
-    if (!ens_run_chain(L, L.order[task], bt, sh, ms)) return;
+    tb = te;
   }
 }
 #endif

@@ -36,7 +36,8 @@ constexpr int kMaxNoise = 64;  // Z2 vectors of one condensate request
 
 class Server {
  public:
-  Server(const gn_ens_params &traj, size_t budget, unsigned long long seed, int gs, long long big_min, int device);
+  Server(const gn_ens_params &traj, size_t budget, unsigned long long seed, int ntier, const int *tier_blocks,
+         const long long *tier_min_volume, int device);
   ~Server();
   int device() const { return device_; }
   int add_chain(int L, double beta, const double *sigma, unsigned long long stream_id);
@@ -64,10 +65,11 @@ class Server {
   };
   struct Program {  // slices [node_begin[k], node_begin[k + 1]) of the op array
     std::vector<int> node_begin;
+    std::vector<int> solves;  // solves in slice k
   };
   struct Req {
     gn_request_info info;
-    int nslices = 0, next = 0;
+    int nslices = 0, next = 0, take = 1;  // slices done; slices this step
     const Program *prog = nullptr;
     long long iters0 = 0;       // the chain's solver iteration count at admission
     unsigned long long serial;  // the request's number on its chain: the Philox counter of its draws
@@ -83,8 +85,14 @@ class Server {
   static double *work_X(const Req &r, size_t V);
   void admit();
 
-  int device_ = 0, capacity_ = 0, gs_ = 4;
-  long long big_min_ = 4096;
+  int device_ = 0, capacity_ = 0;
+  std::vector<int> tier_gs_;          // team sizes, decreasing; the last tier (single blocks) is implicit
+  std::vector<long long> tier_min_;   // a chain with V >= tier_min_[t] (and below the earlier tiers) runs in tier t
+  int tier_of(long long V) const {
+    for (size_t t = 0; t < tier_min_.size(); t++)
+      if (V >= tier_min_[t]) return int(t);
+    return int(tier_gs_.size());
+  }
   size_t budget_ = 0, in_use_ = 0;
   unsigned long long seed_ = 0;
   double tol_ = 1e-10;
@@ -119,9 +127,9 @@ size_t Server::work_bytes(size_t V) {
   return 3 * round256(V * 8) + 5 * round256(2 * V * 8) + round256(V * 4) + 4 * round256(2 * V * 4);
 }
 
-Server::Server(const gn_ens_params &traj, size_t budget, unsigned long long seed, int gs, long long big_min,
-               int device)
-    : device_(device), gs_(gs), big_min_(big_min), budget_(budget), seed_(seed), tol_(traj.tol) {
+Server::Server(const gn_ens_params &traj, size_t budget, unsigned long long seed, int ntier, const int *tier_blocks,
+               const long long *tier_min_volume, int device)
+    : device_(device), budget_(budget), seed_(seed), tol_(traj.tol) {
   if (traj.steps < 1 || traj.integrator < 0 || traj.integrator > 2 || !(traj.tol > 0.0))
     throw GnError(GN_ERR_ARG, "bad trajectory parameters");
   int ndev = 0;
@@ -134,7 +142,17 @@ Server::Server(const gn_ens_params &traj, size_t budget, unsigned long long seed
   check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
   capacity_ = coop_capacity((const void *)ens_node_kernel, kEnsThreads);
   if (capacity_ < 1) throw GnError(GN_ERR_CUDA, "the batched kernel cannot be resident as a cooperative grid");
-  if (gs_ < 1 || gs_ > capacity_) throw GnError(GN_ERR_ARG, "blocks per group out of range");
+  // team tiers: sizes > 1, decreasing, each dividing the previous one (so a
+  // block's team in a later tier lies inside its team of the earlier one)
+  if (ntier < 0 || ntier > kMaxTiers - 1) throw GnError(GN_ERR_ARG, "0 to 3 team tiers");
+  for (int t = 0; t < ntier; t++) {
+    const int gs = tier_blocks[t];
+    if (gs < 2 || gs > capacity_ || (t > 0 && tier_blocks[t - 1] % gs != 0) ||
+        (t > 0 && tier_min_volume[t] > tier_min_volume[t - 1]))
+      throw GnError(GN_ERR_ARG, "team tiers: sizes >= 2, each dividing the previous, volumes decreasing");
+    tier_gs_.push_back(gs);
+    tier_min_.push_back(tier_min_volume[t]);
+  }
   // ---- programs: the trajectory (sliced like the ensemble's), a solve, a condensate
   traj_.node_begin = {0};
   ops_ = {{E_REFRESH, 0.0}, {E_PHI, 0.0}, {E_SOLVE, 0.0}, {E_ENERGY0, 0.0}};
@@ -183,6 +201,13 @@ Server::Server(const gn_ens_params &traj, size_t budget, unsigned long long seed
     ops_.push_back({E_TRACE, 0.0});
     cond_.node_begin.push_back(int(ops_.size()));
   }
+  for (Program *pg : {&traj_, &solve_, &cond_}) {
+    for (size_t k = 0; k + 1 < pg->node_begin.size(); k++) {
+      int n = 0;
+      for (int o = pg->node_begin[k]; o < pg->node_begin[k + 1]; o++) n += ops_[o].code == E_SOLVE;
+      pg->solves.push_back(n);
+    }
+  }
   check(cudaMalloc(&d_ops_, ops_.size() * sizeof(EnsOp)), "cudaMalloc ops");
   check(cudaMemcpyAsync(d_ops_, ops_.data(), ops_.size() * sizeof(EnsOp), cudaMemcpyHostToDevice, stream_), "copy");
   check(cudaMalloc(&d_states_, kMaxChains * sizeof(EnsState)), "cudaMalloc states");
@@ -192,9 +217,10 @@ Server::Server(const gn_ens_params &traj, size_t budget, unsigned long long seed
   check(cudaHostAlloc((void **)&h_states_, kMaxChains * sizeof(EnsState), cudaHostAllocDefault), "cudaHostAlloc");
   memset(h_states_, 0, kMaxChains * sizeof(EnsState));
   check(cudaMalloc(&d_order_, kMaxChains * sizeof(int)), "cudaMalloc order");
-  check(cudaMalloc(&d_queue_, 2 * sizeof(int)), "cudaMalloc queue");
-  check(cudaMalloc(&d_bars_, size_t(capacity_) * sizeof(PhaseBar)), "cudaMalloc bars");
-  check(cudaMalloc(&d_partials_, size_t(capacity_) * 2 * (kSyncQ + 1) * sizeof(double)), "cudaMalloc partials");
+  check(cudaMalloc(&d_queue_, kMaxTiers * sizeof(int)), "cudaMalloc queue");
+  check(cudaMalloc(&d_bars_, size_t(kMaxTiers) * capacity_ * sizeof(PhaseBar)), "cudaMalloc bars");
+  check(cudaMalloc(&d_partials_, size_t(kMaxTiers) * capacity_ * 2 * (kSyncQ + 1) * sizeof(double)),
+        "cudaMalloc partials");
   check(cudaMalloc(&d_cg_state_, size_t(capacity_) * kMaxRhs * sizeof(CgState)), "cudaMalloc cg state");
   check(cudaMalloc(&d_err_, sizeof(int)), "cudaMalloc err");
   check(cudaMemsetAsync(d_err_, 0, sizeof(int), stream_), "memset err");
@@ -294,7 +320,7 @@ EnsChain Server::chain_entry(const Req &r) {
   memset(&e, 0, sizeof e);
   e.state = d_states_ + r.info.chain;
   e.op_begin = r.prog->node_begin[r.next];
-  e.op_end = r.prog->node_begin[r.next + 1];
+  e.op_end = r.prog->node_begin[r.next + r.take];
   e.g = c.g;
   e.w = c.w;
   e.beta_s = c.beta;
@@ -360,29 +386,52 @@ void Server::admit() {
 int Server::step() {
   admit();
   if (running_.empty()) return 0;
-  // the launch's chain table: every running request at its next slice, big ones first
+  // Slices of this step: the launch lasts as long as its costliest slice (cost
+  // ~ V x solves), so every request takes as many further slices as fit in
+  // that time -- small requests finish in one step instead of waiting a step
+  // per slice behind a big one.
+  auto slice_cost = [&](const Req &r, int k) {
+    return double(chains_[r.info.chain].g.V) * double(std::max(1, r.prog->solves[k]));
+  };
+  double span = 0.0;
+  for (long long id : running_) span = std::max(span, slice_cost(reqs_[id], reqs_[id].next));
+  std::vector<double> cost(running_.size());
+  for (size_t i = 0; i < running_.size(); i++) {
+    Req &r = reqs_[running_[i]];
+    double c = slice_cost(r, r.next);
+    r.take = 1;
+    while (r.next + r.take < r.nslices && c + slice_cost(r, r.next + r.take) <= span) c += slice_cost(r, r.next + r.take++);
+    cost[i] = c;
+  }
+  // the launch's chain table: tier by tier, each tier costliest first
   std::vector<int> order(running_.size());
   std::iota(order.begin(), order.end(), 0);
   for (size_t i = 0; i < running_.size(); i++) h_table_[i] = chain_entry(reqs_[running_[i]]);
-  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return h_table_[a].g.V > h_table_[b].g.V; });
-  int nbig = 0;
-  if (gs_ > 1)
-    for (int i : order)
-      if (h_table_[i].g.V >= big_min_) nbig++;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    const int ta = tier_of(h_table_[a].g.V), tb = tier_of(h_table_[b].g.V);
+    if (ta != tb) return ta < tb;
+    return cost[a] > cost[b];
+  });
   const int n = int(running_.size());
   check(cudaMemcpyAsync(d_table_, h_table_, n * sizeof(EnsChain), cudaMemcpyHostToDevice, stream_), "copy table");
   check(cudaMemcpyAsync(d_order_, order.data(), n * sizeof(int), cudaMemcpyHostToDevice, stream_), "copy order");
-  check(cudaMemsetAsync(d_queue_, 0, 2 * sizeof(int), stream_), "memset queue");
-  check(cudaMemsetAsync(d_bars_, 0, size_t(capacity_) * sizeof(PhaseBar), stream_), "memset bars");
+  check(cudaMemsetAsync(d_queue_, 0, kMaxTiers * sizeof(int), stream_), "memset queue");
+  check(cudaMemsetAsync(d_bars_, 0, size_t(kMaxTiers) * capacity_ * sizeof(PhaseBar), stream_), "memset bars");
   EnsLaunch a;
   a.chains = d_table_;
   a.nchains = n;
   a.order = d_order_;
-  a.nbig = nbig;
+  a.ntier = int(tier_gs_.size()) + 1;
+  for (int t = 0; t < a.ntier; t++) {
+    a.tier_gs[t] = t < int(tier_gs_.size()) ? tier_gs_[t] : 1;
+    int end = 0;
+    for (int i : order)
+      if (tier_of(h_table_[i].g.V) <= t) end++;
+    a.tier_end[t] = end;
+  }
   a.ops = d_ops_;
   a.op_begin = -1;
   a.op_end = -1;
-  a.gs = gs_;
   a.queue = d_queue_;
   a.bars = d_bars_;
   a.partials = d_partials_;
@@ -392,9 +441,8 @@ int Server::step() {
   a.tol = tol_;
   a.delta = 0.01;
   a.n_ru = 100;
-  const int groups = capacity_ / gs_;
   void *args[] = {(void *)&a};
-  check(cudaLaunchCooperativeKernel((const void *)ens_node_kernel, dim3(groups * gs_), dim3(kEnsThreads), args, 0,
+  check(cudaLaunchCooperativeKernel((const void *)ens_node_kernel, dim3(capacity_), dim3(kEnsThreads), args, 0,
                                     stream_),
         "ens_node_kernel launch");
   int h_err = 0;
@@ -413,7 +461,7 @@ int Server::step() {
   std::vector<long long> still;
   for (long long id : running_) {
     Req &r = reqs_[id];
-    r.next++;
+    r.next += r.take;
     if (r.next < r.nslices) {
       still.push_back(id);
       continue;
@@ -503,13 +551,16 @@ long long srv_guarded(gn_server *s, F &&f) {
 extern "C" {
 
 int gn_server_create(gn_server **out, const gn_ens_params *traj, double mem_budget_bytes, unsigned long long seed,
-                     int group_blocks, long long big_min_volume, int device) {
+                     int ntiers, const int *tier_blocks, const long long *tier_min_volume, int device) {
   if (out == nullptr || traj == nullptr) return gn::set_last_error(GN_ERR_ARG, "null argument");
+  if (ntiers > 0 && (tier_blocks == nullptr || tier_min_volume == nullptr))
+    return gn::set_last_error(GN_ERR_ARG, "null tier arrays");
   *out = nullptr;
   if (!(mem_budget_bytes > 0)) return gn::set_last_error(GN_ERR_ARG, "memory budget must be positive");
   try {
     auto s = std::make_unique<gn_server>();
-    s->s = std::make_unique<gn::Server>(*traj, size_t(mem_budget_bytes), seed, group_blocks, big_min_volume, device);
+    s->s = std::make_unique<gn::Server>(*traj, size_t(mem_budget_bytes), seed, ntiers, tier_blocks, tier_min_volume,
+                                        device);
     *out = s.release();
     return GN_OK;
   } catch (const gn::GnError &x) {

@@ -144,7 +144,7 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
         "gn_ensemble_stats": ([v, C.POINTER(ChainStats), C.c_int], C.c_int),
         "gn_ensemble_stream": ([v], C.c_void_p),
         "gn_server_create": ([C.POINTER(v), C.POINTER(EnsParams), C.c_double, C.c_ulonglong, C.c_int,
-                              C.c_longlong, C.c_int], C.c_int),
+                              C.POINTER(C.c_int), C.POINTER(C.c_longlong), C.c_int], C.c_int),
         "gn_server_destroy": ([v], None),
         "gn_server_add_chain": ([v, C.c_int, C.c_double, _dp, C.c_ulonglong], C.c_int),
         "gn_server_clock": ([v], C.c_double),
@@ -462,11 +462,15 @@ class Ensemble:
 class Server:
     """Requests on resident chains with continuous batching (gn_server_* of gn_b200.h)."""
 
-    def __init__(self, traj_params, mem_budget_bytes=8e9, seed=1231, group_blocks=4, big_min_volume=4096, device=0):
+    def __init__(self, traj_params, mem_budget_bytes=8e9, seed=1231, tiers=((16, 48 ** 3), (4, 16 ** 3)), device=0):
+        """tiers: (blocks per team, minimum volume) pairs, team sizes dividing each other."""
         self.lib = load_library()
         self.srv = C.c_void_p()
+        nt = len(tiers)
+        tb = (C.c_int * max(nt, 1))(*[int(t[0]) for t in tiers])
+        tv = (C.c_longlong * max(nt, 1))(*[int(t[1]) for t in tiers])
         self._check(self.lib.gn_server_create(C.byref(self.srv), C.byref(traj_params), float(mem_budget_bytes),
-                                              int(seed), group_blocks, big_min_volume, device))
+                                              int(seed), nt, tb, tv, device))
         self.Ls = []
 
     def _check(self, st, allow=(GN_OK,)):

@@ -66,7 +66,7 @@ def parse():
     ap.add_argument("--eps", type=float, default=0.05)
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--case", choices=["cg64", "dirac128", "dirac256", "traj64", "cgscan", "batched"], default=None,
+    ap.add_argument("--case", choices=["cg64", "dirac128", "dirac256", "traj64", "cgscan", "batched", "serve"], default=None,
                     help="run one small case for a profiler instead of the benchmark")
     return ap.parse_args()
 
@@ -483,6 +483,61 @@ def batched_bench(G, dev, nchains=256, ntraj=2, warmup=1, tune=True):
             "graph": info["graph"], "launches_per_trajectory": info["launches_per_trajectory"] + 2}
 
 
+def serve_bench(G, nreq=600, rate=200.0, warm=24, seed=5):
+    """The serving loop: Poisson arrivals at `rate`/s of requests -- one HMC
+    trajectory (70 %), one solve with an N(0, 1) right-hand side (20 %), a
+    condensate estimate from 16 Z2 vectors (10 %) -- on 256 resident chains,
+    32 for each L in 8, 16, ..., 64 with beta_s uniform in [0.6, 1.1];
+    trajectories LFMN2VF 8 x eps 0.08, every solve mixed precision to 1e-10.
+    Latency = completion - scheduled arrival (host clock), so queueing counts.
+    A warm-up of `warm` requests runs and drains first."""
+    rng = np.random.default_rng(seed)
+    Ls = [L for L in range(8, 65, 8) for _ in range(32)]
+    betas = rng.uniform(0.6, 1.1, len(Ls))
+    types = (G.GN_REQ_TRAJECTORY, G.GN_REQ_SOLVE, G.GN_REQ_CONDENSATE)
+    with G.Server(G.Ensemble.params(0.08, 8), mem_budget_bytes=32e9, seed=seed) as srv:
+        for c, (L, b) in enumerate(zip(Ls, betas)):
+            srv.add_chain(L, b, rng.normal(0.0, np.sqrt(2.0 / (NFLAV * b)), L ** 3), stream_id=c)
+        for k in range(warm):
+            t = types[k % 3]
+            srv.submit(int(rng.integers(len(Ls))), t, 16 if t == G.GN_REQ_CONDENSATE else 0)
+        srv.drain()
+        gaps = rng.exponential(1.0 / rate, nreq)
+        kinds = rng.choice(3, size=nreq, p=[0.7, 0.2, 0.1])
+        chains = rng.integers(len(Ls), size=nreq)
+        t0 = srv.clock() + 0.01
+        arrive = t0 + np.cumsum(gaps)
+        ids, nxt, steps = [], 0, 0
+        while True:
+            now = srv.clock()
+            while nxt < nreq and arrive[nxt] <= now:
+                t = types[kinds[nxt]]
+                ids.append(srv.submit(int(chains[nxt]), t, 16 if t == G.GN_REQ_CONDENSATE else 0, arrive[nxt]))
+                nxt += 1
+            ld = srv.load()
+            if ld["running"] == 0 and ld["queued"] == 0:
+                if nxt == nreq:
+                    break
+                time.sleep(max(0.0, arrive[nxt] - srv.clock()))
+                continue
+            srv.step()
+            steps += 1
+        info = [srv.request(i) for i in ids]
+    lat = np.array([r["t_done"] - r["t_arrival"] for r in info])
+    span = max(r["t_done"] for r in info) - arrive[0]
+    out = {"metric": "serving: p50 / p99 request latency and throughput at Poisson 200/s (70 % trajectory, "
+                     "20 % solve, 10 % condensate x 16 Z2), L in {8..64}, mixed CG to 1e-10",
+           "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+           "throughput_req_per_s": nreq / span, "offered_req_per_s": rate, "requests": nreq, "steps": steps,
+           "failed": int(sum(r["failed"] for r in info)), "precision": "mixed"}
+    for name, t in (("trajectory", 0), ("solve", 1), ("condensate", 2)):
+        lt = np.array([r["t_done"] - r["t_arrival"] for r in info if r["type"] == t])
+        if len(lt):
+            out[name] = {"n": int(len(lt)), "p50_ms": float(np.percentile(lt, 50) * 1e3),
+                         "p99_ms": float(np.percentile(lt, 99) * 1e3)}
+    return out
+
+
 def dirac_roofline(G, stream, dev, reps=20, L=256):
     """Dirac M on one FP64 plane at L = 256 (V = 16,777,216): psi, sm and the
     output are 384 MB, three times the L2, so back-to-back launches run from
@@ -532,6 +587,9 @@ def run_case(a):
         return
     if a.case == "batched":
         print(json.dumps(batched_bench(G, dev)))
+        return
+    if a.case == "serve":
+        print(json.dumps(serve_bench(G)))
         return
     L, V = 64, 64 ** 3
     lat = G.Lattice(L, 0)

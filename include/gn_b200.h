@@ -340,9 +340,13 @@ typedef struct {
 
 /* traj: the trajectories' integrator, steps, step size and the tolerance of
  * every solve.  mem_budget_bytes bounds the running requests' work arrays.
- * Chains with V >= big_min_volume run on groups of group_blocks blocks. */
+ * Team tiers (0 to 3): a chain with V >= tier_min_volume[t] (and below the
+ * earlier tiers' bounds) runs on teams of tier_blocks[t] blocks; sizes >= 2,
+ * each dividing the previous one, volumes decreasing; smaller chains run on
+ * single blocks. */
 GN_API int gn_server_create(gn_server **srv, const gn_ens_params *traj, double mem_budget_bytes,
-                            unsigned long long seed, int group_blocks, long long big_min_volume, int device);
+                            unsigned long long seed, int ntiers, const int *tier_blocks,
+                            const long long *tier_min_volume, int device);
 GN_API void gn_server_destroy(gn_server *srv);
 /* A resident chain: returns its index (>= 0) or a negative status. */
 GN_API int gn_server_add_chain(gn_server *srv, int L, double beta_s, const double *sigma,
