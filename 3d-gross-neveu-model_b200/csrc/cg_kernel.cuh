@@ -117,22 +117,29 @@ __device__ __forceinline__ void acc_add(double (&acc)[2 * kMaxRhs], int slot, do
     if (q == slot) acc[q] += v;
 }
 
-// NR: right-hand-side slots unrolled (>= nrhs); BS: threads per block; W:
-// sites per item (divides L/2).
-template <typename T, int NC, int NR, int BS, int W>
-__global__ void __launch_bounds__(BS, 1) cg_kernel(CgArgs<T> a) {
-  __shared__ SyncShared sh;
+// Block-shared state of one FP64 solve (the same values in every block of the team).
+struct CgShared {
+  double alpha[kMaxRhs], beta[kMaxRhs], rr[kMaxRhs], tau[kMaxRhs], r2[kMaxRhs], b2[kMaxRhs];
+  int active[kMaxRhs], status[kMaxRhs], all[kMaxRhs];
+  long long iters[kMaxRhs];
+  SysList run, every;  // systems still iterating / all systems
+};
+
+// One solve by a team (all its threads call it; a.bar, a.partials and a.err
+// are not used: the team's own are).  NR: right-hand-side slots unrolled
+// (>= nrhs); W: sites per item (divides L/2).
+template <typename T, int NC, int NR, int W>
+__device__ __forceinline__ void cg_solve(const CgArgs<T> &a, Team &team, SyncShared &sh, CgShared &cs) {
   double *const s_val = sh.val;
-  __shared__ double s_alpha[kMaxRhs], s_beta[kMaxRhs], s_rr[kMaxRhs], s_tau[kMaxRhs];
-  __shared__ int s_active[kMaxRhs], s_status[kMaxRhs], s_all[kMaxRhs];
-  __shared__ long long s_iters[kMaxRhs];
-  __shared__ double s_r2[kMaxRhs], s_b2[kMaxRhs];
-  __shared__ SysList s_run, s_every;  // systems still iterating / all systems
+  double *const s_alpha = cs.alpha, *const s_beta = cs.beta, *const s_rr = cs.rr, *const s_tau = cs.tau;
+  double *const s_r2 = cs.r2, *const s_b2 = cs.b2;
+  int *const s_active = cs.active, *const s_status = cs.status, *const s_all = cs.all;
+  long long *const s_iters = cs.iters;
+  SysList &s_run = cs.run, &s_every = cs.every;
 
   const Geom g = a.g;
   const uint32_t V = uint32_t(g.V);
   const uint32_t NI = row_items<W>(g);
-  Team team = grid_team(a.bar, a.partials, a.err);
   const T *__restrict__ sm = a.sm;
 
   if (threadIdx.x < kMaxRhs) {
@@ -281,7 +288,7 @@ __global__ void __launch_bounds__(BS, 1) cg_kernel(CgArgs<T> a) {
     // the host's abort request lives in mapped host memory: one thread reads it
     // every 16 iterations, and the value is only used at the end of phase B
     int abort_req = 0;
-    if (blockIdx.x == 0 && threadIdx.x == 0 && a.abort_flag != nullptr && (it & 15) == 0)
+    if (team.brank == 0 && threadIdx.x == 0 && a.abort_flag != nullptr && (it & 15) == 0)
       abort_req = *(volatile const int *)a.abort_flag;
     const bool odd = (it & 1) != 0;
     // phase A: p = r + beta p_old (it > 0), t = M^T p, sum t^2
@@ -391,13 +398,13 @@ __global__ void __launch_bounds__(BS, 1) cg_kernel(CgArgs<T> a) {
     __syncthreads();
     // host abort request: block 0's view decides for everyone at the next phase
     if (sh.flag != 0) {  // block 0 saw the host's abort request at the last phase end
-      if (threadIdx.x == 0 && blockIdx.x == 0) atomicExch(a.err, 2);
+      if (threadIdx.x == 0 && team.brank == 0) atomicExch(team.err, 2);
       ok = false;
       break;
     }
   }
   // ---------------------------------------------------------------- results
-  if (blockIdx.x == 0 && threadIdx.x < kMaxRhs) {
+  if (team.brank == 0 && threadIdx.x < kMaxRhs) {
     const int k = threadIdx.x;
     if (k < a.nrhs) {
       CgState st;
@@ -411,6 +418,15 @@ __global__ void __launch_bounds__(BS, 1) cg_kernel(CgArgs<T> a) {
       a.state[k] = st;
     }
   }
+}
+
+// The single-lattice solve: the whole cooperative grid is the team.
+template <typename T, int NC, int NR, int BS, int W>
+__global__ void __launch_bounds__(BS, 1) cg_kernel(CgArgs<T> a) {
+  __shared__ SyncShared sh;
+  __shared__ CgShared cs;
+  Team team = grid_team(a.bar, a.partials, a.err);
+  cg_solve<T, NC, NR, W>(a, team, sh, cs);
 }
 
 }  // namespace gn

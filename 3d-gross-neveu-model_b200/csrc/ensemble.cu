@@ -42,6 +42,7 @@ class Ensemble {
   void load_sigma(int c, const double *h);
   void store_sigma(int c, double *sigma, double *sm);
   void set_layout(int gs, long long big_min);
+  void set_precision(int prec);
   void tune(const gn_ens_params &p, int *gs, long long *big_min);
   void run(const gn_ens_params &p, int ntraj, bool graph);
   void stats(gn_chain_stats *out, bool reset);
@@ -121,6 +122,7 @@ Ensemble::Ensemble(int n, const int *L, const double *beta_s, const unsigned lon
     };
     double *s0 = dv(1), *s1 = dv(1), *sm = dv(1), *P = dv(1), *F = dv(1), *save = dv(1);
     double *chi = dv(2), *phi = dv(2), *X = dv(2), *Y = dv(2), *t64 = dv(2);
+    double *r64 = dv(2), *pa64 = dv(2), *pb64 = dv(2);
     float *sm32 = fv(1), *rh = fv(2), *ph = fv(2), *th = fv(2), *xh = fv(2);
     if (ch) {
       ch->g = make_geom(L[c]);
@@ -143,6 +145,10 @@ Ensemble::Ensemble(int n, const int *L, const double *beta_s, const unsigned lon
       ch->ph = ph;
       ch->th = th;
       ch->xh = xh;
+      ch->r64 = r64;
+      ch->pa64 = pa64;
+      ch->pb64 = pb64;
+      ch->precision = GN_PREC_MIXED;
     }
     return used;
   };
@@ -236,6 +242,14 @@ void Ensemble::build_order() {
   check(cudaStreamSynchronize(stream_), "order");
 }
 
+// The chains' solver precision (uploaded with the chain table when it changes).
+void Ensemble::set_precision(int prec) {
+  if (!chains_.empty() && chains_[0].precision == prec) return;
+  for (EnsChain &ch : chains_) ch.precision = prec;
+  check(cudaMemcpyAsync(d_chains_, chains_.data(), n_ * sizeof(EnsChain), cudaMemcpyHostToDevice, stream_), "copy");
+  check(cudaStreamSynchronize(stream_), "precision");
+}
+
 void Ensemble::set_layout(int gs, long long big_min) {
   if (gs < 1 || gs > capacity_) throw GnError(GN_ERR_ARG, "blocks per group out of range");
   gs_ = gs;
@@ -245,7 +259,7 @@ void Ensemble::set_layout(int gs, long long big_min) {
 }
 
 Ensemble::Plan &Ensemble::plan_for(const gn_ens_params &p) {
-  const std::vector<double> key = {p.eps, double(p.steps), double(p.integrator), p.tol};
+  const std::vector<double> key = {p.eps, double(p.steps), double(p.integrator), p.tol, double(p.precision)};
   auto it = plans_.find(key);
   if (it != plans_.end()) return *it->second;
   auto pl = std::make_unique<Plan>();
@@ -358,6 +372,9 @@ void Ensemble::check_err() {
 void Ensemble::run(const gn_ens_params &p, int ntraj, bool graph) {
   if (p.steps < 1 || p.integrator < 0 || p.integrator > 2 || !(p.tol > 0.0) || ntraj < 0)
     throw GnError(GN_ERR_ARG, "bad ensemble parameters");
+  if (p.precision != GN_PREC_MIXED && p.precision != GN_PREC_FP64)
+    throw GnError(GN_ERR_ARG, "ensemble precision: GN_PREC_MIXED or GN_PREC_FP64");
+  set_precision(p.precision);
   Plan &pl = plan_for(p);
   last_launches_ = int(pl.node_begin.size()) - 1;
   if (graph && !pl.graph_failed && (pl.graph == nullptr || pl.layout_epoch != layout_epoch_)) {
@@ -393,6 +410,7 @@ void Ensemble::run(const gn_ens_params &p, int ntraj, bool graph) {
 }
 
 void Ensemble::tune(const gn_ens_params &p, int *gs_out, long long *big_out) {
+  set_precision(p.precision == GN_PREC_FP64 ? GN_PREC_FP64 : GN_PREC_MIXED);
   Plan &pl = plan_for(p);
   std::vector<long long> vols;
   for (const EnsChain &ch : chains_) vols.push_back(ch.g.V);

@@ -15,6 +15,7 @@
 // number as the counter, so a chain's results do not depend on the chains
 // beside it or on which team ran it (for a fixed team size).
 #pragma once
+#include "../../include/gn_b200.h"
 #include "mixed_kernel.cuh"
 #include "ops_kernels.cuh"
 #include "philox.cuh"
@@ -60,6 +61,8 @@ struct EnsChain {
   double *chi, *phi, *X, *Y;  // two flavour planes each
   double *t64;                // solver FP64 scratch, two planes
   float *sm32, *rh, *ph, *th, *xh;  // solver FP32 vectors, two planes each
+  double *r64, *pa64, *pb64;  // FP64 solver vectors (with t64), two planes each
+  int precision;              // GN_PREC_MIXED or GN_PREC_FP64
 };
 
 // One chain's mutable state (device).
@@ -115,11 +118,15 @@ __device__ __forceinline__ void team_dirac2(const Geom &g, const Team &t, const 
   }
 }
 
-// The solver of one chain, one function per item width (each gets its own
+// The solvers of one chain, one function per item width (each gets its own
 // register allocation instead of sharing the caller's).
 template <int W>
 __device__ __noinline__ void ens_solve(const MixedArgs &a, Team &t, SyncShared &sh, MixedShared &ms) {
   mixed_solve<1, 2, W>(a, t, sh, ms);
+}
+template <int W>
+__device__ __noinline__ void ens_solve64(const CgArgs<double> &a, Team &t, SyncShared &sh, CgShared &cs) {
+  cg_solve<double, 1, 2, W>(a, t, sh, cs);
 }
 
 // Box-Muller on two uniforms: two N(0, 1) values.
@@ -132,7 +139,8 @@ __device__ __forceinline__ void box_muller(uint64_t a, uint64_t b, double &z0, d
 }
 
 // The chain's ops [op_begin, op_end) by team t.  Returns false on a barrier timeout.
-static __device__ __noinline__ bool ens_run_chain(const EnsLaunch &L, int c, Team &t, SyncShared &sh, MixedShared &ms) {
+static __device__ __noinline__ bool ens_run_chain(const EnsLaunch &L, int c, Team &t, SyncShared &sh, MixedShared &ms,
+                                                  CgShared &cs) {
   const EnsChain &ch = L.chains[c];
   EnsState *st = ch.state;
   const int op_begin = L.op_begin >= 0 ? L.op_begin : ch.op_begin;
@@ -173,41 +181,75 @@ static __device__ __noinline__ bool ens_run_chain(const EnsLaunch &L, int c, Tea
       else team_dirac2<1, 0>(g, t, ch.sm, ch.chi, ch.phi);
       ok = end_phase<0>(acc, sh, t);
     } else if (op.code == E_SOLVE) {
-      MixedArgs a;
-      a.g = g;
-      a.sm = ch.sm;
-      a.sm32 = ch.sm32;
-      for (int k = 0; k < kMaxRhs; k++) {
-        const int kk = k < 2 ? k : 1;
-        a.b[k] = ch.phi + size_t(kk) * V;
-        a.x[k] = ch.X + size_t(kk) * V;
-        a.t64[k] = ch.t64 + size_t(kk) * V;
-        a.rh[k] = ch.rh + size_t(kk) * V;
-        a.ph[k] = ch.ph + size_t(kk) * V;
-        a.th[k] = ch.th + size_t(kk) * V;
-        a.xh[k] = ch.xh + size_t(kk) * V;
+      const int nrhs = op.c > 0.0 ? int(op.c) : 2;
+      const int *status;
+      const long long *iters;
+      if (ch.precision == GN_PREC_FP64) {
+        CgArgs<double> a;
+        a.g = g;
+        a.sm = ch.sm;
+        for (int k = 0; k < kMaxRhs; k++) {
+          const size_t off = size_t(k < 2 ? k : 1) * V;
+          a.b[k] = ch.phi + off;
+          a.x[k] = ch.X + off;
+          a.r[k] = ch.r64 + off;
+          a.p0[k] = ch.pa64 + off;
+          a.p1[k] = ch.pb64 + off;
+          a.t[k] = ch.t64 + off;
+        }
+        a.nrhs = nrhs;
+        a.variant = 1;
+        a.rel = 1;
+        a.tol = L.tol;
+        a.max_iter = (long long)V + 1;
+        a.partials = nullptr;
+        a.bar = nullptr;
+        a.err = t.err;
+        a.abort_flag = nullptr;
+        a.state = L.cg_state + size_t(blockIdx.x) * kMaxRhs;
+        if (ch.w >= 2) ens_solve64<2>(a, t, sh, cs);
+        else ens_solve64<1>(a, t, sh, cs);
+        status = cs.status;
+        iters = cs.iters;
+      } else {
+        MixedArgs a;
+        a.g = g;
+        a.sm = ch.sm;
+        a.sm32 = ch.sm32;
+        for (int k = 0; k < kMaxRhs; k++) {
+          const size_t off = size_t(k < 2 ? k : 1) * V;
+          a.b[k] = ch.phi + off;
+          a.x[k] = ch.X + off;
+          a.t64[k] = ch.t64 + off;
+          a.rh[k] = ch.rh + off;
+          a.ph[k] = ch.ph + off;
+          a.th[k] = ch.th + off;
+          a.xh[k] = ch.xh + off;
+        }
+        a.nrhs = nrhs;
+        a.variant = 1;
+        a.rel = 1;
+        a.tol = L.tol;
+        a.max_iter = (long long)V + 1;
+        a.delta = L.delta;
+        a.n_ru = L.n_ru;
+        a.partials = nullptr;
+        a.bar = nullptr;
+        a.err = t.err;
+        a.abort_flag = nullptr;
+        a.state = L.cg_state + size_t(blockIdx.x) * kMaxRhs;
+        if (ch.w == 4) ens_solve<4>(a, t, sh, ms);
+        else if (ch.w == 2) ens_solve<2>(a, t, sh, ms);
+        else ens_solve<1>(a, t, sh, ms);
+        status = ms.status;
+        iters = ms.iters;
       }
-      a.nrhs = op.c > 0.0 ? int(op.c) : 2;
-      a.variant = 1;
-      a.rel = 1;
-      a.tol = L.tol;
-      a.max_iter = (long long)V + 1;
-      a.delta = L.delta;
-      a.n_ru = L.n_ru;
-      a.partials = nullptr;
-      a.bar = nullptr;
-      a.err = t.err;
-      a.abort_flag = nullptr;
-      a.state = L.cg_state + size_t(blockIdx.x) * kMaxRhs;
-      if (ch.w == 4) ens_solve<4>(a, t, sh, ms);
-      else if (ch.w == 2) ens_solve<2>(a, t, sh, ms);
-      else ens_solve<1>(a, t, sh, ms);
       if (leader) {
-        for (int k = 0; k < a.nrhs; k++) {
-          const int s = ms.status[k];
+        for (int k = 0; k < nrhs; k++) {
+          const int s = status[k];
           if (s != kCgConverged && s != kCgConvergedStart) st->failed = 1;
-          st->iters += (s == kCgConverged) ? ms.iters[k] : 0;
-          st->reliable += ms.nru[k];
+          st->iters += (s == kCgConverged) ? iters[k] : 0;
+          if (ch.precision != GN_PREC_FP64) st->reliable += ms.nru[k];
         }
       }
       ok = ld_relaxed_int(t.err) == 0;
@@ -319,6 +361,7 @@ __global__ void __launch_bounds__(kEnsThreads, 1) ens_node_kernel(EnsLaunch L);
 __global__ void __launch_bounds__(kEnsThreads, 1) ens_node_kernel(EnsLaunch L) {
   __shared__ SyncShared sh;
   __shared__ MixedShared ms;
+  __shared__ CgShared cs;
   __shared__ int s_task;
   int tb = 0;  // first order index of the tier
   for (int tier = 0; tier < L.ntier; tier++) {
@@ -345,7 +388,7 @@ __global__ void __launch_bounds__(kEnsThreads, 1) ens_node_kernel(EnsLaunch L) {
           if (!end_phase<0>(acc, sh, gt, task)) return;  // the team leader's task, to every block
           task = sh.flag;
           if (task >= te) break;
-          if (!ens_run_chain(L, L.order[task], gt, sh, ms)) return;
+          if (!ens_run_chain(L, L.order[task], gt, sh, ms, cs)) return;
         }
       }
     } else {
@@ -364,7 +407,7 @@ __global__ void __launch_bounds__(kEnsThreads, 1) ens_node_kernel(EnsLaunch L) {
         const int task = s_task;
         __syncthreads();
         if (task >= te) break;
-        if (!ens_run_chain(L, L.order[task], bt, sh, ms)) return;
+        if (!ens_run_chain(L, L.order[task], bt, sh, ms, cs)) return;
       }
     }
     tb = te;

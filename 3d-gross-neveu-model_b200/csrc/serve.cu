@@ -12,7 +12,10 @@
 // chain is free and its work arrays fit the memory budget.  Work arrays come
 // from the stream-ordered allocator at admission and go back at retirement.
 // A request's numbers depend only on its chain's state and its serial number on
-// that chain (the Philox counter of its draws), not on the requests beside it.
+// that chain (the Philox counter of its draws), not on the requests beside it --
+// bit for bit where its team size is fixed; the top tier's team size follows
+// the load (a lone big request gets the whole GPU), which changes only the
+// order of the solver's sums.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -96,6 +99,7 @@ class Server {
   size_t budget_ = 0, in_use_ = 0;
   unsigned long long seed_ = 0;
   double tol_ = 1e-10;
+  int precision_ = GN_PREC_MIXED;
   cudaStream_t stream_ = nullptr;
   std::chrono::steady_clock::time_point t0_;
   std::vector<Chain> chains_;
@@ -121,16 +125,18 @@ class Server {
 static size_t round256(size_t b) { return (b + 255) & ~size_t(255); }
 
 // A running request's arrays: P, F, sigma_save (1 plane each), chi, phi, X,
-// Y, t64 (2 planes), sm32 (1 plane of float), the solver's r^, p^, t^, x^
-// (2 planes of float each).
+// Y, t64 (2 planes), sm32 (1 plane of float), the mixed solver's r^, p^, t^,
+// x^ (2 planes of float each), the FP64 solver's r, p, p' (2 planes each).
 size_t Server::work_bytes(size_t V) {
-  return 3 * round256(V * 8) + 5 * round256(2 * V * 8) + round256(V * 4) + 4 * round256(2 * V * 4);
+  return 3 * round256(V * 8) + 5 * round256(2 * V * 8) + round256(V * 4) + 4 * round256(2 * V * 4) +
+         3 * round256(2 * V * 8);
 }
 
 Server::Server(const gn_ens_params &traj, size_t budget, unsigned long long seed, int ntier, const int *tier_blocks,
                const long long *tier_min_volume, int device)
-    : device_(device), budget_(budget), seed_(seed), tol_(traj.tol) {
-  if (traj.steps < 1 || traj.integrator < 0 || traj.integrator > 2 || !(traj.tol > 0.0))
+    : device_(device), budget_(budget), seed_(seed), tol_(traj.tol), precision_(traj.precision) {
+  if (traj.steps < 1 || traj.integrator < 0 || traj.integrator > 2 || !(traj.tol > 0.0) ||
+      (traj.precision != GN_PREC_MIXED && traj.precision != GN_PREC_FP64))
     throw GnError(GN_ERR_ARG, "bad trajectory parameters");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) throw GnError(GN_ERR_NO_DEVICE, "no CUDA device");
@@ -352,6 +358,10 @@ EnsChain Server::chain_entry(const Req &r) {
   e.ph = fv(2);
   e.th = fv(2);
   e.xh = fv(2);
+  e.r64 = dv(2);
+  e.pa64 = dv(2);
+  e.pb64 = dv(2);
+  e.precision = precision_;
   return e;
 }
 
@@ -386,12 +396,26 @@ void Server::admit() {
 int Server::step() {
   admit();
   if (running_.empty()) return 0;
-  // Slices of this step: the launch lasts as long as its costliest slice (cost
-  // ~ V x solves), so every request takes as many further slices as fit in
-  // that time -- small requests finish in one step instead of waiting a step
-  // per slice behind a big one.
+  // Team size of the top tier this step: the whole GPU shared among the
+  // running top-tier requests (at least the configured size, a multiple of the
+  // next tier's so the teams nest), so a lone big request gets every SM.
+  const int ntier_cfg = int(tier_gs_.size());
+  int top = ntier_cfg > 0 ? tier_gs_[0] : 1;
+  if (ntier_cfg > 0) {
+    int n0 = 0;
+    for (long long id : running_) n0 += tier_of(chains_[reqs_[id].info.chain].g.V) == 0 ? 1 : 0;
+    const int unit = ntier_cfg > 1 ? tier_gs_[1] : 1;
+    const int share = (capacity_ / std::max(1, n0)) / unit * unit;
+    top = std::max(top, share);
+  }
+  auto team_size = [&](int tier) { return tier == 0 ? top : (tier < ntier_cfg ? tier_gs_[tier] : 1); };
+  // Slices of this step: the launch lasts about as long as its costliest slice
+  // (cost ~ V x solves / team size), so every request takes as many further
+  // slices as fit in that time -- small requests finish in one step instead of
+  // waiting a step per slice behind a big one.
   auto slice_cost = [&](const Req &r, int k) {
-    return double(chains_[r.info.chain].g.V) * double(std::max(1, r.prog->solves[k]));
+    const double V = double(chains_[r.info.chain].g.V);
+    return V * double(std::max(1, r.prog->solves[k])) / double(team_size(tier_of(int64_t(V))));
   };
   double span = 0.0;
   for (long long id : running_) span = std::max(span, slice_cost(reqs_[id], reqs_[id].next));
@@ -423,7 +447,7 @@ int Server::step() {
   a.order = d_order_;
   a.ntier = int(tier_gs_.size()) + 1;
   for (int t = 0; t < a.ntier; t++) {
-    a.tier_gs[t] = t < int(tier_gs_.size()) ? tier_gs_[t] : 1;
+    a.tier_gs[t] = team_size(t);
     int end = 0;
     for (int i : order)
       if (tier_of(h_table_[i].g.V) <= t) end++;

@@ -59,7 +59,8 @@ class TrajResult(C.Structure):
 
 
 class EnsParams(C.Structure):
-    _fields_ = [("eps", C.c_double), ("steps", C.c_int), ("integrator", C.c_int), ("tol", C.c_double)]
+    _fields_ = [("eps", C.c_double), ("steps", C.c_int), ("integrator", C.c_int), ("tol", C.c_double),
+                ("precision", C.c_int)]
 
 
 class ChainStats(C.Structure):
@@ -428,8 +429,8 @@ class Ensemble:
         return s, sm
 
     @staticmethod
-    def params(eps, steps, integrator=GN_LFMN2VF, tol=1e-10):
-        return EnsParams(eps, steps, integrator, tol)
+    def params(eps, steps, integrator=GN_LFMN2VF, tol=1e-10, precision=GN_PREC_MIXED):
+        return EnsParams(eps, steps, integrator, tol, precision)
 
     def set_layout(self, group_blocks, big_min_volume):
         self._check(self.lib.gn_ensemble_set_layout(self.ens, group_blocks, big_min_volume))

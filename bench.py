@@ -351,7 +351,12 @@ def run_ours(a, world, rank, local):
     # dominant kernel: one two-flavour mixed CG solve, events around the kernel
     roof = kernel_roofline(lat, stream, a, G)
     dirac = dirac_roofline(G, stream, dev)
-    batched = batched_bench(G, dev) if world == 1 else None
+    batched = None
+    if world == 1:
+        batched = batched_bench(G, dev)
+        batched["fp64"] = {k: v for k, v in batched_bench(G, dev, tune=False, precision=G.GN_PREC_FP64).items()
+                           if k in ("value", "ms_per_ensemble_trajectory", "cg_iterations_per_chain_trajectory",
+                                    "solver_gbs")}
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -441,7 +446,7 @@ def kernel_roofline(lat, stream, a, G):
                     f"{(2 * 5 * 4 + 8 * 3) * V / 1e6:.0f} MB is L2-resident within the solve"}
 
 
-def batched_bench(G, dev, nchains=256, ntraj=2, warmup=1, tune=True):
+def batched_bench(G, dev, nchains=256, ntraj=2, warmup=1, tune=True, precision=None):
     """The batched ensemble: nchains chains with L uniform in {8, 12, 16, 24, 32,
     48} (seeded), beta_s on a uniform grid over [0.5, 1.2], LFMN2VF 8 x eps 0.08,
     every solve mixed precision to 1e-10 (true relative residual), device
@@ -450,10 +455,11 @@ def batched_bench(G, dev, nchains=256, ntraj=2, warmup=1, tune=True):
     of every chain after `warmup`.  Algorithmic bytes: 96 per site per pair of
     solver iterations (the two flavours' FP32 sweeps, 8 + 2 x 44 B)."""
     import torch
+    prec = G.GN_PREC_MIXED if precision is None else precision
     rng = np.random.default_rng(4242)
     Ls = [int(x) for x in rng.choice([8, 12, 16, 24, 32, 48], size=nchains)]
     betas = list(np.linspace(0.5, 1.2, nchains))
-    p = G.Ensemble.params(0.08, 8)
+    p = G.Ensemble.params(0.08, 8, precision=prec)
     with G.Ensemble(Ls, betas, seed=1231) as e:
         for c, (L, b) in enumerate(zip(Ls, betas)):
             e.load_sigma(c, rng.normal(0.0, np.sqrt(2.0 / (NFLAV * b)), L ** 3))
@@ -473,7 +479,8 @@ def batched_bench(G, dev, nchains=256, ntraj=2, warmup=1, tune=True):
     iters = sum(s["cg_iterations"] for s in stats)
     acc = sum(s["accepted"] for s in stats) / (nchains * ntraj)
     nbytes = sum(L ** 3 * s["cg_iterations"] / 2 * 96 for L, s in zip(Ls, stats))
-    return {"metric": "chain trajectories/s, 256 chains L in {8..48}, LFMN2VF 8 x eps 0.08, mixed CG to 1e-10",
+    return {"metric": "chain trajectories/s, 256 chains L in {8..48}, LFMN2VF 8 x eps 0.08, CG to 1e-10",
+            "precision": "mixed" if prec == G.GN_PREC_MIXED else "fp64",
             "value": nchains * ntraj / (ms / 1e3), "unit": "traj/s",
             "site_trajectories_per_s": sites * ntraj / (ms / 1e3), "ms_per_ensemble_trajectory": ms / ntraj,
             "chains": nchains, "sites": sites, "acceptance": acc,
@@ -483,7 +490,7 @@ def batched_bench(G, dev, nchains=256, ntraj=2, warmup=1, tune=True):
             "graph": info["graph"], "launches_per_trajectory": info["launches_per_trajectory"] + 2}
 
 
-def serve_bench(G, nreq=600, rate=200.0, warm=24, seed=5):
+def serve_bench(G, nreq=600, rate=200.0, warm=24, seed=5, precision=None):
     """The serving loop: Poisson arrivals at `rate`/s of requests -- one HMC
     trajectory (70 %), one solve with an N(0, 1) right-hand side (20 %), a
     condensate estimate from 16 Z2 vectors (10 %) -- on 256 resident chains,
@@ -491,11 +498,12 @@ def serve_bench(G, nreq=600, rate=200.0, warm=24, seed=5):
     trajectories LFMN2VF 8 x eps 0.08, every solve mixed precision to 1e-10.
     Latency = completion - scheduled arrival (host clock), so queueing counts.
     A warm-up of `warm` requests runs and drains first."""
+    prec = G.GN_PREC_MIXED if precision is None else precision
     rng = np.random.default_rng(seed)
     Ls = [L for L in range(8, 65, 8) for _ in range(32)]
     betas = rng.uniform(0.6, 1.1, len(Ls))
     types = (G.GN_REQ_TRAJECTORY, G.GN_REQ_SOLVE, G.GN_REQ_CONDENSATE)
-    with G.Server(G.Ensemble.params(0.08, 8), mem_budget_bytes=32e9, seed=seed) as srv:
+    with G.Server(G.Ensemble.params(0.08, 8, precision=prec), mem_budget_bytes=32e9, seed=seed) as srv:
         for c, (L, b) in enumerate(zip(Ls, betas)):
             srv.add_chain(L, b, rng.normal(0.0, np.sqrt(2.0 / (NFLAV * b)), L ** 3), stream_id=c)
         for k in range(warm):
@@ -524,12 +532,13 @@ def serve_bench(G, nreq=600, rate=200.0, warm=24, seed=5):
             steps += 1
         info = [srv.request(i) for i in ids]
     lat = np.array([r["t_done"] - r["t_arrival"] for r in info])
-    span = max(r["t_done"] for r in info) - arrive[0]
-    out = {"metric": "serving: p50 / p99 request latency and throughput at Poisson 200/s (70 % trajectory, "
-                     "20 % solve, 10 % condensate x 16 Z2), L in {8..64}, mixed CG to 1e-10",
+    span = max(r["t_done"] for r in info) - arrive[0]  # first arrival to last completion
+    out = {"metric": f"serving: p50 / p99 request latency and throughput at Poisson {rate:g}/s (70 % trajectory, "
+                     "20 % solve, 10 % condensate x 16 Z2), L in {8..64}, CG to 1e-10",
            "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
            "throughput_req_per_s": nreq / span, "offered_req_per_s": rate, "requests": nreq, "steps": steps,
-           "failed": int(sum(r["failed"] for r in info)), "precision": "mixed"}
+           "failed": int(sum(r["failed"] for r in info)),
+           "precision": "mixed" if prec == G.GN_PREC_MIXED else "fp64"}
     for name, t in (("trajectory", 0), ("solve", 1), ("condensate", 2)):
         lt = np.array([r["t_done"] - r["t_arrival"] for r in info if r["type"] == t])
         if len(lt):
@@ -586,10 +595,14 @@ def run_case(a):
         cg_scan(G, dev)
         return
     if a.case == "batched":
-        print(json.dumps(batched_bench(G, dev)))
+        for prec in (G.GN_PREC_MIXED, G.GN_PREC_FP64):
+            print(json.dumps(batched_bench(G, dev, precision=prec)), flush=True)
         return
     if a.case == "serve":
-        print(json.dumps(serve_bench(G)))
+        for prec in (G.GN_PREC_MIXED, G.GN_PREC_FP64):
+            print(json.dumps(serve_bench(G, precision=prec)), flush=True)
+        for prec in (G.GN_PREC_MIXED, G.GN_PREC_FP64):  # a load the GPU sustains
+            print(json.dumps(serve_bench(G, nreq=300, rate=50.0, precision=prec)), flush=True)
         return
     L, V = 64, 64 ** 3
     lat = G.Lattice(L, 0)

@@ -245,7 +245,7 @@ GN_API long long gn_cg_noalloc_max_volume(void);
  * beta_s, on one GPU.  Every trajectory is the reference's (the integrators of
  * moleculardynamics.c:859 / :1018 / :1234, energy of :299, Metropolis test
  * u <= exp(-dH) with sigma restored on reject); every solve is the
- * mixed-precision CG to a true relative residual `tol`, from x = 0.  The
+ * CG (mixed precision or FP64) to a true relative residual `tol`, from x = 0.  The
  * random numbers (momenta, pseudofermion sources, the Metropolis uniform) come
  * from the chain's own Philox4x64-10 stream, key (seed, stream id), counter
  * (trajectory number, field, site block): a chain's trajectory depends only on
@@ -259,6 +259,7 @@ typedef struct {
   int steps;      /* MD steps per trajectory (>= 1) */
   int integrator; /* GN_LFMN2VF, GN_LF2 or GN_LFMN2 */
   double tol;     /* relative tolerance of every solve, true residual (> 0) */
+  int precision;  /* GN_PREC_MIXED or GN_PREC_FP64 */
 } gn_ens_params;
 
 typedef struct {
@@ -307,7 +308,7 @@ GN_API int gn_ensemble_info(gn_ensemble *ens, int *group_blocks, long long *big_
 /* No counterpart in the reference.  A server keeps chains resident on the GPU
  * (sigma and its mass) and runs requests on them with continuous batching:
  *   GN_REQ_TRAJECTORY  one HMC trajectory of the chain (the ensemble's: the
- *                      parameters given at creation, mixed-precision solves);
+ *                      parameters given at creation, solves in their precision);
  *   GN_REQ_SOLVE       one solve of (M M^T) x = b at the chain's sigma, b ~ N(0, 1);
  *   GN_REQ_CONDENSATE  the estimate (1/n) sum_k xi_k . M^T (M M^T)^-1 xi_k / V
  *                      of tr M^-1 / V (condensate.c:142-145) from n Z2 vectors.
@@ -315,7 +316,7 @@ GN_API int gn_ensemble_info(gn_ensemble *ens, int *group_blocks, long long *big_
  * advances by one slice (a trajectory has one per MD step, a solve one, a
  * condensate one per two noise vectors), finished requests retire, and queued
  * ones are admitted in arrival order when their chain is free and their work
- * arrays (about 148 bytes per site) fit the memory budget.  A request's draws
+ * arrays (about 196 bytes per site) fit the memory budget.  A request's draws
  * come from its chain's Philox stream with its number among the chain's
  * requests (trajectories: the chain's trajectory number) as the counter, so its
  * result does not depend on the requests running beside it.  Times are seconds on the server's clock
@@ -338,12 +339,16 @@ typedef struct {
   long long cg_iterations;
 } gn_request_info;
 
-/* traj: the trajectories' integrator, steps, step size and the tolerance of
- * every solve.  mem_budget_bytes bounds the running requests' work arrays.
+/* traj: the trajectories' integrator, steps, step size, and the tolerance and
+ * precision of every solve.  mem_budget_bytes bounds the running requests'
+ * work arrays.
  * Team tiers (0 to 3): a chain with V >= tier_min_volume[t] (and below the
  * earlier tiers' bounds) runs on teams of tier_blocks[t] blocks; sizes >= 2,
  * each dividing the previous one, volumes decreasing; smaller chains run on
- * single blocks. */
+ * single blocks.  The top tier's teams grow to share the whole GPU among the
+ * running top-tier requests (tier_blocks[0] is their minimum size), so a
+ * request's result is bit for bit independent of the load below the top tier
+ * and agrees to the solver tolerance in it. */
 GN_API int gn_server_create(gn_server **srv, const gn_ens_params *traj, double mem_budget_bytes,
                             unsigned long long seed, int ntiers, const int *tier_blocks,
                             const long long *tier_min_volume, int device);

@@ -125,3 +125,22 @@ def test_autotuner_and_mixed_sizes():
     assert all(s["trajectories"] == 3 and s["failed"] == 0 for s in st)
     assert max(abs(s["last_dH"]) for s in st) < 5.0
     assert all(s["cg_iterations"] > 0 for s in st)
+
+
+def test_fp64_and_mixed_chains_agree():
+    """The same chains with FP64 and with mixed-precision solves (both to a
+    true relative residual of 1e-10): the trajectories agree to the solver
+    tolerance."""
+    import gn_b200 as G
+    Ls, betas = [8, 12, 16], [0.7, 0.9, 1.1]
+    out = {}
+    for prec in (G.GN_PREC_FP64, G.GN_PREC_MIXED):
+        p = G.Ensemble.params(0.08, 8, precision=prec)
+        with G.Ensemble(Ls, betas, seed=3) as e:
+            for c, (L, b) in enumerate(zip(Ls, betas)):
+                e.load_sigma(c, _sigma0(L, b, 50 + c))
+            e.run(p, 2)
+            out[prec] = ([e.store_sigma(c)[0] for c in range(3)], [s["sum_dH"] for s in e.stats()])
+    for a, b in zip(out[G.GN_PREC_FP64][0], out[G.GN_PREC_MIXED][0]):
+        assert np.max(np.abs(a - b)) / np.max(np.abs(a)) < 1e-7
+    assert np.allclose(out[G.GN_PREC_FP64][1], out[G.GN_PREC_MIXED][1], rtol=0, atol=1e-6)
