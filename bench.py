@@ -357,6 +357,11 @@ def run_ours(a, world, rank, local):
         batched["fp64"] = {k: v for k, v in batched_bench(G, dev, tune=False, precision=G.GN_PREC_FP64).items()
                            if k in ("value", "ms_per_ensemble_trajectory", "cg_iterations_per_chain_trajectory",
                                     "solver_gbs")}
+    serving = None
+    if world == 1:
+        serving = serve_bench(G)
+        serving["fp64"] = {k: v for k, v in serve_bench(G, precision=G.GN_PREC_FP64).items()
+                           if k in ("p50_ms", "p99_ms", "throughput_req_per_s")}
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -389,7 +394,8 @@ def run_ours(a, world, rank, local):
             "cpu_baseline": cpu,
             "clocks": mixed["clocks"],
             "gpu_launches": int(round(mixed["launches"] * a.steps)),
-            "batched": batched}
+            "batched": batched,
+            "serving": serving}
     if rank == 0:
         print(json.dumps(line), flush=True)
     lat.close()
