@@ -100,6 +100,14 @@ int gn_set_parity_mode(gn_context *ctx, int on) {
   });
 }
 
+int gn_set_reliable_interval(gn_context *ctx, int n) {
+  if (n < 1) return fail(GN_ERR_ARG, "reliable-update interval must be >= 1");
+  return guarded(ctx, [&](gn::Engine &E) {
+    E.reliable_every = n;
+    return GN_OK;
+  });
+}
+
 long long gn_volume(const gn_context *ctx) { return (ctx && ctx->eng) ? (long long)ctx->eng->V() : 0; }
 
 void gn_request_abort(gn_context *ctx, int on) {

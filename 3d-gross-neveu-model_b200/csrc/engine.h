@@ -78,6 +78,7 @@ class Engine {
   // energy and the condensate (set by gn_set_parity_mode and by the
   // operations run with precision GN_PREC_FP64_EXACT).
   bool exact = false;
+  int reliable_every = 100;  // mixed precision: a reliable update at least every this many iterations
 
   // One trajectory on the resident state; see gn_trajectory in gn_b200.h.
   int trajectory(const gn_hmc_params &hp, double (*gauss)(void), double (*uniform)(void), const double *pre_P,

@@ -12,7 +12,6 @@ namespace gn {
 
 constexpr int kMixedVecs = 4;  // r^, p^, t^, x^ per right-hand side
 constexpr double kDelta = 0.01;  // reliable update when |r^| drops by this factor
-constexpr int kReliableEvery = 100;
 
 void Engine::mixed_init() {
   const size_t V = size_t(V_);
@@ -64,7 +63,7 @@ int Engine::solve_mixed(const double *sm, const double *const *b, double *const 
   a.tol = tol;
   a.max_iter = max_iter;
   a.delta = kDelta;
-  a.n_ru = kReliableEvery;
+  a.n_ru = reliable_every;
   a.partials = partials_;
   a.bar = bar_;
   a.err = err_;

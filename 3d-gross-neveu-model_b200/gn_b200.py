@@ -134,6 +134,7 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
         "gn_launch_count": ([v], C.c_longlong),
         "gn_flush_l2": ([v], C.c_int),
         "gn_set_parity_mode": ([v, C.c_int], C.c_int),
+        "gn_set_reliable_interval": ([v, C.c_int], C.c_int),
         "gn_ensemble_create": ([C.POINTER(v), C.c_int, C.POINTER(C.c_int), _dp, C.POINTER(C.c_ulonglong),
                                 C.c_ulonglong, C.c_int], C.c_int),
         "gn_ensemble_destroy": ([v], None),
@@ -350,6 +351,10 @@ class Lattice:
     def set_parity_mode(self, on=True):
         """M^T and the energy in the reference's exact order (see GN_PREC_FP64_EXACT)."""
         self._check(self.lib.gn_set_parity_mode(self.ctx, int(on)))
+
+    def set_reliable_interval(self, n):
+        """Mixed precision: a reliable update at least every n inner iterations."""
+        self._check(self.lib.gn_set_reliable_interval(self.ctx, int(n)))
 
     def request_abort(self, on=True):
         self.lib.gn_request_abort(self.ctx, int(on))

@@ -66,7 +66,7 @@ def parse():
     ap.add_argument("--eps", type=float, default=0.05)
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--case", choices=["cg64", "dirac128", "dirac256", "traj64", "cgscan", "batched", "serve"], default=None,
+    ap.add_argument("--case", choices=["cg64", "dirac128", "dirac256", "traj64", "cgscan", "batched", "serve", "l128"], default=None,
                     help="run one small case for a profiler instead of the benchmark")
     return ap.parse_args()
 
@@ -354,9 +354,11 @@ def run_ours(a, world, rank, local):
     batched = None
     if world == 1:
         batched = batched_bench(G, dev)
-        batched["fp64"] = {k: v for k, v in batched_bench(G, dev, tune=False, precision=G.GN_PREC_FP64).items()
+        lay = (batched["layout"]["group_blocks"], batched["layout"]["big_min_volume"])
+        batched["fp64"] = {k: v for k, v in batched_bench(G, dev, precision=G.GN_PREC_FP64, layout=lay).items()
                            if k in ("value", "ms_per_ensemble_trajectory", "cg_iterations_per_chain_trajectory",
                                     "solver_gbs")}
+    l128 = l128_case(G, dev) if world == 1 else None
     serving = None
     if world == 1:
         serving = serve_bench(G)
@@ -395,7 +397,8 @@ def run_ours(a, world, rank, local):
             "clocks": mixed["clocks"],
             "gpu_launches": int(round(mixed["launches"] * a.steps)),
             "batched": batched,
-            "serving": serving}
+            "serving": serving,
+            "mixed_precision_L128": l128}
     if rank == 0:
         print(json.dumps(line), flush=True)
     lat.close()
@@ -452,7 +455,7 @@ def kernel_roofline(lat, stream, a, G):
                     f"{(2 * 5 * 4 + 8 * 3) * V / 1e6:.0f} MB is L2-resident within the solve"}
 
 
-def batched_bench(G, dev, nchains=256, ntraj=2, warmup=1, tune=True, precision=None):
+def batched_bench(G, dev, nchains=256, ntraj=2, warmup=1, tune=True, precision=None, layout=None):
     """The batched ensemble: nchains chains with L uniform in {8, 12, 16, 24, 32,
     48} (seeded), beta_s on a uniform grid over [0.5, 1.2], LFMN2VF 8 x eps 0.08,
     every solve mixed precision to 1e-10 (true relative residual), device
@@ -469,7 +472,10 @@ def batched_bench(G, dev, nchains=256, ntraj=2, warmup=1, tune=True, precision=N
     with G.Ensemble(Ls, betas, seed=1231) as e:
         for c, (L, b) in enumerate(zip(Ls, betas)):
             e.load_sigma(c, rng.normal(0.0, np.sqrt(2.0 / (NFLAV * b)), L ** 3))
-        layout = e.tune(p) if tune else (1, 0)
+        if layout is not None:
+            e.set_layout(*layout)
+        else:
+            layout = e.tune(p) if tune else (1, 0)
         e.run(p, warmup)
         e.stats(reset=True)
         st = torch.cuda.ExternalStream(e.stream, device=dev)
@@ -553,6 +559,68 @@ def serve_bench(G, nreq=600, rate=200.0, warm=24, seed=5, precision=None):
     return out
 
 
+def l128_case(G, dev, betas=(0.7, 0.85, 1.0), L=128, md_steps=10, eps=0.05, tol=1e-10, reliable=50):
+    """Mixed precision at L = 128 (V = 2,097,152): FP32 fields and inner CG,
+    FP64 reliable updates at least every `reliable` iterations, FP64 dH and
+    Metropolis.  Per beta_s, against the FP64 path on the same fields (sigma
+    ~ N(0, 2/(N_f beta_s)), chi ~ N(0, 1), phi = M chi): the relative error of
+    x = (M M^T)^-1 phi and of the sigma force (both solved to a true relative
+    residual of 1e-10), |dH_mixed - dH_fp64| of one trajectory from the same
+    state and draws (LFMN2VF md_steps x eps), the iteration counts and the
+    solve and trajectory times (CUDA events)."""
+    import torch
+    rows = []
+    V = L ** 3
+    for beta in betas:
+        rng = np.random.default_rng(int(beta * 100))
+        sigma = rng.normal(0.0, np.sqrt(2.0 / (NFLAV * beta)), V)
+        draws = torch.tensor(rng.normal(size=3 * V), dtype=torch.float64, device=dev)
+        with G.Lattice(L, dev.index) as lat:
+            lat.set_reliable_interval(reliable)
+            st = torch.cuda.ExternalStream(lat.stream, device=dev)
+            lat.load_sigma(sigma)
+            sm = lat.store_sigma()[1]
+            phi = np.stack([lat.dirac(sm, rng.normal(size=V), G.GN_OP_M) for _ in range(2)])
+            row = {"beta_s": beta}
+            out = {}
+            for prec, name in ((G.GN_PREC_FP64, "fp64"), (G.GN_PREC_MIXED, "mixed")):
+                lat.load_sigma(sigma)  # the previous pass's trajectory moved sigma
+                lat.write_state(G.GN_F_PHI, phi.reshape(-1))
+                e0, e1 = cuda_events()
+                e0.record(st)
+                infos, stt = lat.cg_device(lat.field_ptr(G.GN_F_SM), lat.field_ptr(G.GN_F_PHI),
+                                           lat.field_ptr(G.GN_F_X), 2, 1, tol, 1, True, 0, prec)
+                e1.record(st)
+                e1.synchronize()
+                x = lat.read_state(G.GN_F_X).copy()
+                F, X, Y, finfo, _ = lat.sigma_force(beta, sigma, sm, phi, np.zeros((2, V)), tol,
+                                                    precision=prec)
+                lat.load_sigma(sigma)
+                t0, t1 = cuda_events()
+                t0.record(st)
+                r = lat.trajectory_device(draws.data_ptr(), draws.data_ptr() + 8 * V, beta, eps, md_steps, None,
+                                          tol_medium=tol, tol_high=tol, relative=True, precision=prec)
+                t1.record(st)
+                t1.synchronize()
+                out[name] = dict(x=x, F=F, dH=r["dH"])
+                row[name] = {"iterations": int(max(i["inner_iterations"] for i in infos)),
+                             "reliable_updates": int(sum(i["reliable_updates"] for i in infos)),
+                             "solve_ms": e0.elapsed_time(e1), "trajectory_ms": t0.elapsed_time(t1),
+                             "trajectory_cg_iterations": r["cg_iterations"]}
+            row["x_rel_err"] = float(np.linalg.norm(out["mixed"]["x"] - out["fp64"]["x"]) /
+                                     np.linalg.norm(out["fp64"]["x"]))
+            row["force_rel_err"] = float(np.linalg.norm(out["mixed"]["F"] - out["fp64"]["F"]) /
+                                         np.linalg.norm(out["fp64"]["F"]))
+            row["dH_abs_diff"] = abs(out["mixed"]["dH"] - out["fp64"]["dH"])
+            row["dH_fp64"] = out["fp64"]["dH"]
+            row["iteration_overhead"] = row["mixed"]["iterations"] / row["fp64"]["iterations"] - 1.0
+            row["solve_speedup"] = row["fp64"]["solve_ms"] / row["mixed"]["solve_ms"]
+            row["trajectory_speedup"] = row["fp64"]["trajectory_ms"] / row["mixed"]["trajectory_ms"]
+        rows.append(row)
+    return {"case": f"mixed precision at L={L}, reliable updates every {reliable} iterations, tol {tol:g}",
+            "rows": rows}
+
+
 def dirac_roofline(G, stream, dev, reps=20, L=256):
     """Dirac M on one FP64 plane at L = 256 (V = 16,777,216): psi, sm and the
     output are 384 MB, three times the L2, so back-to-back launches run from
@@ -600,9 +668,14 @@ def run_case(a):
     if a.case == "cgscan":
         cg_scan(G, dev)
         return
+    if a.case == "l128":
+        print(json.dumps(l128_case(G, dev)))
+        return
     if a.case == "batched":
-        for prec in (G.GN_PREC_MIXED, G.GN_PREC_FP64):
-            print(json.dumps(batched_bench(G, dev, precision=prec)), flush=True)
+        r = batched_bench(G, dev)
+        print(json.dumps(r), flush=True)
+        lay = (r["layout"]["group_blocks"], r["layout"]["big_min_volume"])
+        print(json.dumps(batched_bench(G, dev, precision=G.GN_PREC_FP64, layout=lay)), flush=True)
         return
     if a.case == "serve":
         for prec in (G.GN_PREC_MIXED, G.GN_PREC_FP64):

@@ -102,6 +102,11 @@ GN_API void gn_request_abort(gn_context *ctx, int on);
  * M^T, gn_energy): on = the reference's exact order of operations. */
 GN_API int gn_set_parity_mode(gn_context *ctx, int on);
 
+/* Mixed precision: a reliable update (x folded into FP64, the true residual
+ * recomputed) at least every n inner iterations, besides the ones the
+ * residual's drop by 100x triggers.  Default 100; n >= 1. */
+GN_API int gn_set_reliable_interval(gn_context *ctx, int n);
+
 /* ---- host-buffer operators (one call = one reference function) -------- */
 
 /* ComputeFullSigmaMass, sigma.c:75-94: sm(x) = 1/8 sum of sigma over the 8
