@@ -593,7 +593,10 @@ def l128_case(G, dev, betas=(0.7, 0.85, 1.0), L=128, md_steps=10, eps=0.05, tol=
                 e1.record(st)
                 e1.synchronize()
                 x = lat.read_state(G.GN_F_X).copy()
-                F, X, Y, finfo, _ = lat.sigma_force(beta, sigma, sm, phi, np.zeros((2, V)), tol,
+                # gn_sigma_force takes the reference's absolute tolerance: the
+                # relative 1e-10 of this case, for the smaller of the two |phi_f|
+                tol_abs = tol * float(min(np.linalg.norm(phi[0]), np.linalg.norm(phi[1])))
+                F, X, Y, finfo, _ = lat.sigma_force(beta, sigma, sm, phi, np.zeros((2, V)), tol_abs,
                                                     precision=prec)
                 lat.load_sigma(sigma)
                 t0, t1 = cuda_events()
