@@ -124,7 +124,7 @@ class Engine {
   double *table_ = nullptr;
   // solver workspace
   double *cg_work_ = nullptr;  // kMaxRhs * 4 vectors * 2 planes * V
-  float *mx_work_ = nullptr;   // mixed precision: kMaxRhs * 4 vectors * 2 planes * V
+  float *mx_work_ = nullptr;   // mixed precision: kMaxRhs * 5 vectors * 2 planes * V
   float *sm32_ = nullptr;
   double *partials_ = nullptr;
   double *h_partials_ = nullptr;

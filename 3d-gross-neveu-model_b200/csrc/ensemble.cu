@@ -123,7 +123,7 @@ Ensemble::Ensemble(int n, const int *L, const double *beta_s, const unsigned lon
     double *s0 = dv(1), *s1 = dv(1), *sm = dv(1), *P = dv(1), *F = dv(1), *save = dv(1);
     double *chi = dv(2), *phi = dv(2), *X = dv(2), *Y = dv(2), *t64 = dv(2);
     double *r64 = dv(2), *pa64 = dv(2), *pb64 = dv(2);
-    float *sm32 = fv(1), *rh = fv(2), *ph = fv(2), *th = fv(2), *xh = fv(2);
+    float *sm32 = fv(1), *rh = fv(2), *ph = fv(2), *uh = fv(2), *ah = fv(2), *xh = fv(2);
     if (ch) {
       ch->g = make_geom(L[c]);
       ch->w = row_width(L[c], 4);
@@ -143,7 +143,8 @@ Ensemble::Ensemble(int n, const int *L, const double *beta_s, const unsigned lon
       ch->sm32 = sm32;
       ch->rh = rh;
       ch->ph = ph;
-      ch->th = th;
+      ch->uh = uh;
+      ch->ah = ah;
       ch->xh = xh;
       ch->r64 = r64;
       ch->pa64 = pa64;

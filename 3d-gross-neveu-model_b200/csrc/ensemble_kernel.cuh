@@ -60,7 +60,7 @@ struct EnsChain {
   double *sm, *P, *F, *sigma_save;
   double *chi, *phi, *X, *Y;  // two flavour planes each
   double *t64;                // solver FP64 scratch, two planes
-  float *sm32, *rh, *ph, *th, *xh;  // solver FP32 vectors, two planes each
+  float *sm32, *rh, *ph, *uh, *ah, *xh;  // solver FP32 vectors, two planes each
   double *r64, *pa64, *pb64;  // FP64 solver vectors (with t64), two planes each
   int precision;              // GN_PREC_MIXED or GN_PREC_FP64
 };
@@ -223,12 +223,14 @@ static __device__ __noinline__ bool ens_run_chain(const EnsLaunch &L, int c, Tea
           a.t64[k] = ch.t64 + off;
           a.rh[k] = ch.rh + off;
           a.ph[k] = ch.ph + off;
-          a.th[k] = ch.th + off;
+          a.uh[k] = ch.uh + off;
+          a.ah[k] = ch.ah + off;
           a.xh[k] = ch.xh + off;
         }
         a.nrhs = nrhs;
         a.variant = 1;
         a.rel = 1;
+        a.scheme = mixed_scheme(g.V, nrhs, 1);
         a.tol = L.tol;
         a.max_iter = (long long)V + 1;
         a.delta = L.delta;

@@ -10,7 +10,7 @@
 
 namespace gn {
 
-constexpr int kMixedVecs = 4;  // r^, p^, t^, x^ per right-hand side
+constexpr int kMixedVecs = 5;  // r^, p^, u^, a^, x^ per right-hand side
 constexpr double kDelta = 0.01;  // reliable update when |r^| drops by this factor
 
 void Engine::mixed_init() {
@@ -54,12 +54,14 @@ int Engine::solve_mixed(const double *sm, const double *const *b, double *const 
     a.t64[k] = cg_work_ + size_t(k) * 4 * 2 * V;
     a.rh[k] = w;
     a.ph[k] = w + 2 * V;
-    a.th[k] = w + 4 * V;
-    a.xh[k] = w + 6 * V;
+    a.uh[k] = w + 4 * V;
+    a.ah[k] = w + 6 * V;
+    a.xh[k] = w + 8 * V;
   }
   a.nrhs = nrhs;
   a.variant = variant;
   a.rel = rel;
+  a.scheme = mixed_scheme(V_, nrhs, ncomp);
   a.tol = tol;
   a.max_iter = max_iter;
   a.delta = kDelta;

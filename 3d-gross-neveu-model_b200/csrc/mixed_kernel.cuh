@@ -13,12 +13,33 @@
 // passes the tolerance; the solve stops only on the FP64 true residual, so its
 // stopping rule is the same as the FP64 solver's.
 //
-// Inner iteration, two phases (11 FP32 words per site and RHS):
+// Two inner iterations, chosen per solve by MixedArgs::scheme:
+//
+// kMixedSplit -- Chronopoulos & Gear's CG (J. Comput. Appl. Math. 25 (1989)
+// 153), whose two global sums g = (r,r) and d = (r, A r) = |M^T r|^2 are taken
+// together, with A = M M^T applied as two stencil sweeps:
+//   S1: u^ = M^T r^, sums (r^,r^), (u^,u^)                   -> phase end with sums
+//       beta = g / g_old, alpha = g / (d - beta g / alpha_old)   (beta = 0 first;
+//       a non-positive denominator restarts the direction)
+//   S2: a^ <- M u^ + beta a^ (= A p^), p^ <- r^ + beta p^,
+//       x^ += alpha p^, r^ -= alpha a^                         -> team barrier
+// One phase end with sums and one plain barrier per iteration (about 1.5 us
+// against 3.2 - 3.7 us for a phase end with sums on B200): the faster scheme
+// while the FP32 vectors stay in L2 and the iteration is latency-bound.
+//
+// kMixedTwoPhase -- the CG of the FP64 solver, two phase ends with sums:
 //   A: p^ <- r^ + beta p^, t^ <- M^T r^ + beta t^ (= M^T p^), sum t^2
 //   B: x^ += alpha p^, r^ -= alpha M t^, sum r^2
-// Reliable update, two phases (FP64):
+// Four FP32 vectors instead of five (t^ lives in u^'s array): the faster
+// scheme once the working set no longer fits in L2.  Both move 13 FP32 words
+// per site and RHS per iteration.
+//
+// Reliable update (FP64), when the iterated residual has dropped far enough
+// (in kMixedSplit S2 is then skipped for that system):
 //   C: t = M^T (x + x^) (on the fly at the 7 points)
 //   D: x += x^, x^ = 0, r = b - M t, r^ = (float) r, sum r^2
+// and the iteration goes on from the true residual, keeping p^ (and a^), as
+// the reliable-update CG of Clark et al. keeps p.
 // The FP32 phases sweep row items of W sites (rowvec.cuh; W = 4, one float4
 // per vector, when 4 divides L/2), the FP64 phases items of min(W, 2) sites;
 // a work unit is one (system, item) pair, as in cg_kernel.cuh.
@@ -27,6 +48,19 @@
 
 namespace gn {
 
+enum MixedScheme : int { kMixedTwoPhase = 0, kMixedSplit = 1 };
+
+// The split iteration while its FP32 vectors (five per system and plane, and
+// sm) take at most 48 MB: measured on B200 with two systems, it is faster at
+// L = 96 (39 MB; 17.9 against 18.3 us per iteration) and slower at L = 128
+// (92 MB, a working set the 126 MB L2 no longer holds across the sweeps; 33.4
+// against 29.1 us).
+constexpr double kMixedSplitMaxBytes = 48.0 * (1 << 20);
+__host__ __device__ inline int mixed_scheme(int64_t V, int nrhs, int ncomp) {
+  const double bytes = double(5 * nrhs * ncomp + 1) * double(V) * 4.0;
+  return bytes <= kMixedSplitMaxBytes ? kMixedSplit : kMixedTwoPhase;
+}
+
 struct MixedArgs {
   Geom g;
   const double *sm;
@@ -34,13 +68,15 @@ struct MixedArgs {
   const double *b[kMaxRhs];
   double *x[kMaxRhs];
   double *t64[kMaxRhs];
-  float *rh[kMaxRhs];
-  float *ph[kMaxRhs];
-  float *th[kMaxRhs];
-  float *xh[kMaxRhs];
+  float *rh[kMaxRhs];  // r^
+  float *ph[kMaxRhs];  // p^
+  float *uh[kMaxRhs];  // u^ = M^T r^ (kMixedSplit) or t^ = M^T p^ (kMixedTwoPhase)
+  float *ah[kMaxRhs];  // a^ = A p^
+  float *xh[kMaxRhs];  // x^
   int nrhs;
   int variant;
   int rel;
+  int scheme;  // MixedScheme
   double tol;
   long long max_iter;
   double delta;  // reliable update when |r^| < delta * max |r^| since the last one
@@ -56,8 +92,9 @@ struct MixedArgs {
 struct MixedShared {
   double alpha[kMaxRhs], beta[kMaxRhs], rr[kMaxRhs], tau[kMaxRhs], rmax[kMaxRhs], r2[kMaxRhs], b2[kMaxRhs];
   int active[kMaxRhs], status[kMaxRhs], ru[kMaxRhs], since[kMaxRhs], nru[kMaxRhs], all[kMaxRhs];
+  int first[kMaxRhs], step[kMaxRhs];
   long long iters[kMaxRhs];
-  SysList run, every, upd;  // systems iterating / all systems / taking a reliable update
+  SysList run, every, upd, stp;  // systems iterating / all / taking a reliable update / taking a CG step
 };
 
 // One mixed-precision solve by a team (all its threads call it; a.bar,
@@ -69,9 +106,9 @@ __device__ __forceinline__ void mixed_solve(const MixedArgs &a, Team &team, Sync
   double *const s_alpha = ms.alpha, *const s_beta = ms.beta, *const s_rr = ms.rr, *const s_tau = ms.tau;
   double *const s_rmax = ms.rmax, *const s_r2 = ms.r2, *const s_b2 = ms.b2;
   int *const s_active = ms.active, *const s_status = ms.status, *const s_ru = ms.ru, *const s_since = ms.since;
-  int *const s_nru = ms.nru, *const s_all = ms.all;
+  int *const s_nru = ms.nru, *const s_all = ms.all, *const s_first = ms.first, *const s_step = ms.step;
   long long *const s_iters = ms.iters;
-  SysList &s_run = ms.run, &s_every = ms.every, &s_upd = ms.upd;
+  SysList &s_run = ms.run, &s_every = ms.every, &s_upd = ms.upd, &s_stp = ms.stp;
 
   const Geom g = a.g;
   const uint32_t V = uint32_t(g.V);
@@ -89,6 +126,8 @@ __device__ __forceinline__ void mixed_solve(const MixedArgs &a, Team &team, Sync
     s_ru[k] = 0;
     s_since[k] = 0;
     s_nru[k] = 0;
+    s_first[k] = 1;
+    s_step[k] = 0;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -168,7 +207,9 @@ __device__ __forceinline__ void mixed_solve(const MixedArgs &a, Team &team, Sync
     if (threadIdx.x == 0) sys_list_from(s_run, s_active, a.nrhs);
     __syncthreads();
   }
-  // x = 0, x^ = 0, r^ = p^ = (float) b, sm32 = (float) sm ; sums r^2 (FP32 values), b^2
+  const bool split = a.scheme == kMixedSplit;
+  // x = 0, x^ = 0, r^ = (float) b, p^ = (float) b (two-phase) or 0 (split),
+  // a^ = 0, sm32 = (float) sm; sums r^2 (FP32 values), b^2
   zero_acc();
   if (ok) {
     for (uint32_t j = team.tid; j < NI64; j += team.nthreads) {
@@ -184,9 +225,6 @@ __device__ __forceinline__ void mixed_solve(const MixedArgs &a, Team &team, Sync
       const uint32_t own = make_item<W64>(g, j).own;
       const double *bk = pick<NR>(a.b, k);
       double *xk = pick<NR>(a.x, k);
-      float *xhk = pick<NR>(a.xh, k);
-      float *rhk = pick<NR>(a.rh, k);
-      float *phk = pick<NR>(a.ph, k);
 #pragma unroll
       for (int c = 0; c < NC; c++) {
         const size_t off = size_t(c) * V + own;
@@ -205,9 +243,10 @@ __device__ __forceinline__ void mixed_solve(const MixedArgs &a, Team &team, Sync
         acc_add<NR>(acc, k, sf);
         acc_add<NR>(acc, NR + k, sb);
         vstore<double, W64>(xk + off, z64);
-        vstore<float, W64>(xhk + off, z32);
-        vstore<float, W64>(rhk + off, bf);
-        vstore<float, W64>(phk + off, bf);
+        vstore<float, W64>(pick<NR>(a.xh, k) + off, z32);
+        vstore<float, W64>(pick<NR>(a.ph, k) + off, split ? z32 : bf);
+        vstore<float, W64>(pick<NR>(a.ah, k) + off, z32);
+        vstore<float, W64>(pick<NR>(a.rh, k) + off, bf);
       }
     });
   }
@@ -237,113 +276,182 @@ __device__ __forceinline__ void mixed_solve(const MixedArgs &a, Team &team, Sync
   for (; ok && it < a.max_iter; it++) {
     if (s_run.n == 0) break;
     // the host's abort request lives in mapped host memory: one thread reads it
-    // every 16 iterations, and the value is only used at the end of phase B
+    // every 16 passes, and the value is only used at the end of the pass's
+    // last phase with sums
     int abort_req = 0;
     if (team.brank == 0 && threadIdx.x == 0 && a.abort_flag != nullptr && (it & 15) == 0)
       abort_req = *(volatile const int *)a.abort_flag;
-    // A: p^ = r^ + beta p^, t^ = M^T p^ = M^T r^ + beta t^ (linearity: only r^
-    // is gathered; p^ and t^ are updated in place at the unit's own sites)
-    zero_acc();
-    for_units(NI, s_run, team, [&](int k, uint32_t j) {
-      const RowItem ri = make_item<W>(g, j);
-      float smi[W];
-      vload<float, W>(a.sm32 + ri.own, smi);
-      const float beta = float(s_beta[k]);
-      float *const pk = pick<NR>(a.ph, k);
-      const float *rk = pick<NR>(a.rh, k);
-      float *tk = pick<NR>(a.th, k);
+    if (split) {
+      // S1: u^ = M^T r^, sums (r^,r^), (u^,u^)
+      zero_acc();
+      for_units(NI, s_run, team, [&](int k, uint32_t j) {
+        const RowItem ri = make_item<W>(g, j);
+        float smi[W];
+        vload<float, W>(a.sm32 + ri.own, smi);
+        const float *rk = pick<NR>(a.rh, k);
+        float *uk = pick<NR>(a.uh, k);
 #pragma unroll
-      for (int c = 0; c < NC; c++) {
-        const size_t off = size_t(c) * V;
-        Nb<float> n[W];
-        float ti[W];
-        if (it == 0) {  // p^ = b^ (set above): t^ = M^T p^
-          gather_item<float, W>(ri, pk + off, n);
-          item_Mt<float, W>(ri, smi, n, ti);
-        } else {
-          float u[W], told[W], pold[W];
+        for (int c = 0; c < NC; c++) {
+          const size_t off = size_t(c) * V;
+          Nb<float> n[W];
+          float u[W];
           gather_item<float, W>(ri, rk + off, n);
-          vload<float, W>(tk + off + ri.own, told);
-          vload<float, W>(pk + off + ri.own, pold);
           item_Mt<float, W>(ri, smi, n, u);
+          vstore<float, W>(uk + off + ri.own, u);
+          double sg = 0.0, sd = 0.0;
 #pragma unroll
           for (int e = 0; e < W; e++) {
-            ti[e] = fmaf(beta, told[e], u[e]);
-            pold[e] = fmaf(beta, pold[e], n[e].c);
+            sg += double(n[e].c) * double(n[e].c);
+            sd += double(u[e]) * double(u[e]);
           }
-          vstore<float, W>(pk + off + ri.own, pold);
+          acc_add<NR>(acc, k, sg);
+          acc_add<NR>(acc, NR + k, sd);
         }
-        vstore<float, W>(tk + off + ri.own, ti);
-        double st = 0.0;
-#pragma unroll
-        for (int e = 0; e < W; e++) st += double(ti[e]) * double(ti[e]);
-        acc_add<NR>(acc, k, st);
-      }
-    });
-    ok = end_phase<NR>(acc, sh, team);
-    if (!ok) break;
-    if (threadIdx.x < kMaxRhs) {
-      const int k = threadIdx.x;
-      if (k < a.nrhs && s_active[k]) s_alpha[k] = s_rr[k] / s_val[k];
-    }
-    __syncthreads();
-    // B: x^ += alpha p^, r^ -= alpha M t^
-    zero_acc();
-    for_units(NI, s_run, team, [&](int k, uint32_t j) {
-      const RowItem ri = make_item<W>(g, j);
-      float smi[W];
-      vload<float, W>(a.sm32 + ri.own, smi);
-      const float alpha = float(s_alpha[k]);
-      const float *const pn = pick<NR>(a.ph, k);
-      const float *tk = pick<NR>(a.th, k);
-      float *xhk = pick<NR>(a.xh, k);
-      float *rk = pick<NR>(a.rh, k);
-#pragma unroll
-      for (int c = 0; c < NC; c++) {
-        const size_t off = size_t(c) * V + ri.own;
-        Nb<float> n[W];
-        float ap[W], pv[W], xv[W], rv[W];
-        gather_item<float, W>(ri, tk + size_t(c) * V, n);
-        vload<float, W>(pn + off, pv);
-        vload<float, W>(xhk + off, xv);
-        vload<float, W>(rk + off, rv);
-        item_M<float, W>(ri, smi, n, ap);
-        double sr = 0.0;
-#pragma unroll
-        for (int e = 0; e < W; e++) {
-          xv[e] = fmaf(alpha, pv[e], xv[e]);
-          rv[e] = fmaf(-alpha, ap[e], rv[e]);
-          sr += double(rv[e]) * double(rv[e]);
+      });
+      ok = end_phase<2 * NR>(acc, sh, team, abort_req);
+      if (!ok) break;
+      if (threadIdx.x < kMaxRhs) {
+        const int k = threadIdx.x;
+        s_ru[k] = 0;
+        s_step[k] = 0;
+        if (k < a.nrhs && s_active[k]) {
+          const double gn = s_val[k], dn = s_val[NR + k];
+          const double rn = sqrt(gn);
+          s_r2[k] = gn;
+          if (rn > s_rmax[k]) s_rmax[k] = rn;
+          if (rn < s_tau[k] || rn < a.delta * s_rmax[k] || s_since[k] >= a.n_ru || !(rn == rn)) {
+            s_ru[k] = 1;  // the true residual replaces r^; a later S1 takes the step
+          } else {
+            double bt = 0.0, den = dn;
+            if (!s_first[k]) {
+              bt = gn / s_rr[k];
+              den = dn - bt * gn / s_alpha[k];
+              if (!(den > 0.0)) {
+                bt = 0.0;
+                den = dn;
+              }
+            }
+            s_first[k] = 0;
+            s_beta[k] = bt;
+            s_alpha[k] = gn / den;
+            s_rr[k] = gn;
+            s_since[k]++;
+            s_step[k] = 1;
+          }
         }
-        acc_add<NR>(acc, k, sr);
-        vstore<float, W>(xhk + off, xv);
-        vstore<float, W>(rk + off, rv);
       }
-    });
-    ok = end_phase<NR>(acc, sh, team, abort_req);
-    if (!ok) break;
-    const int abort_seen = sh.flag;  // block 0's abort flag (the next phase ends overwrite sh.flag)
-    if (threadIdx.x < kMaxRhs) {
-      const int k = threadIdx.x;
-      s_ru[k] = 0;
-      if (k < a.nrhs && s_active[k]) {
-        const double r2 = s_val[k];
-        const double rn = sqrt(r2);
-        s_since[k]++;
-        if (rn > s_rmax[k]) s_rmax[k] = rn;
-        if (rn < s_tau[k] || rn < a.delta * s_rmax[k] || s_since[k] >= a.n_ru || !(rn == rn)) {
-          s_ru[k] = 1;
-          s_r2[k] = r2;  // beta is formed from the true residual below
-        } else {
-          s_beta[k] = r2 / s_rr[k];
-          s_rr[k] = r2;
+    } else {
+      // A: p^ = r^ + beta p^, t^ = M^T p^ = M^T r^ + beta t^ (linearity: only r^
+      // is gathered; p^ and t^ are updated in place at the unit's own sites)
+      zero_acc();
+      for_units(NI, s_run, team, [&](int k, uint32_t j) {
+        const RowItem ri = make_item<W>(g, j);
+        float smi[W];
+        vload<float, W>(a.sm32 + ri.own, smi);
+        const float beta = float(s_beta[k]);
+        float *const pk = pick<NR>(a.ph, k);
+        const float *rk = pick<NR>(a.rh, k);
+        float *tk = pick<NR>(a.uh, k);
+#pragma unroll
+        for (int c = 0; c < NC; c++) {
+          const size_t off = size_t(c) * V;
+          Nb<float> n[W];
+          float ti[W];
+          if (it == 0) {  // p^ = b^ (set above): t^ = M^T p^
+            gather_item<float, W>(ri, pk + off, n);
+            item_Mt<float, W>(ri, smi, n, ti);
+          } else {
+            float u[W], told[W], pold[W];
+            gather_item<float, W>(ri, rk + off, n);
+            vload<float, W>(tk + off + ri.own, told);
+            vload<float, W>(pk + off + ri.own, pold);
+            item_Mt<float, W>(ri, smi, n, u);
+#pragma unroll
+            for (int e = 0; e < W; e++) {
+              ti[e] = fmaf(beta, told[e], u[e]);
+              pold[e] = fmaf(beta, pold[e], n[e].c);
+            }
+            vstore<float, W>(pk + off + ri.own, pold);
+          }
+          vstore<float, W>(tk + off + ri.own, ti);
+          double st = 0.0;
+#pragma unroll
+          for (int e = 0; e < W; e++) st += double(ti[e]) * double(ti[e]);
+          acc_add<NR>(acc, k, st);
+        }
+      });
+      ok = end_phase<NR>(acc, sh, team);
+      if (!ok) break;
+      if (threadIdx.x < kMaxRhs) {
+        const int k = threadIdx.x;
+        if (k < a.nrhs && s_active[k]) s_alpha[k] = s_rr[k] / s_val[k];
+      }
+      __syncthreads();
+      // B: x^ += alpha p^, r^ -= alpha M t^
+      zero_acc();
+      for_units(NI, s_run, team, [&](int k, uint32_t j) {
+        const RowItem ri = make_item<W>(g, j);
+        float smi[W];
+        vload<float, W>(a.sm32 + ri.own, smi);
+        const float alpha = float(s_alpha[k]);
+        const float *const pn = pick<NR>(a.ph, k);
+        const float *tk = pick<NR>(a.uh, k);
+        float *xhk = pick<NR>(a.xh, k);
+        float *rk = pick<NR>(a.rh, k);
+#pragma unroll
+        for (int c = 0; c < NC; c++) {
+          const size_t off = size_t(c) * V + ri.own;
+          Nb<float> n[W];
+          float ap[W], pv[W], xv[W], rv[W];
+          gather_item<float, W>(ri, tk + size_t(c) * V, n);
+          vload<float, W>(pn + off, pv);
+          vload<float, W>(xhk + off, xv);
+          vload<float, W>(rk + off, rv);
+          item_M<float, W>(ri, smi, n, ap);
+          double sr = 0.0;
+#pragma unroll
+          for (int e = 0; e < W; e++) {
+            xv[e] = fmaf(alpha, pv[e], xv[e]);
+            rv[e] = fmaf(-alpha, ap[e], rv[e]);
+            sr += double(rv[e]) * double(rv[e]);
+          }
+          acc_add<NR>(acc, k, sr);
+          vstore<float, W>(xhk + off, xv);
+          vstore<float, W>(rk + off, rv);
+        }
+      });
+      ok = end_phase<NR>(acc, sh, team, abort_req);
+      if (!ok) break;
+      if (threadIdx.x < kMaxRhs) {
+        const int k = threadIdx.x;
+        s_ru[k] = 0;
+        if (k < a.nrhs && s_active[k]) {
+          const double r2 = s_val[k];
+          const double rn = sqrt(r2);
+          s_since[k]++;
           s_r2[k] = r2;
+          if (rn > s_rmax[k]) s_rmax[k] = rn;
+          if (rn < s_tau[k] || rn < a.delta * s_rmax[k] || s_since[k] >= a.n_ru || !(rn == rn)) {
+            s_ru[k] = 1;  // beta is formed from the true residual below
+          } else {
+            s_beta[k] = r2 / s_rr[k];
+            s_rr[k] = r2;
+          }
         }
       }
     }
+    const int abort_seen = sh.flag;  // block 0's abort flag (the next phase ends overwrite sh.flag)
     __syncthreads();
-    if (threadIdx.x == 0) sys_list_from(s_upd, s_ru, a.nrhs);
+    if (threadIdx.x == 0) {
+      sys_list_from(s_upd, s_ru, a.nrhs);
+      if (split) sys_list_from(s_stp, s_step, a.nrhs);
+    }
     __syncthreads();
+    if (abort_seen != 0) {  // block 0 saw the host's abort request
+      if (threadIdx.x == 0 && team.brank == 0) atomicExch(team.err, 2);
+      ok = false;
+      break;
+    }
     if (s_upd.n > 0) {
       // C: t = M^T (x + x^) in FP64
       for_units(NI64, s_upd, team, [&](int k, uint32_t j) {
@@ -431,7 +539,7 @@ __device__ __forceinline__ void mixed_solve(const MixedArgs &a, Team &team, Sync
             s_active[k] = 0;
             s_status[k] = kCgConverged;
             s_iters[k] = it + 1;
-          } else {
+          } else if (!split) {
             s_beta[k] = r2 / s_rr[k];
             s_rr[k] = r2;
           }
@@ -441,10 +549,45 @@ __device__ __forceinline__ void mixed_solve(const MixedArgs &a, Team &team, Sync
       if (threadIdx.x == 0) sys_list_from(s_run, s_active, a.nrhs);
       __syncthreads();
     }
-    if (abort_seen != 0) {  // block 0 saw the host's abort request at the end of phase B
-      if (threadIdx.x == 0 && team.brank == 0) atomicExch(team.err, 2);
-      ok = false;
-      break;
+    if (split && s_stp.n > 0) {
+      // S2: a^ = M u^ + beta a^, p^ = r^ + beta p^, x^ += alpha p^, r^ -= alpha a^
+      for_units(NI, s_stp, team, [&](int k, uint32_t j) {
+        const RowItem ri = make_item<W>(g, j);
+        float smi[W];
+        vload<float, W>(a.sm32 + ri.own, smi);
+        const float alpha = float(s_alpha[k]), beta = float(s_beta[k]);
+        const float *uk = pick<NR>(a.uh, k);
+#pragma unroll
+        for (int c = 0; c < NC; c++) {
+          const size_t off = size_t(c) * V;
+          const size_t o = off + ri.own;
+          Nb<float> n[W];
+          float w[W], av[W], pv[W], xv[W], rv[W];
+          gather_item<float, W>(ri, uk + off, n);
+          float *const ak = pick<NR>(a.ah, k) + o;
+          float *const pk = pick<NR>(a.ph, k) + o;
+          float *const xk = pick<NR>(a.xh, k) + o;
+          float *const rk = pick<NR>(a.rh, k) + o;
+          vload<float, W>(ak, av);
+          vload<float, W>(pk, pv);
+          vload<float, W>(xk, xv);
+          vload<float, W>(rk, rv);
+          item_M<float, W>(ri, smi, n, w);
+#pragma unroll
+          for (int e = 0; e < W; e++) {
+            av[e] = fmaf(beta, av[e], w[e]);
+            pv[e] = fmaf(beta, pv[e], rv[e]);
+            xv[e] = fmaf(alpha, pv[e], xv[e]);
+            rv[e] = fmaf(-alpha, av[e], rv[e]);
+          }
+          vstore<float, W>(ak, av);
+          vstore<float, W>(pk, pv);
+          vstore<float, W>(xk, xv);
+          vstore<float, W>(rk, rv);
+        }
+      });
+      ok = team_barrier(sh, team);
+      if (!ok) break;
     }
   }
   // ---------------------------------------------------------------- results

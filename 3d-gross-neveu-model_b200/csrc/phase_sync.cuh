@@ -162,4 +162,34 @@ __device__ __forceinline__ bool end_phase(double (&acc)[kSyncQ], SyncShared &sh,
   return ok;
 }
 
+
+// A team barrier without sums: on return the team's writes before the call
+// are visible to this block.  About 1.5 us on B200 for a grid of 64 - 148
+// blocks of 1024 threads, against 3.2 - 3.7 us for an end_phase with sums
+// (the block and team reductions and the read of the partials are what it
+// saves); 0.28 us for a one-block team.  Counts as one phase of the team.
+__device__ __forceinline__ bool team_barrier(SyncShared &sh, Team &t) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    if (t.nblocks > 1) {
+      red_release_add64(&t.bar->arrived, 1ull);
+      const unsigned long long target = (t.nph + 1ull) * t.nblocks;
+      unsigned spins = 0;
+      while (ld_relaxed64(&t.bar->arrived) < target) {
+        if (++spins > (1u << 22)) {  // ~ a second: give up, report, return
+          atomicExch(t.err, 1);
+          ok = 0;
+          break;
+        }
+      }
+      fence_acquire();
+    }
+    sh.ok = ok;
+  }
+  t.nph++;
+  __syncthreads();
+  return sh.ok != 0;
+}
+
 }  // namespace gn

@@ -125,10 +125,10 @@ class Server {
 static size_t round256(size_t b) { return (b + 255) & ~size_t(255); }
 
 // A running request's arrays: P, F, sigma_save (1 plane each), chi, phi, X,
-// Y, t64 (2 planes), sm32 (1 plane of float), the mixed solver's r^, p^, t^,
-// x^ (2 planes of float each), the FP64 solver's r, p, p' (2 planes each).
+// Y, t64 (2 planes), sm32 (1 plane of float), the mixed solver's r^, p^, u^,
+// a^, x^ (2 planes of float each), the FP64 solver's r, p, p' (2 planes each).
 size_t Server::work_bytes(size_t V) {
-  return 3 * round256(V * 8) + 5 * round256(2 * V * 8) + round256(V * 4) + 4 * round256(2 * V * 4) +
+  return 3 * round256(V * 8) + 5 * round256(2 * V * 8) + round256(V * 4) + 5 * round256(2 * V * 4) +
          3 * round256(2 * V * 8);
 }
 
@@ -356,7 +356,8 @@ EnsChain Server::chain_entry(const Req &r) {
   e.sm32 = fv(1);
   e.rh = fv(2);
   e.ph = fv(2);
-  e.th = fv(2);
+  e.uh = fv(2);
+  e.ah = fv(2);
   e.xh = fv(2);
   e.r64 = dv(2);
   e.pa64 = dv(2);

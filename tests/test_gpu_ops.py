@@ -170,3 +170,25 @@ def test_mixed_precision_solver(lattices, port):
         assert np.linalg.norm(r) < 1e-10 * np.linalg.norm(b[k]) * 1.01
         assert im[k]["reliable_updates"] >= 1
         assert rel(xm[k], x64[k]) < 1e-8
+
+
+@pytest.mark.parametrize("L", [96, 128])
+def test_mixed_precision_schemes(lattices, port, L):
+    """Both inner iterations of the mixed solver: the split (Chronopoulos-Gear)
+    one at L = 96, whose FP32 vectors fit the L2, and the two-phase one at
+    L = 128.  Each reaches the FP64 stopping rule on the true residual within
+    a few per cent of the FP64 solver's iteration count."""
+    import gn_b200 as G
+    rng = np.random.default_rng(L)
+    V = L ** 3
+    lat = lattices(L)
+    sm = lat.sigma_mass(rng.normal(0, 0.77, V))
+    b = np.stack([rng.normal(size=V) for _ in range(2)])
+    x64, i64, st = lat.cg(sm, b, None, 1e-10, variant=1, relative=True)
+    xm, im, st2 = lat.cg(sm, b, None, 1e-10, variant=1, relative=True, precision=G.GN_PREC_MIXED)
+    assert st == 0 and st2 == 0
+    for k in range(2):
+        r = b[k] - port.dirac(L, sm, port.dirac(L, sm, xm[k], 1), 0)
+        assert np.linalg.norm(r) < 1e-10 * np.linalg.norm(b[k]) * 1.01
+        assert im[k]["iterations"] <= 1.1 * i64[k]["iterations"] + 20
+        assert rel(xm[k], x64[k]) < 1e-7
