@@ -33,6 +33,7 @@ UNITS = {
     "exact.cu": ["--fmad=false"],
     "ensemble.cu": ["--fmad=false"],
     "serve.cu": ["--fmad=false"],
+    "checkpoint.cu": [],
 }
 CORE_LIB = LIB / "libgn_b200.so"
 DROPIN_LIB = LIB / "libgn_dropin.so"

@@ -8,6 +8,7 @@
 #include <string>
 
 #include "../../include/gn_b200.h"
+#include "checkpoint.h"
 #include "engine.h"
 #include "errors.h"
 
@@ -266,6 +267,63 @@ int gn_condensate(gn_context *ctx, const double *sigmamass, double tol, double *
     if (cg_iterations) *cg_iterations = it;
     if (cg_calls) *cg_calls = calls;
     return st;
+  });
+}
+
+int gn_condensate_sigma(gn_context *ctx, const double *sigma, double *out) {
+  if (!out) return fail(GN_ERR_ARG, "null pointer");
+  return guarded(ctx, [&](gn::Engine &E) {
+    const double *d = E.sigma();
+    if (sigma) {
+      up(E, ctx->io, sigma, size_t(E.V()));
+      d = ctx->io;
+    }
+    E.sigma_observables(d, out);
+    return GN_OK;
+  });
+}
+
+int gn_condensate_sigma_device(gn_context *ctx, const double *sigma, double *out) {
+  if (!sigma || !out) return fail(GN_ERR_ARG, "null pointer");
+  return guarded(ctx, [&](gn::Engine &E) {
+    E.sigma_observables(sigma, out);
+    return GN_OK;
+  });
+}
+
+int gn_checkpoint_save(gn_context *ctx, const char *path, const char *path_copy, const gn_hmc_counters *c) {
+  if (!path || !c) return fail(GN_ERR_ARG, "null pointer");
+  return guarded(ctx, [&](gn::Engine &E) -> int {
+    const size_t V = size_t(E.V());
+    std::vector<double> sigma(V), sm(V);
+    down(E, sigma.data(), E.sigma(), V);
+    down(E, sm.data(), E.sm(), V);
+    sync(E);
+    const int st = gn::write_lattice_file(path, path_copy, E.L(), sigma.data(), sm.data(), nullptr, *c);
+    return st == GN_OK ? GN_OK : fail(st, "cannot write the lattice file");
+  });
+}
+
+int gn_checkpoint_load(gn_context *ctx, const char *path, const char *path_copy, gn_hmc_counters *c) {
+  if (!path) return fail(GN_ERR_ARG, "null pointer");
+  return guarded(ctx, [&](gn::Engine &E) -> int {
+    const size_t V = size_t(E.V());
+    double *d_sigma = ctx->io, *d_sm = ctx->io + V;
+    auto sm_of = [&](const double *sigma, double *sm) {  // on staging buffers: the resident field stays
+      up(E, d_sigma, sigma, V);
+      E.sigma_mass(d_sigma, nullptr, 0.0, nullptr, d_sm);
+      down(E, sm, d_sm, V);
+      sync(E);
+    };
+    auto accept = [&](const double *sigma) {
+      up(E, E.sigma(), sigma, V);
+      E.sigma_mass(E.sigma(), nullptr, 0.0, nullptr, E.sm());
+      sync(E);
+    };
+    const int st = gn::load_lattice(path, path_copy, E.L(), c, sm_of, accept);
+    if (st == GN_ERR_NOT_FOUND) return fail(st, "no lattice file (a fresh start)");
+    if (st != GN_OK) return fail(st, "no lattice file passed its check");
+    return GN_OK;
   });
 }
 

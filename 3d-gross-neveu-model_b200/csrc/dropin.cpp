@@ -348,4 +348,12 @@ void ComputeCondensateDirac(const Lattice *lat, double *tr1, double *tr1_abs, do
   for (int k = 0; k < 11; k++) *dst[k] = out[k];
 }
 
+void CondensateSigmaPi(const Lattice *lat, const Info *, double *condensate_sigma, double *condensate_sigma_abs,
+                       double *mu2, double *mu4, double *chi, double *chip, double *chip_pbc1, double *chip_pbc2) {
+  double out[8];
+  if (gn_condensate_sigma(ctx(), lat->sigma, out) != GN_OK) fatal("gn_condensate_sigma");
+  double *dst[8] = {condensate_sigma, condensate_sigma_abs, mu2, mu4, chi, chip, chip_pbc1, chip_pbc2};
+  for (int k = 0; k < 8; k++) *dst[k] = out[k];
+}
+
 }  // extern "C"

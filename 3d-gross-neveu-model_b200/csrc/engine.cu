@@ -174,6 +174,21 @@ void Engine::cond_dots(const double *v, const double *D, double out[3]) {
   for (int q = 0; q < 3; q++) out[q] = sum_partials(h_partials_, nb, q);
 }
 
+void Engine::sigma_observables(const double *sigma, double out[8]) {
+  const int nb = op_blocks(V_, num_sms_);
+  sigma_obs_kernel<<<nb, kOpThreads, 0, stream_>>>(g_, sigma, partials_);
+  check(cudaGetLastError(), "sigma_obs_kernel");
+  launches++;
+  check(cudaMemcpyAsync(h_partials_, partials_, sizeof(double) * 2 * kSigmaObsSums * nb, cudaMemcpyDeviceToHost,
+                        stream_),
+        "copy");
+  check(cudaStreamSynchronize(stream_), "sigma observables sync");
+  double sums[kSigmaObsSums], o[kSigmaObs];
+  for (int q = 0; q < kSigmaObsSums; q++) sums[q] = sum_partials(h_partials_, nb, q);
+  sigma_obs_finish(sums, double(V_), o);
+  for (int q = 0; q < kSigmaObs; q++) out[q] = o[q];
+}
+
 void Engine::cond_fill(int mode, const signed char *signs, const double *table, const double *sm, double *v) {
   cond_fill_kernel<<<op_blocks(V_, num_sms_), kOpThreads, 0, stream_>>>(g_, mode, signs, table, sm, v);
   check(cudaGetLastError(), "cond_fill_kernel");

@@ -50,6 +50,9 @@ class Engine {
   void energy_terms(const double *P, const double *phi, const double *X, const double *sigma, double out[3]);
   // sum Re(conj v D)/V, sum Re(conj v D), sum Im(conj v D); synchronises.
   void cond_dots(const double *v, const double *D, double out[3]);
+  // CondensateSigmaPi of a device sigma (fermion order): the 8 outputs in the
+  // reference's argument order
+  void sigma_observables(const double *sigma, double out[8]);
   void cond_fill(int mode, const signed char *signs, const double *table, const double *sm, double *v);
 
   // CG on M M^T for nrhs right-hand sides of ncomp planes each (b[k], x[k] are

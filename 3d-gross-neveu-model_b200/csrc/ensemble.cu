@@ -22,6 +22,7 @@
 #include "../../include/gn_b200.h"
 #define GN_DEFINE_ENSEMBLE_KERNEL
 #include "ensemble_kernel.cuh"
+#include "checkpoint.h"
 #include "errors.h"
 #include "launch.h"
 #include "schedule.h"
@@ -46,6 +47,9 @@ class Ensemble {
   void tune(const gn_ens_params &p, int *gs, long long *big_min);
   void run(const gn_ens_params &p, int ntraj, bool graph);
   void stats(gn_chain_stats *out, bool reset);
+  void observables(double *out);
+  int checkpoint_save(int c, const char *path, const char *copy, const gn_hmc_counters &cnt);
+  int checkpoint_load(int c, const char *path, const char *copy, gn_hmc_counters *cnt);
   void info(int *gs, long long *big_min, int *graph_used, int *launches);
 
  private:
@@ -472,12 +476,47 @@ void Ensemble::stats(gn_chain_stats *out, bool reset) {
     if (reset) {
       h[c].n = h[c].nacc = h[c].iters = h[c].reliable = h[c].fails = 0;
       h[c].sum_dH = h[c].sum_exp_mdH = h[c].sum_sigma2 = 0.0;
+      for (int q = 0; q < kSigmaObs; q++) h[c].sum_obs[q] = 0.0;
     }
   }
   if (reset) {
     check(cudaMemcpyAsync(d_states_, h.data(), n_ * sizeof(EnsState), cudaMemcpyHostToDevice, stream_), "copy");
     check(cudaStreamSynchronize(stream_), "states");
   }
+}
+
+void Ensemble::observables(double *out) {
+  std::vector<EnsState> h(n_);
+  check(cudaMemcpyAsync(h.data(), d_states_, n_ * sizeof(EnsState), cudaMemcpyDeviceToHost, stream_), "copy states");
+  check(cudaStreamSynchronize(stream_), "states");
+  for (int c = 0; c < n_; c++)
+    for (int q = 0; q < kSigmaObs; q++)
+      out[size_t(c) * kSigmaObs + q] = h[c].n > 0 ? h[c].sum_obs[q] / double(h[c].n) : 0.0;
+}
+
+int Ensemble::checkpoint_save(int c, const char *path, const char *copy, const gn_hmc_counters &cnt) {
+  if (c < 0 || c >= n_) throw GnError(GN_ERR_ARG, "bad chain");
+  const size_t V = size_t(chains_[c].g.V);
+  std::vector<double> sigma(V), sm(V);
+  store_sigma(c, sigma.data(), sm.data());
+  return write_lattice_file(path, copy, chains_[c].g.L, sigma.data(), sm.data(), nullptr, cnt);
+}
+
+int Ensemble::checkpoint_load(int c, const char *path, const char *copy, gn_hmc_counters *cnt) {
+  if (c < 0 || c >= n_) throw GnError(GN_ERR_ARG, "bad chain");
+  const size_t V = size_t(chains_[c].g.V);
+  std::vector<double> old(V);
+  store_sigma(c, old.data(), nullptr);
+  bool replaced = false;
+  auto sm_of = [&](const double *sigma, double *sm) {  // the chain's own arrays; restored on failure
+    load_sigma(c, sigma);
+    store_sigma(c, nullptr, sm);
+    replaced = true;
+  };
+  auto accept = [&](const double *sigma) { load_sigma(c, sigma); };
+  const int st = load_lattice(path, copy, chains_[c].g.L, cnt, sm_of, accept);
+  if (st != GN_OK && replaced) load_sigma(c, old.data());
+  return st;
 }
 
 void Ensemble::info(int *gs, long long *big_min, int *graph_used, int *launches) {
@@ -572,6 +611,34 @@ int gn_ensemble_run(gn_ensemble *e, const gn_ens_params *p, int ntraj, int use_g
 int gn_ensemble_stats(gn_ensemble *e, gn_chain_stats *out, int reset) {
   return ens_guarded(e, [&](gn::Ensemble &E) {
     E.stats(out, reset != 0);
+    return GN_OK;
+  });
+}
+
+int gn_ensemble_observables(gn_ensemble *e, double *out) {
+  if (out == nullptr) return gn::set_last_error(GN_ERR_ARG, "null pointer");
+  return ens_guarded(e, [&](gn::Ensemble &E) {
+    E.observables(out);
+    return GN_OK;
+  });
+}
+
+int gn_ensemble_checkpoint_save(gn_ensemble *e, int chain, const char *path, const char *path_copy,
+                                const gn_hmc_counters *c) {
+  if (path == nullptr || c == nullptr) return gn::set_last_error(GN_ERR_ARG, "null pointer");
+  return ens_guarded(e, [&](gn::Ensemble &E) -> int {
+    const int st = E.checkpoint_save(chain, path, path_copy, *c);
+    return st == GN_OK ? GN_OK : gn::set_last_error(st, "cannot write the lattice file");
+  });
+}
+
+int gn_ensemble_checkpoint_load(gn_ensemble *e, int chain, const char *path, const char *path_copy,
+                                gn_hmc_counters *c) {
+  if (path == nullptr) return gn::set_last_error(GN_ERR_ARG, "null pointer");
+  return ens_guarded(e, [&](gn::Ensemble &E) -> int {
+    const int st = E.checkpoint_load(chain, path, path_copy, c);
+    if (st == GN_ERR_NOT_FOUND) return gn::set_last_error(st, "no lattice file (a fresh start)");
+    if (st != GN_OK) return gn::set_last_error(st, "no lattice file passed its check");
     return GN_OK;
   });
 }

@@ -74,6 +74,7 @@ struct EnsState {
   // accumulated since the last reset
   long long n, nacc, iters, reliable, fails;
   double sum_dH, sum_exp_mdH, sum_sigma2, last_dH;
+  double sum_obs[kSigmaObs];  // CondensateSigmaPi outputs after each trajectory
   int last_acc;
   // the current request of a served chain
   unsigned long long serial;  // Philox counter of the request's draws
@@ -297,10 +298,21 @@ static __device__ __noinline__ bool ens_run_chain(const EnsLaunch &L, int c, Tea
         cur ^= 1;
       }
       ok = end_phase<0>(acc, sh, t);
+      // sum sigma^2 and the CondensateSigmaPi sums of the chain's sigma
       const double *fin = ch.sigma[cur];
-      for (uint32_t i = t.tid; i < V; i += t.nthreads) acc[0] += fin[i] * fin[i];
-      ok = end_phase<1>(acc, sh, t) && ok;
+      for (uint32_t i = t.tid; i < V; i += t.nthreads) {
+        double v[kSigmaObsSums];
+        sigma_obs_site(g, i, fin, v);
+        acc[0] += fin[i] * fin[i];
+#pragma unroll
+        for (int q = 0; q < kSigmaObsSums; q++) acc[1 + q] += v[q];
+      }
+      ok = end_phase<1 + kSigmaObsSums>(acc, sh, t) && ok;
       if (leader) {
+        double sums[kSigmaObsSums], o[kSigmaObs];
+        for (int q = 0; q < kSigmaObsSums; q++) sums[q] = sh.val[1 + q];
+        sigma_obs_finish(sums, double(V), o);
+        for (int q = 0; q < kSigmaObs; q++) st->sum_obs[q] += o[q];
         st->n++;
         st->nacc += accept;
         st->fails += failed;

@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(kOpThreads) force_kernel(Geom g, const T *__re
     force_site<T>(g, i, X, Y, sigma, gcoef, F, P, pcoef);
 }
 
-// Compensated block sums of up to 4 quantities: per thread a Neumaier sum,
+// Compensated block sums of up to 7 quantities: per thread a Neumaier sum,
 // per block a tree of (hi, lo) pairs.  Writes part[q*2*nb + 2*block + {0,1}].
 template <int NQ>
 __device__ __forceinline__ void publish_compensated(double (&hi)[NQ], double (&lo)[NQ], double *part) {
@@ -235,6 +235,61 @@ static __global__ void __launch_bounds__(kOpThreads) cond_fill_kernel(Geom g, in
       v[V + i] = v[V + i] * sm[i];
     }
   }
+}
+
+
+// ------------------------------------------------------------------ sigma observables
+// CondensateSigmaPi (observables.c:323-369, the Z2 model): with t = sigma(x) / V,
+//   s0 = sum_x t,   s1+2d + i s2+2d = sum_x exp(i P_MIN x_d) t   (d = 0, 1, 2),
+// P_MIN = 2 PI / L formed as macro.h:178 forms it, the angle as the
+// reference's product P_MIN * x_d.  From the sums (sigma_obs_finish):
+//   condensate = s0, |condensate|, mu2 = s0^2, mu4 = mu2^2, chi = V mu2,
+//   chip = V |box_2|^2, chip_pbc1 = V |box_0|^2, chip_pbc2 = V |box_1|^2.
+constexpr double kPi = 3.14159265358979323846;
+constexpr int kSigmaObsSums = 7;
+constexpr int kSigmaObs = 8;
+
+__device__ __forceinline__ void sigma_obs_site(const Geom &g, uint32_t i, const double *__restrict__ sigma,
+                                               double (&v)[kSigmaObsSums]) {
+  uint32_t x[3], par, row, k;
+  site_coords(g, i, x[0], x[1], x[2], par, row, k);
+  const double t = sigma[i] / double(g.V);
+  const double pmin = (2 * kPi) / double(g.L);
+  v[0] = t;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    double sn, cs;
+    sincos(pmin * double(x[d]), &sn, &cs);
+    v[1 + 2 * d] = cs * t;
+    v[2 + 2 * d] = sn * t;
+  }
+}
+
+__host__ __device__ inline void sigma_obs_finish(const double (&s)[kSigmaObsSums], double V, double (&out)[kSigmaObs]) {
+  const double c = s[0];
+  out[0] = c;
+  out[1] = c < 0 ? -c : c;
+  out[2] = c * c;
+  out[3] = out[2] * out[2];
+  out[4] = V * out[2];
+  out[5] = V * (s[5] * s[5] + s[6] * s[6]);
+  out[6] = V * (s[1] * s[1] + s[2] * s[2]);
+  out[7] = V * (s[3] * s[3] + s[4] * s[4]);
+}
+
+static __global__ void __launch_bounds__(kOpThreads) sigma_obs_kernel(Geom g, const double *__restrict__ sigma,
+                                                                      double *part) {
+  double hi[kSigmaObsSums], lo[kSigmaObsSums];
+#pragma unroll
+  for (int q = 0; q < kSigmaObsSums; q++) hi[q] = lo[q] = 0.0;
+  const uint32_t V = uint32_t(g.V);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x) {
+    double v[kSigmaObsSums];
+    sigma_obs_site(g, i, sigma, v);
+#pragma unroll
+    for (int q = 0; q < kSigmaObsSums; q++) neumaier(hi[q], lo[q], v[q]);
+  }
+  publish_compensated<kSigmaObsSums>(hi, lo, part);
 }
 
 }  // namespace gn

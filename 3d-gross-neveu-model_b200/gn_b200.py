@@ -25,8 +25,13 @@ GN_OP_M, GN_OP_MT, GN_OP_SUB_M = 0, 1, 2
 GN_PREC_FP64, GN_PREC_MIXED, GN_PREC_FP64_EXACT = 0, 1, 2
 GN_LFMN2VF, GN_LF2, GN_LFMN2 = 0, 1, 2
 GN_F_P, GN_F_F, GN_F_CHI, GN_F_PHI, GN_F_X, GN_F_Y, GN_F_SIGMA, GN_F_SM = range(8)
+GN_ERR_IO, GN_ERR_NOT_FOUND, GN_ERR_FORMAT = -6, -7, -8
 STATUS_NAMES = {0: "GN_OK", 1: "GN_NOT_CONVERGED", -1: "GN_ERR_ARG", -2: "GN_ERR_CUDA", -3: "GN_ERR_TIMEOUT",
-                -4: "GN_ERR_ABORTED", -5: "GN_ERR_NO_DEVICE"}
+                -4: "GN_ERR_ABORTED", -5: "GN_ERR_NO_DEVICE", -6: "GN_ERR_IO", -7: "GN_ERR_NOT_FOUND",
+                -8: "GN_ERR_FORMAT"}
+# CondensateSigmaPi's outputs (observables.c:323), in its argument order
+SIGMA_OBSERVABLES = ("condensate_sigma", "condensate_sigma_abs", "mu2", "mu4", "chi", "chip", "chip_pbc1",
+                     "chip_pbc2")
 DRAW_FN = C.CFUNCTYPE(C.c_double)
 
 
@@ -84,6 +89,21 @@ class ReqInfo(C.Structure):
 
 
 GN_REQ_TRAJECTORY, GN_REQ_SOLVE, GN_REQ_CONDENSATE = 0, 1, 2
+
+
+class HmcCounters(C.Structure):
+    """The HMC bookkeeping of the reference's lattice file (gn_hmc_counters)."""
+    _fields_ = [("epsilon_link", C.c_double), ("epsilon_pi", C.c_double), ("story_link", C.c_int),
+                ("story_sigma", C.c_int), ("story_pi", C.c_int), ("accepted_link", C.c_int), ("done_link", C.c_int),
+                ("accepted_sigma", C.c_int), ("done_sigma", C.c_int), ("accepted_pi", C.c_int),
+                ("done_pi", C.c_int), ("measure", C.c_int)]
+
+    @classmethod
+    def from_dict(cls, d):
+        return cls(**{k: (float if t is C.c_double else int)(d.get(k, 0)) for k, t in cls._fields_})
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 _dp = C.POINTER(C.c_double)
 _lib = None
@@ -158,6 +178,19 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
         "gn_server_load": ([v, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_longlong)], C.c_int),
         "gn_ensemble_info": ([v, C.POINTER(C.c_int), C.POINTER(C.c_longlong), C.POINTER(C.c_int),
                               C.POINTER(C.c_int)], C.c_int),
+        "gn_condensate_sigma": ([v, _dp, _dp], C.c_int),
+        "gn_condensate_sigma_device": ([v, C.c_void_p, _dp], C.c_int),
+        "gn_checkpoint_write_file": ([C.c_char_p, C.c_char_p, C.c_int, _dp, _dp, _dp, C.POINTER(HmcCounters)],
+                                     C.c_int),
+        "gn_checkpoint_read_file": ([C.c_char_p, C.c_int, _dp, _dp, C.POINTER(HmcCounters), _dp], C.c_int),
+        "gn_checkpoint_check_value": ([C.c_int, _dp, _dp], C.c_double),
+        "gn_checkpoint_save": ([v, C.c_char_p, C.c_char_p, C.POINTER(HmcCounters)], C.c_int),
+        "gn_checkpoint_load": ([v, C.c_char_p, C.c_char_p, C.POINTER(HmcCounters)], C.c_int),
+        "gn_ensemble_observables": ([v, _dp], C.c_int),
+        "gn_ensemble_checkpoint_save": ([v, C.c_int, C.c_char_p, C.c_char_p, C.POINTER(HmcCounters)], C.c_int),
+        "gn_ensemble_checkpoint_load": ([v, C.c_int, C.c_char_p, C.c_char_p, C.POINTER(HmcCounters)], C.c_int),
+        "gn_format_measure_line": ([C.c_char_p, C.c_size_t, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                    C.c_double, C.c_double, _dp, _dp], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -169,6 +202,58 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
 
 def _p(a):
     return a.ctypes.data_as(_dp)
+
+
+def _path(p):
+    return None if p is None else str(p).encode()
+
+
+def _raise(st):
+    raise GnError(st, load_library().gn_last_error().decode())
+
+
+# ---- the reference's lattice file (host functions, no device needed)
+def checkpoint_write_file(path, path_copy, L, sigma, sigmamass, counters, links=None):
+    """WriteBinaryLattice's file (simulation.c:129-185): links None = unit links."""
+    lib = load_library()
+    s = np.ascontiguousarray(sigma, np.float64)
+    sm = np.ascontiguousarray(sigmamass, np.float64)
+    lk = None if links is None else _p(np.ascontiguousarray(links, np.float64))
+    c = counters if isinstance(counters, HmcCounters) else HmcCounters.from_dict(counters)
+    st = lib.gn_checkpoint_write_file(_path(path), _path(path_copy), int(L), _p(s), _p(sm), lk, C.byref(c))
+    if st != GN_OK:
+        _raise(st)
+
+
+def checkpoint_read_file(path, L):
+    """One lattice file: (sigma, links (V, 3, 2), counters dict, stored check value)."""
+    lib = load_library()
+    V = int(L) ** 3
+    s, lk, chk = np.empty(V), np.empty(6 * V), C.c_double()
+    c = HmcCounters()
+    st = lib.gn_checkpoint_read_file(_path(path), int(L), _p(s), _p(lk), C.byref(c), C.byref(chk))
+    if st != GN_OK:
+        _raise(st)
+    return s, lk.reshape(V, 3, 2), c.as_dict(), chk.value
+
+
+def checkpoint_check_value(L, sigmamass, links=None):
+    """TestWriteReadLattice (simulation.c:101-120) of (sigmamass, links)."""
+    sm = np.ascontiguousarray(sigmamass, np.float64)
+    lk = None if links is None else _p(np.ascontiguousarray(links, np.float64))
+    return load_library().gn_checkpoint_check_value(int(L), _p(sm), lk)
+
+
+def format_measure_line(measure, L, beta, beta_scalar, mass, avg_iterations, avg_distance, cond_dirac=None,
+                        cond_sigma=None):
+    """TakeMeasures' observables line (observables.c:266-292)."""
+    lib = load_library()
+    cd = None if cond_dirac is None else _p(np.ascontiguousarray(cond_dirac, np.float64))
+    cs = None if cond_sigma is None else _p(np.ascontiguousarray(cond_sigma, np.float64))
+    n = lib.gn_format_measure_line(None, 0, measure, L, beta, beta_scalar, mass, avg_iterations, avg_distance, cd, cs)
+    buf = C.create_string_buffer(n + 1)
+    lib.gn_format_measure_line(buf, n + 1, measure, L, beta, beta_scalar, mass, avg_iterations, avg_distance, cd, cs)
+    return buf.value.decode()
 
 
 def _planes(a) -> tuple[np.ndarray, int]:
@@ -392,6 +477,25 @@ class Lattice:
     def flush_l2(self):
         self._check(self.lib.gn_flush_l2(self.ctx))
 
+    # ---- observables and checkpoints
+    def condensate_sigma(self, sigma=None):
+        """CondensateSigmaPi of sigma (host array) or of the resident sigma (None)."""
+        out = np.empty(8)
+        s = None if sigma is None else _p(np.ascontiguousarray(sigma, np.float64))
+        self._check(self.lib.gn_condensate_sigma(self.ctx, s, _p(out)))
+        return out
+
+    def checkpoint_save(self, path, path_copy, counters):
+        c = counters if isinstance(counters, HmcCounters) else HmcCounters.from_dict(counters)
+        self._check(self.lib.gn_checkpoint_save(self.ctx, _path(path), _path(path_copy), C.byref(c)))
+
+    def checkpoint_load(self, path, path_copy=None):
+        """(status, counters): GN_OK, GN_ERR_NOT_FOUND (a fresh start) or GN_ERR_FORMAT."""
+        c = HmcCounters()
+        st = self._check(self.lib.gn_checkpoint_load(self.ctx, _path(path), _path(path_copy), C.byref(c)),
+                         allow=(GN_OK, GN_ERR_NOT_FOUND, GN_ERR_FORMAT))
+        return st, c.as_dict()
+
 
 class Ensemble:
     """Many independent sigma-HMC chains (gn_ensemble_* of gn_b200.h)."""
@@ -457,6 +561,24 @@ class Ensemble:
     def stream(self):
         """The cudaStream_t (as an int) the ensemble runs on."""
         return self.lib.gn_ensemble_stream(self.ens)
+
+    def observables(self):
+        """(nchains, 8): per-chain means of CondensateSigmaPi's outputs over the
+        trajectories since the last stats reset."""
+        out = np.empty(8 * self.n)
+        self._check(self.lib.gn_ensemble_observables(self.ens, _p(out)))
+        return out.reshape(self.n, 8)
+
+    def checkpoint_save(self, c, path, path_copy, counters):
+        cnt = counters if isinstance(counters, HmcCounters) else HmcCounters.from_dict(counters)
+        self._check(self.lib.gn_ensemble_checkpoint_save(self.ens, c, _path(path), _path(path_copy), C.byref(cnt)))
+
+    def checkpoint_load(self, c, path, path_copy=None):
+        cnt = HmcCounters()
+        st = self._check(self.lib.gn_ensemble_checkpoint_load(self.ens, c, _path(path), _path(path_copy),
+                                                              C.byref(cnt)),
+                         allow=(GN_OK, GN_ERR_NOT_FOUND, GN_ERR_FORMAT))
+        return st, cnt.as_dict()
 
     def info(self):
         gs, vmin, g, nl = C.c_int(), C.c_longlong(), C.c_int(), C.c_int()

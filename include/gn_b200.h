@@ -45,7 +45,10 @@ enum gn_status {
   GN_ERR_CUDA = -2,     /* a CUDA call failed */
   GN_ERR_TIMEOUT = -3,  /* a device-side wait ran out (bounded barrier) */
   GN_ERR_ABORTED = -4,  /* gn_request_abort() stopped a solve */
-  GN_ERR_NO_DEVICE = -5 /* no usable sm_100 device */
+  GN_ERR_NO_DEVICE = -5, /* no usable sm_100 device */
+  GN_ERR_IO = -6,        /* a file could not be written */
+  GN_ERR_NOT_FOUND = -7, /* a file could not be opened for reading */
+  GN_ERR_FORMAT = -8     /* a file is short or its check value differs */
 };
 
 enum gn_op { GN_OP_M = 0, GN_OP_MT = 1, GN_OP_SUB_M = 2 };
@@ -159,6 +162,64 @@ GN_API int gn_evolve_momenta(gn_context *ctx, double *P, const double *F, double
  * amounts the reference adds to kit->iterations / kit->CG_call. */
 GN_API int gn_condensate(gn_context *ctx, const double *sigmamass, double tol, double *target, double *D,
                   double (*uniform)(void), double *out, double *cg_iterations, long long *cg_calls, int precision);
+
+/* CondensateSigmaPi (observables.c:323-369, the Z2 model) of a sigma field:
+ * sigma (V doubles, fermion order) on the host, or NULL for the resident
+ * sigma (no transfer of the field).  out[8] = condensate_sigma,
+ * |condensate_sigma|, mu2, mu4, chi, chip, chip_pbc1, chip_pbc2, the
+ * reference's argument order.  The sums run on the device. */
+GN_API int gn_condensate_sigma(gn_context *ctx, const double *sigma, double *out);
+/* The same for a device sigma (V doubles). */
+GN_API int gn_condensate_sigma_device(gn_context *ctx, const double *sigma, double *out);
+
+/* ---- checkpoints: the reference's lattice file ------------------------- */
+
+/* The HMC bookkeeping the file carries (simulation.c:162-178, struct Info
+ * fields, info.h).  The lengths of the HMC trajectories are not in the file,
+ * as in the reference. */
+typedef struct gn_hmc_counters {
+  double epsilon_link, epsilon_pi;
+  int story_link, story_sigma, story_pi;
+  int accepted_link, done_link;
+  int accepted_sigma, done_sigma;
+  int accepted_pi, done_pi;
+  int measure;
+} gn_hmc_counters;
+
+/* The file of WriteBinaryLattice / ReadBinaryLattice (simulation.c:129-401)
+ * for the sigma model (SIGMA_INTERACTION without PI_INTERACTION), DIM = 3:
+ *   V x 3 complex links (lexicographic site, then direction), V sigma values
+ *   (fermion order), the check value sum_x sum_d (carg(link) + sigmamass[x]/3)
+ *   accumulated in that order, then the counters: epsilon_link, an 8-byte
+ *   slot, accepted_link, done_link, a slot, accepted_sigma, done_sigma,
+ *   epsilon_pi, a slot, accepted_pi, done_pi, measure.  The reference writes
+ *   the int story fields with sizeof(double), so the three slots hold the
+ *   ints {story_link, story_sigma}, {story_sigma, story_pi}, {story_pi, the
+ *   struct's padding (written 0 here)}.
+ * Host functions, no device needed.  links (6V doubles: re, im per link) may
+ * be NULL: unit links, the reference's START_LINK_IDENTITY.
+ *
+ * write: as WriteBinaryLattice, an existing path_copy is removed and path is
+ * renamed to path_copy before path is written (path_copy may be NULL: no
+ * rotation).  Returns GN_OK or GN_ERR_IO. */
+GN_API int gn_checkpoint_write_file(const char *path, const char *path_copy, int L, const double *sigma,
+                                    const double *sigmamass, const double *links, const gn_hmc_counters *c);
+/* read one file: sigma (V), links (6V, may be NULL), counters, and the stored
+ * check value.  GN_OK, GN_ERR_NOT_FOUND (cannot open) or GN_ERR_FORMAT (short). */
+GN_API int gn_checkpoint_read_file(const char *path, int L, double *sigma, double *links, gn_hmc_counters *c,
+                                   double *check);
+/* The check value of (sigmamass, links) in the reference's order (links NULL: unit). */
+GN_API double gn_checkpoint_check_value(int L, const double *sigmamass, const double *links);
+
+/* A context's resident sigma: save writes it (sigmamass computed on the
+ * device, links unit).  load follows ReadBinaryLattice with try_copy: path,
+ * else path_copy when path cannot be opened or fails (short, or the check
+ * value recomputed from the loaded sigma differs bit for bit); on success
+ * sigma becomes the resident field and c receives the counters.  Returns
+ * GN_OK, GN_ERR_NOT_FOUND (neither file exists: a fresh start) or
+ * GN_ERR_FORMAT (every candidate failed). */
+GN_API int gn_checkpoint_save(gn_context *ctx, const char *path, const char *path_copy, const gn_hmc_counters *c);
+GN_API int gn_checkpoint_load(gn_context *ctx, const char *path, const char *path_copy, gn_hmc_counters *c);
 
 /* ---- resident sigma-HMC state ------------------------------------------ */
 
@@ -302,6 +363,29 @@ GN_API int gn_ensemble_run(gn_ensemble *ens, const gn_ens_params *p, int ntraj, 
 /* Per-chain statistics into out[nchains] (may be NULL); reset = 1 zeroes the
  * accumulators afterwards. */
 GN_API int gn_ensemble_stats(gn_ensemble *ens, gn_chain_stats *out, int reset);
+/* Per-chain means of the CondensateSigmaPi outputs (gn_condensate_sigma's
+ * order) over the trajectories that gn_chain_stats.trajectories counts:
+ * out[8 * nchains].  The kernel takes the sums on the device after every
+ * trajectory, so no sigma leaves the GPU (TakeMeasures' averaging,
+ * observables.c:259-292, with IMEAS = the trajectories since the last reset);
+ * gn_ensemble_stats(..., reset = 1) zeroes them with the other accumulators. */
+GN_API int gn_ensemble_observables(gn_ensemble *ens, double *out);
+/* Checkpoint of chain c in the reference's lattice file (gn_checkpoint_save /
+ * gn_checkpoint_load; load puts sigma in place of the chain's). */
+GN_API int gn_ensemble_checkpoint_save(gn_ensemble *ens, int chain, const char *path, const char *path_copy,
+                                       const gn_hmc_counters *c);
+GN_API int gn_ensemble_checkpoint_load(gn_ensemble *ens, int chain, const char *path, const char *path_copy,
+                                       gn_hmc_counters *c);
+
+/* The observables line TakeMeasures appends (observables.c:266-292) with
+ * OBS_CONDENSATE and OBS_CONDENSATE_SIGMA defined: measure, L, beta,
+ * beta_scalar, mass, average CG iterations, average sigma distance, then
+ * cond_dirac[11] (gn_condensate's out; NULL leaves the group out) and
+ * cond_sigma[8] (NULL leaves it out), tab-separated, every double "%.16f",
+ * and a newline.  Returns the length snprintf reports, or GN_ERR_ARG. */
+GN_API int gn_format_measure_line(char *buf, size_t size, int measure, int L, double beta, double beta_scalar,
+                                  double mass, double avg_iterations, double avg_distance, const double *cond_dirac,
+                                  const double *cond_sigma);
 /* The CUDA stream (cudaStream_t) the ensemble's work runs on. */
 GN_API void *gn_ensemble_stream(gn_ensemble *ens);
 /* The layout in use, whether the last run used the graph, kernel launches per trajectory. */

@@ -168,6 +168,13 @@ GN_API void ComputeCondensateDirac(const struct Lattice *lat, double *condensate
                                    const struct Fermioncoor *fermioncoor, double inversion_precision,
                                    struct Fermionkit *kit, int f);
 
+/* ---- observables.c ----------------------------------------------------------- */
+/* observables.c:323 (the Z2 model: SIGMA_INTERACTION without PI_INTERACTION);
+ * the sums over lat->sigma run on the device */
+GN_API void CondensateSigmaPi(const struct Lattice *lat, const struct Info *info, double *condensate_sigma,
+                              double *condensate_sigma_abs, double *mu2, double *mu4, double *chi, double *chip,
+                              double *chip_pbc1, double *chip_pbc2);
+
 #undef GN_COMPLEX
 #ifdef __cplusplus
 }

@@ -245,6 +245,10 @@ class Ref:
         lib.gnref_info.argtypes = [_ip, _ip, _dp]
         lib.gnref_condensate.argtypes = [C.c_double, _dp]
         lib.gnref_seed.argtypes = [C.c_uint]
+        lib.gnref_condensate_sigma.argtypes = [_dp]
+        lib.gnref_write_lattice.argtypes = [C.c_char_p, C.c_char_p, _dp, _ip]
+        lib.gnref_read_lattice.argtypes = [C.c_char_p, C.c_char_p, _dp, _ip]
+        lib.gnref_read_lattice.restype = C.c_double
 
     def init(self, seed=1231, beta_s=0.85, eps=0.2, steps=2):
         self.lib.gnref_init(seed, beta_s, eps, steps)
@@ -346,3 +350,31 @@ class Ref:
         out = np.zeros(11)
         self.lib.gnref_condensate(tol, _p(out))
         return out
+
+    # ---- observables.c:323 and the lattice file (simulation.c:129-401) ----
+    COUNTER_INTS = ("story_link", "story_sigma", "story_pi", "accepted_link", "done_link", "accepted_sigma",
+                    "done_sigma", "accepted_pi", "done_pi", "measure")
+
+    def condensate_sigma(self):
+        """CondensateSigmaPi of the current sigma: the 8 outputs in its argument order."""
+        out = np.zeros(8)
+        self.lib.gnref_condensate_sigma(_p(out))
+        return out
+
+    def write_lattice(self, path, copy, counters):
+        """WriteBinaryLattice of the current sigma (links: identity); counters a dict
+        with epsilon_link, epsilon_pi and the COUNTER_INTS keys."""
+        eps = np.array([counters["epsilon_link"], counters["epsilon_pi"]], dtype=np.float64)
+        ints = (C.c_int * 10)(*[int(counters[k]) for k in self.COUNTER_INTS])
+        self.lib.gnref_write_lattice(str(path).encode(), str(copy).encode(), _p(eps), ints)
+
+    def read_lattice(self, path, copy):
+        """ReadBinaryLattice(path, try_copy): returns (sigma, counters, check),
+        check = TestWriteReadLattice of what was read.  Only for files that read
+        in full (the reference exits otherwise)."""
+        eps = np.zeros(2)
+        ints = (C.c_int * 10)()
+        check = self.lib.gnref_read_lattice(str(path).encode(), str(copy).encode(), _p(eps), ints)
+        counters = {"epsilon_link": float(eps[0]), "epsilon_pi": float(eps[1])}
+        counters.update({k: int(ints[i]) for i, k in enumerate(self.COUNTER_INTS)})
+        return self.sigma(), counters, check

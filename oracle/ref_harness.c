@@ -326,3 +326,74 @@ int gnref_layout(long *out)
     out[n++] = sizeof(struct RandomVec);
     return n;
 }
+
+/* ---- observables and the lattice file (outside the solver path) ---------- */
+#include "observables.h"
+#include "simulation.h"
+
+/* CondensateSigmaPi (observables.c:323) of the harness sigma; out[8] in its
+ * argument order. */
+void gnref_condensate_sigma(double *out)
+{
+    CondensateSigmaPi(&g_lat, &g_info, &out[0], &out[1], &out[2], &out[3], &out[4], &out[5], &out[6], &out[7]);
+}
+
+/* A Simulation around the harness lattice, for the reference's file functions. */
+static void sim_around_lattice(struct Simulation *sim, const char *path, const char *copy)
+{
+    memset(sim, 0, sizeof(*sim));
+    sim->lattice = &g_lat;
+    sim->fcor = &g_fcor;
+    sim->kit = &g_kit;
+    sim->info = g_info;
+    strncpy(sim->terma_file, path, sizeof(sim->terma_file) - 1);
+    strncpy(sim->terma_file_copy, copy, sizeof(sim->terma_file_copy) - 1);
+}
+
+/* WriteBinaryLattice (simulation.c:129) of the harness sigma (its mass
+ * recomputed by ComputeFullSigmaMass first).  eps[2] = epsilon_link_HMC,
+ * epsilon_pi_HMC; ints[10] = story_link, story_sigma, story_pi,
+ * hybrid_accepted/done_link, _sigma, _pi, measure. */
+void gnref_write_lattice(const char *path, const char *copy, const double *eps, const int *ints)
+{
+    struct Simulation sim;
+    sim_around_lattice(&sim, path, copy);
+    ComputeFullSigmaMass(&g_lat, &g_fcor, g_lat.sigmamass);
+    sim.info.epsilon_link_HMC = eps[0];
+    sim.info.epsilon_pi_HMC = eps[1];
+    sim.info.story_link = ints[0];
+    sim.info.story_sigma = ints[1];
+    sim.info.story_pi = ints[2];
+    sim.info.hybrid_accepted_link = ints[3];
+    sim.info.hybrid_done_link = ints[4];
+    sim.info.hybrid_accepted_sigma = ints[5];
+    sim.info.hybrid_done_sigma = ints[6];
+    sim.info.hybrid_accepted_pi = ints[7];
+    sim.info.hybrid_done_pi = ints[8];
+    sim.info.measure = ints[9];
+    WriteBinaryLattice(&sim);
+}
+
+/* ReadBinaryLattice (simulation.c:191) with try_copy into the harness lattice;
+ * the counters as above; returns TestWriteReadLattice of what it read (the
+ * value the reader compares with the stored one).  Only for files that read
+ * in full: the reference exits when a file and its copy both fail. */
+double gnref_read_lattice(const char *path, const char *copy, double *eps, int *ints)
+{
+    struct Simulation sim;
+    sim_around_lattice(&sim, path, copy);
+    ReadBinaryLattice(&sim, path, true);
+    eps[0] = sim.info.epsilon_link_HMC;
+    eps[1] = sim.info.epsilon_pi_HMC;
+    ints[0] = sim.info.story_link;
+    ints[1] = sim.info.story_sigma;
+    ints[2] = sim.info.story_pi;
+    ints[3] = sim.info.hybrid_accepted_link;
+    ints[4] = sim.info.hybrid_done_link;
+    ints[5] = sim.info.hybrid_accepted_sigma;
+    ints[6] = sim.info.hybrid_done_sigma;
+    ints[7] = sim.info.hybrid_accepted_pi;
+    ints[8] = sim.info.hybrid_done_pi;
+    ints[9] = sim.info.measure;
+    return TestWriteReadLattice(&sim);
+}
