@@ -48,7 +48,10 @@ class Ensemble {
   void run(const gn_ens_params &p, int ntraj, bool graph);
   void stats(gn_chain_stats *out, bool reset);
   void observables(double *out);
-  int checkpoint_save(int c, const char *path, const char *copy, const gn_hmc_counters &cnt);
+  int checkpoint_save(int c, const char *path, const char *copy, const gn_hmc_counters *cnt);
+  void set_autoregulation(int c, bool on);
+  EnsState state(int c);
+  void set_state(int c, const EnsState &h);
   int checkpoint_load(int c, const char *path, const char *copy, gn_hmc_counters *cnt);
   void info(int *gs, long long *big_min, int *graph_used, int *launches);
 
@@ -472,6 +475,11 @@ void Ensemble::stats(gn_chain_stats *out, bool reset) {
       o.last_dH = h[c].last_dH;
       o.last_accepted = h[c].last_acc;
       o.total_trajectories = h[c].ntraj;
+      o.total_accepted = h[c].total_acc;
+      o.story = h[c].story;
+      o.local_accepted = h[c].local_acc;
+      o.local_done = h[c].local_done;
+      o.epsilon_scale = h[c].eps_scale > 0.0 ? h[c].eps_scale : 1.0;
     }
     if (reset) {
       h[c].n = h[c].nacc = h[c].iters = h[c].reliable = h[c].fails = 0;
@@ -494,12 +502,43 @@ void Ensemble::observables(double *out) {
       out[size_t(c) * kSigmaObs + q] = h[c].n > 0 ? h[c].sum_obs[q] / double(h[c].n) : 0.0;
 }
 
-int Ensemble::checkpoint_save(int c, const char *path, const char *copy, const gn_hmc_counters &cnt) {
+EnsState Ensemble::state(int c) {
+  EnsState h;
+  check(cudaMemcpyAsync(&h, d_states_ + c, sizeof(EnsState), cudaMemcpyDeviceToHost, stream_), "copy state");
+  check(cudaStreamSynchronize(stream_), "state");
+  return h;
+}
+
+void Ensemble::set_state(int c, const EnsState &h) {
+  check(cudaMemcpyAsync(d_states_ + c, &h, sizeof(EnsState), cudaMemcpyHostToDevice, stream_), "copy state");
+  check(cudaStreamSynchronize(stream_), "state");
+}
+
+void Ensemble::set_autoregulation(int c, bool on) {
+  if (c >= n_) throw GnError(GN_ERR_ARG, "bad chain");
+  for (int k = (c < 0 ? 0 : c); k < (c < 0 ? n_ : c + 1); k++) {
+    EnsState h = state(k);
+    h.autoreg = on ? 1 : 0;
+    h.local_acc = h.local_done = 0;
+    set_state(k, h);
+  }
+}
+
+int Ensemble::checkpoint_save(int c, const char *path, const char *copy, const gn_hmc_counters *cnt) {
   if (c < 0 || c >= n_) throw GnError(GN_ERR_ARG, "bad chain");
   const size_t V = size_t(chains_[c].g.V);
   std::vector<double> sigma(V), sm(V);
   store_sigma(c, sigma.data(), sm.data());
-  return write_lattice_file(path, copy, chains_[c].g.L, sigma.data(), sm.data(), nullptr, cnt);
+  gn_hmc_counters own;
+  memset(&own, 0, sizeof own);
+  if (cnt == nullptr) {  // the chain's own bookkeeping
+    const EnsState h = state(c);
+    own.accepted_sigma = int(h.total_acc);
+    own.done_sigma = int(h.ntraj);
+    own.story_sigma = h.story;
+    cnt = &own;
+  }
+  return write_lattice_file(path, copy, chains_[c].g.L, sigma.data(), sm.data(), nullptr, *cnt);
 }
 
 int Ensemble::checkpoint_load(int c, const char *path, const char *copy, gn_hmc_counters *cnt) {
@@ -514,9 +553,19 @@ int Ensemble::checkpoint_load(int c, const char *path, const char *copy, gn_hmc_
     replaced = true;
   };
   auto accept = [&](const double *sigma) { load_sigma(c, sigma); };
-  const int st = load_lattice(path, copy, chains_[c].g.L, cnt, sm_of, accept);
-  if (st != GN_OK && replaced) load_sigma(c, old.data());
-  return st;
+  gn_hmc_counters got;
+  const int st = load_lattice(path, copy, chains_[c].g.L, &got, sm_of, accept);
+  if (st != GN_OK) {
+    if (replaced) load_sigma(c, old.data());
+    return st;
+  }
+  EnsState h = state(c);  // resume the chain's bookkeeping and Philox counter
+  h.ntraj = got.done_sigma;
+  h.total_acc = got.accepted_sigma;
+  h.story = got.story_sigma;
+  set_state(c, h);
+  if (cnt) *cnt = got;
+  return GN_OK;
 }
 
 void Ensemble::info(int *gs, long long *big_min, int *graph_used, int *launches) {
@@ -623,11 +672,18 @@ int gn_ensemble_observables(gn_ensemble *e, double *out) {
   });
 }
 
+int gn_ensemble_set_autoregulation(gn_ensemble *e, int chain, int on) {
+  return ens_guarded(e, [&](gn::Ensemble &E) {
+    E.set_autoregulation(chain, on != 0);
+    return GN_OK;
+  });
+}
+
 int gn_ensemble_checkpoint_save(gn_ensemble *e, int chain, const char *path, const char *path_copy,
                                 const gn_hmc_counters *c) {
-  if (path == nullptr || c == nullptr) return gn::set_last_error(GN_ERR_ARG, "null pointer");
+  if (path == nullptr) return gn::set_last_error(GN_ERR_ARG, "null pointer");
   return ens_guarded(e, [&](gn::Ensemble &E) -> int {
-    const int st = E.checkpoint_save(chain, path, path_copy, *c);
+    const int st = E.checkpoint_save(chain, path, path_copy, c);
     return st == GN_OK ? GN_OK : gn::set_last_error(st, "cannot write the lattice file");
   });
 }

@@ -76,6 +76,12 @@ struct EnsState {
   double sum_dH, sum_exp_mdH, sum_sigma2, last_dH;
   double sum_obs[kSigmaObs];  // CondensateSigmaPi outputs after each trajectory
   int last_acc;
+  // HMC bookkeeping of the reference's struct Info (moleculardynamics.c:1385-1416)
+  long long total_acc;  // hybrid_accepted_sigma (total_acc of ntraj trajectories)
+  int story;            // story_sigma: +n after n accepts in a row, -n after n rejects
+  int local_acc, local_done;
+  int autoreg;          // UpdateHMCParameters (info.c:123-135) after every trajectory
+  double eps_scale;     // the chain's epsilon / the launch's (0 stands for 1)
   // the current request of a served chain
   unsigned long long serial;  // Philox counter of the request's draws
   double result;              // E_TRACE accumulator
@@ -138,6 +144,9 @@ __device__ __forceinline__ void box_muller(uint64_t a, uint64_t b, double &z0, d
   z0 = r * c;
   z1 = r * s;
 }
+
+// The factor of the chain's own step size on the launch's step coefficients.
+__device__ __forceinline__ double eps_scale(const EnsState *st) { return st->eps_scale > 0.0 ? st->eps_scale : 1.0; }
 
 // The chain's ops [op_begin, op_end) by team t.  Returns false on a barrier timeout.
 static __device__ __noinline__ bool ens_run_chain(const EnsLaunch &L, int c, Team &t, SyncShared &sh, MixedShared &ms,
@@ -261,15 +270,18 @@ static __device__ __noinline__ bool ens_run_chain(const EnsLaunch &L, int c, Tea
       else team_dirac2<1, 1>(g, t, ch.sm, ch.X, ch.Y);
       ok = end_phase<0>(acc, sh, t);
       const double gcoef = (4 * ch.beta_s / 2.0);  // (NFLAV * beta_scalar / 2.0), moleculardynamics.c:580
+      const double pc = op.c * eps_scale(st);
       for (uint32_t i = t.tid; i < V && ok; i += t.nthreads)
-        force_site<double, false>(g, i, ch.X, ch.Y, sig, gcoef, ch.F, ch.P, op.c);
+        force_site<double, false>(g, i, ch.X, ch.Y, sig, gcoef, ch.F, ch.P, pc);
       ok = end_phase<0>(acc, sh, t) && ok;
     } else if (op.code == E_P) {
-      for (uint32_t i = t.tid; i < V; i += t.nthreads) ch.P[i] = ch.P[i] + ch.F[i] * op.c;
+      const double pc = op.c * eps_scale(st);
+      for (uint32_t i = t.tid; i < V; i += t.nthreads) ch.P[i] = ch.P[i] + ch.F[i] * pc;
       ok = end_phase<0>(acc, sh, t);
     } else if (op.code == E_Q) {
+      const double qc = op.c * eps_scale(st);
       for (uint32_t i = t.tid; i < V; i += t.nthreads)
-        sigma_mass_site<double, false>(g, i, sig, ch.P, op.c, sig_o, ch.sm);
+        sigma_mass_site<double, false>(g, i, sig, ch.P, qc, sig_o, ch.sm);
       cur ^= 1;
       ok = end_phase<0>(acc, sh, t);
     } else if (op.code == E_ENERGY0 || op.code == E_ENERGY1) {
@@ -322,6 +334,24 @@ static __device__ __noinline__ bool ens_run_chain(const EnsLaunch &L, int c, Tea
         st->last_dH = dH;
         st->last_acc = accept;
         st->ntraj++;
+        // acceptance bookkeeping and epsilon autoregulation (a failed solve
+        // counts as a reject here; the reference exits instead)
+        st->total_acc += accept;
+        st->local_acc += accept;
+        st->local_done++;
+        if (accept) st->story = st->story >= 0 ? st->story + 1 : -1;
+        else st->story = st->story >= 0 ? -1 : st->story - 1;
+        if (st->autoreg && st->local_done == 100) {
+          const double a = double(st->local_acc) / double(st->local_done);
+          double sc = eps_scale(st);
+          if (a >= 0.85) sc = sc * 1.15;
+          else if (a >= 0.8) sc = sc * 1.08;
+          else if (a >= 0.75) sc = sc / 1.08;
+          else sc = sc / 1.15;
+          st->eps_scale = sc;
+          st->local_acc = 0;
+          st->local_done = 0;
+        }
       }
     } else if (op.code == E_RHS) {
       const unsigned long long serial = st->serial;

@@ -72,7 +72,9 @@ class ChainStats(C.Structure):
     _fields_ = [("trajectories", C.c_longlong), ("accepted", C.c_longlong), ("failed", C.c_longlong),
                 ("cg_iterations", C.c_longlong), ("reliable_updates", C.c_longlong), ("sum_dH", C.c_double),
                 ("sum_exp_mdH", C.c_double), ("sum_sigma2", C.c_double), ("last_dH", C.c_double),
-                ("last_accepted", C.c_int), ("total_trajectories", C.c_longlong)]
+                ("last_accepted", C.c_int), ("total_trajectories", C.c_longlong), ("total_accepted", C.c_longlong),
+                ("story", C.c_int), ("local_accepted", C.c_int), ("local_done", C.c_int),
+                ("epsilon_scale", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -104,6 +106,7 @@ class HmcCounters(C.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
 
 _dp = C.POINTER(C.c_double)
 _lib = None
@@ -187,6 +190,7 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
         "gn_checkpoint_save": ([v, C.c_char_p, C.c_char_p, C.POINTER(HmcCounters)], C.c_int),
         "gn_checkpoint_load": ([v, C.c_char_p, C.c_char_p, C.POINTER(HmcCounters)], C.c_int),
         "gn_ensemble_observables": ([v, _dp], C.c_int),
+        "gn_ensemble_set_autoregulation": ([v, C.c_int, C.c_int], C.c_int),
         "gn_ensemble_checkpoint_save": ([v, C.c_int, C.c_char_p, C.c_char_p, C.POINTER(HmcCounters)], C.c_int),
         "gn_ensemble_checkpoint_load": ([v, C.c_int, C.c_char_p, C.c_char_p, C.POINTER(HmcCounters)], C.c_int),
         "gn_format_measure_line": ([C.c_char_p, C.c_size_t, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
@@ -569,9 +573,17 @@ class Ensemble:
         self._check(self.lib.gn_ensemble_observables(self.ens, _p(out)))
         return out.reshape(self.n, 8)
 
-    def checkpoint_save(self, c, path, path_copy, counters):
-        cnt = counters if isinstance(counters, HmcCounters) else HmcCounters.from_dict(counters)
-        self._check(self.lib.gn_ensemble_checkpoint_save(self.ens, c, _path(path), _path(path_copy), C.byref(cnt)))
+    def set_autoregulation(self, on=True, chain=-1):
+        """UpdateHMCParameters per chain after every trajectory (chain -1: all)."""
+        self._check(self.lib.gn_ensemble_set_autoregulation(self.ens, int(chain), int(on)))
+
+    def checkpoint_save(self, c, path, path_copy=None, counters=None):
+        """counters None: the chain's own (accepted, done, story)."""
+        if counters is None:
+            cnt = None
+        else:
+            cnt = C.byref(counters if isinstance(counters, HmcCounters) else HmcCounters.from_dict(counters))
+        self._check(self.lib.gn_ensemble_checkpoint_save(self.ens, c, _path(path), _path(path_copy), cnt))
 
     def checkpoint_load(self, c, path, path_copy=None):
         cnt = HmcCounters()

@@ -339,6 +339,11 @@ typedef struct {
   double last_dH;
   int last_accepted;
   long long total_trajectories; /* since creation (the Philox counter of the next one) */
+  /* the reference's struct Info bookkeeping of the chain (moleculardynamics.c:1385-1416) */
+  long long total_accepted;     /* hybrid_accepted_sigma; hybrid_done_sigma is total_trajectories */
+  int story;                    /* story_sigma: +n after n accepts in a row, -n after n rejects */
+  int local_accepted, local_done;
+  double epsilon_scale;         /* the chain's epsilon / gn_ens_params.eps (autoregulation) */
 } gn_chain_stats;
 
 /* nchains chains: L[c], beta_s[c]; stream_ids[c] (NULL: c) keys each chain's
@@ -370,8 +375,21 @@ GN_API int gn_ensemble_stats(gn_ensemble *ens, gn_chain_stats *out, int reset);
  * observables.c:259-292, with IMEAS = the trajectories since the last reset);
  * gn_ensemble_stats(..., reset = 1) zeroes them with the other accumulators. */
 GN_API int gn_ensemble_observables(gn_ensemble *ens, double *out);
+/* UpdateHMCParameters (info.c:123-135, the reference's AUTOREGULATION) for
+ * chain c (c < 0: every chain), on the device after every trajectory: after
+ * 100 trajectories the chain's epsilon is multiplied by 1.15 / 1.08 or
+ * divided by 1.08 / 1.15 for a local acceptance >= 0.85 / >= 0.8 / >= 0.75 /
+ * below, and the local counters restart.  Switching on restarts them too.
+ * The epsilon of chain c is gn_ens_params.eps times its epsilon_scale. */
+GN_API int gn_ensemble_set_autoregulation(gn_ensemble *ens, int chain, int on);
 /* Checkpoint of chain c in the reference's lattice file (gn_checkpoint_save /
- * gn_checkpoint_load; load puts sigma in place of the chain's). */
+ * gn_checkpoint_load).  save with c == NULL takes the sigma counters from the
+ * chain (accepted_sigma = total_accepted, done_sigma = total_trajectories,
+ * story_sigma = story; the others 0).  load puts sigma in place of the
+ * chain's and sets total_trajectories, total_accepted and story from the
+ * file's done_sigma, accepted_sigma and story_sigma: the trajectory count is
+ * the chain's Philox counter, so a chain reloaded with the same seed and
+ * stream id continues its random stream where it stopped. */
 GN_API int gn_ensemble_checkpoint_save(gn_ensemble *ens, int chain, const char *path, const char *path_copy,
                                        const gn_hmc_counters *c);
 GN_API int gn_ensemble_checkpoint_load(gn_ensemble *ens, int chain, const char *path, const char *path_copy,

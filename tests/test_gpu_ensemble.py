@@ -144,3 +144,75 @@ def test_fp64_and_mixed_chains_agree():
     for a, b in zip(out[G.GN_PREC_FP64][0], out[G.GN_PREC_MIXED][0]):
         assert np.max(np.abs(a - b)) / np.max(np.abs(a)) < 1e-7
     assert np.allclose(out[G.GN_PREC_FP64][1], out[G.GN_PREC_MIXED][1], rtol=0, atol=1e-6)
+
+
+def test_checkpoint_resume_is_exact(tmp_path):
+    """Two trajectories, a checkpoint of every chain (the chain's own counters),
+    a new ensemble with the same seed and stream ids loading them, two more
+    trajectories: bit for bit the chain that ran four trajectories without a
+    stop.  The file's done_sigma is the chain's Philox counter."""
+    import gn_b200 as G
+    Ls, betas = [8, 12], [0.85, 1.0]
+    p = G.Ensemble.params(0.08, 4, tol=1e-10)
+
+    def fresh():
+        e = G.Ensemble(Ls, betas, seed=2024)
+        for c, L in enumerate(Ls):
+            e.load_sigma(c, _sigma0(L, betas[c], 31 + c))
+        return e
+
+    with fresh() as whole:
+        whole.run(p, 4)
+        want = [whole.store_sigma(c)[0] for c in range(len(Ls))]
+        want_stats = whole.stats()
+    with fresh() as first:
+        first.run(p, 2)
+        for c in range(len(Ls)):
+            first.checkpoint_save(c, tmp_path / f"chain{c}.bin")
+    with G.Ensemble(Ls, betas, seed=2024) as second:
+        for c in range(len(Ls)):
+            st, cnt = second.checkpoint_load(c, tmp_path / f"chain{c}.bin")
+            assert st == G.GN_OK and cnt["done_sigma"] == 2
+        second.run(p, 2)
+        for c in range(len(Ls)):
+            assert np.array_equal(second.store_sigma(c)[0], want[c])
+        got = second.stats()
+        for c in range(len(Ls)):
+            assert got[c]["total_trajectories"] == 4
+            assert got[c]["total_accepted"] == want_stats[c]["total_accepted"]
+            assert got[c]["story"] == want_stats[c]["story"]
+
+
+def test_autoregulation_follows_update_hmc_parameters():
+    """UpdateHMCParameters (info.c:123-135) after 100 trajectories: the step
+    grows by 1.15 at local acceptance >= 0.85 (a small step) and shrinks by
+    1.15 below 0.75 (a large one); the local counters restart."""
+    import gn_b200 as G
+    Ls, betas = [4, 4], [0.85, 0.85]
+    with G.Ensemble(Ls, betas, seed=5) as ens:
+        for c in range(2):
+            ens.load_sigma(c, _sigma0(4, 0.85, 70 + c))
+        ens.set_autoregulation(True)
+        acc = [[], []]  # a small step: acceptance near 1
+        for _ in range(100):
+            ens.run(G.Ensemble.params(0.05, 4, tol=1e-10), 1)
+            for c, s in enumerate(ens.stats()):
+                acc[c].append(s["last_accepted"])
+        st = ens.stats()
+        for c in range(2):
+            a = sum(acc[c]) / 100.0
+            want = 1.15 if a >= 0.85 else 1.08 if a >= 0.8 else 1 / 1.08 if a >= 0.75 else 1 / 1.15
+            assert st[c]["epsilon_scale"] == pytest.approx(want, rel=1e-15)
+            assert st[c]["local_done"] == 0 and st[c]["local_accepted"] == 0
+            assert st[c]["total_trajectories"] == 100
+    with G.Ensemble([4], [0.85], seed=6) as ens:  # a large step: acceptance low
+        ens.load_sigma(0, _sigma0(4, 0.85, 80))
+        ens.set_autoregulation(True)
+        acc = []
+        for _ in range(100):
+            ens.run(G.Ensemble.params(1.5, 4, tol=1e-10), 1)
+            acc.append(ens.stats()[0]["last_accepted"])
+        a = sum(acc) / 100.0
+        want = 1.15 if a >= 0.85 else 1.08 if a >= 0.8 else 1 / 1.08 if a >= 0.75 else 1 / 1.15
+        assert a < 0.75
+        assert ens.stats()[0]["epsilon_scale"] == pytest.approx(want, rel=1e-15)
