@@ -34,6 +34,7 @@ UNITS = {
     "ensemble.cu": ["--fmad=false"],
     "serve.cu": ["--fmad=false"],
     "checkpoint.cu": [],
+    "u1.cu": ["--fmad=false"],
 }
 CORE_LIB = LIB / "libgn_b200.so"
 DROPIN_LIB = LIB / "libgn_dropin.so"

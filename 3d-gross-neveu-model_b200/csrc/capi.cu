@@ -327,6 +327,146 @@ int gn_checkpoint_load(gn_context *ctx, const char *path, const char *path_copy,
   });
 }
 
+// ---- the U(1) model
+int gn_set_u1(gn_context *ctx, int on) {
+  return guarded(ctx, [&](gn::Engine &E) {
+    E.set_u1(on != 0);
+    return GN_OK;
+  });
+}
+
+int gn_load_pi(gn_context *ctx, const double *pi) {
+  if (!pi) return fail(GN_ERR_ARG, "null pointer");
+  return guarded(ctx, [&](gn::Engine &E) {
+    E.set_u1(true);
+    up(E, E.pi(), pi, size_t(E.V()));
+    E.sigma_mass(E.pi(), nullptr, 0.0, nullptr, E.pm());  // ComputeFullPiMass: the same 8-corner mean
+    sync(E);
+    return GN_OK;
+  });
+}
+
+int gn_store_pi(gn_context *ctx, double *pi, double *pimass) {
+  return guarded(ctx, [&](gn::Engine &E) -> int {
+    if (!E.u1()) return fail(GN_ERR_ARG, "the context is not in the U(1) model");
+    if (pi) down(E, pi, E.pi(), size_t(E.V()));
+    if (pimass) down(E, pimass, E.pm(), size_t(E.V()));
+    sync(E);
+    return GN_OK;
+  });
+}
+
+int gn_dirac_u1(gn_context *ctx, const double *sigmamass, const double *pimass, const double *in, double *out,
+                int nsys, int op) {
+  if (!sigmamass || !pimass || !in || !out) return fail(GN_ERR_ARG, "null pointer");
+  if (nsys < 1 || nsys > 4 || op < 0 || op > 2) return fail(GN_ERR_ARG, "bad nsys / op");
+  return guarded(ctx, [&](gn::Engine &E) {
+    const size_t V = size_t(E.V());
+    double *d_sm = ctx->io, *d_pm = d_sm + V, *d_in = d_pm + V, *d_out = d_in + 8 * V;
+    up(E, d_sm, sigmamass, V);
+    up(E, d_pm, pimass, V);
+    up(E, d_in, in, 2 * size_t(nsys) * V);
+    if (op == GN_OP_SUB_M) up(E, d_out, out, 2 * size_t(nsys) * V);
+    E.dirac_cm(d_sm, d_pm, d_in, d_out, nsys, op);
+    down(E, out, d_out, 2 * size_t(nsys) * V);
+    sync(E);
+    return GN_OK;
+  });
+}
+
+int gn_cg_u1(gn_context *ctx, const double *sigmamass, const double *pimass, const double *b, double *x, int nrhs,
+             double tol, int variant, int relative, long long max_iter, gn_cg_info *info) {
+  if (!sigmamass || !pimass || !b || !x) return fail(GN_ERR_ARG, "null pointer");
+  if (nrhs < 1 || nrhs > 2) return fail(GN_ERR_ARG, "nrhs must be 1 or 2");
+  return guarded(ctx, [&](gn::Engine &E) {
+    const size_t V = size_t(E.V());
+    double *d_sm = ctx->io, *d_pm = d_sm + V, *d_b = d_pm + V, *d_x = d_b + 4 * V;
+    up(E, d_sm, sigmamass, V);
+    up(E, d_pm, pimass, V);
+    up(E, d_b, b, 2 * size_t(nrhs) * V);
+    up(E, d_x, x, 2 * size_t(nrhs) * V);
+    const double *bs[2] = {d_b, d_b + 2 * V};
+    double *xs[2] = {d_x, d_x + 2 * V};
+    gn::SolveInfo si[2];
+    const int st = E.solve_cm(d_sm, d_pm, bs, xs, nrhs, tol, variant, relative, max_iter, si);
+    down(E, x, d_x, 2 * size_t(nrhs) * V);
+    sync(E);
+    if (info)
+      for (int k = 0; k < nrhs; k++) fill_info(si[k], &info[k]);
+    return st;
+  });
+}
+
+static int force_u1(gn_context *ctx, bool pi, double beta_s, const double *field, const double *sigmamass,
+                    const double *pimass, const double *phi, double *X, double *Y, double tol, double *force,
+                    gn_cg_info *info) {
+  if (!field || !sigmamass || !pimass || !phi || !X || !Y || !force) return fail(GN_ERR_ARG, "null pointer");
+  return guarded(ctx, [&](gn::Engine &E) {
+    const size_t V = size_t(E.V());
+    double *d_f = ctx->io, *d_sm = d_f + V, *d_pm = d_sm + V, *d_phi = d_pm + V, *d_X = d_phi + 4 * V,
+           *d_Y = d_X + 4 * V, *d_F = d_Y + 4 * V;
+    up(E, d_f, field, V);
+    up(E, d_sm, sigmamass, V);
+    up(E, d_pm, pimass, V);
+    up(E, d_phi, phi, 4 * V);
+    up(E, d_X, X, 4 * V);
+    const double *bs[2] = {d_phi, d_phi + 2 * V};
+    double *xs[2] = {d_X, d_X + 2 * V};
+    gn::SolveInfo si[2];
+    const int st = E.solve_cm(d_sm, d_pm, bs, xs, 2, tol, 0, 0, 0, si);
+    if (st == GN_OK) {
+      E.dirac_cm(d_sm, d_pm, d_X, d_Y, 2, GN_OP_MT);
+      // (NFLAV * beta_scalar / 4.0) for pi (moleculardynamics.c:685), / 2.0 for sigma (:580)
+      const double gcoef = pi ? (4 * beta_s / 4.0) : (4 * beta_s / 2.0);
+      E.force_cm(pi, d_X, d_Y, d_f, gcoef, d_F, nullptr, 0.0);
+      down(E, Y, d_Y, 4 * V);
+      down(E, force, d_F, V);
+    }
+    down(E, X, d_X, 4 * V);
+    sync(E);
+    if (st != GN_OK) memset(force, 0, V * sizeof(double));  // the force was zeroed first
+    if (info)
+      for (int k = 0; k < 2; k++) fill_info(si[k], &info[k]);
+    return st;
+  });
+}
+
+int gn_sigma_force_u1(gn_context *ctx, double beta_s, const double *sigma, const double *sigmamass,
+                      const double *pimass, const double *phi, double *X, double *Y, double tol, double *force,
+                      gn_cg_info *info) {
+  return force_u1(ctx, false, beta_s, sigma, sigmamass, pimass, phi, X, Y, tol, force, info);
+}
+
+int gn_pi_force(gn_context *ctx, double beta_s, const double *pi, const double *sigmamass, const double *pimass,
+                const double *phi, double *X, double *Y, double tol, double *force, gn_cg_info *info) {
+  return force_u1(ctx, true, beta_s, pi, sigmamass, pimass, phi, X, Y, tol, force, info);
+}
+
+int gn_energy_u1(gn_context *ctx, int which, double beta_s, const double *field, const double *P, const double *phi,
+                 const double *X, double *H) {
+  if (!field || !P || !phi || !X || !H) return fail(GN_ERR_ARG, "null pointer");
+  if (which != 0 && which != 1) return fail(GN_ERR_ARG, "which: 0 sigma, 1 pi");
+  return guarded(ctx, [&](gn::Engine &E) {
+    const size_t V = size_t(E.V());
+    double *d_f = ctx->io, *d_P = d_f + V, *d_phi = d_P + V, *d_X = d_phi + 4 * V;
+    up(E, d_f, field, V);
+    up(E, d_P, P, V);
+    up(E, d_phi, phi, 4 * V);
+    up(E, d_X, X, 4 * V);
+    double e[3];
+    E.energy_cm(d_P, d_phi, d_X, d_f, e);
+    const double coef = which == 0 ? (4 * beta_s / 4.0) : (4 * beta_s / 8.0);
+    *H = (e[0] + e[1]) + coef * e[2];
+    return GN_OK;
+  });
+}
+
+int gn_trajectory_pi(gn_context *ctx, const gn_hmc_params *params, void (*gauss_pair)(double *, double *),
+                     double (*gauss)(void), double (*uniform)(void), gn_traj_result *res) {
+  if (!params || !res) return fail(GN_ERR_ARG, "null pointer");
+  return guarded(ctx, [&](gn::Engine &E) { return E.trajectory_pi(*params, gauss_pair, gauss, uniform, res); });
+}
+
 int gn_load_sigma(gn_context *ctx, const double *sigma) {
   if (!sigma) return fail(GN_ERR_ARG, "null pointer");
   return guarded(ctx, [&](gn::Engine &E) {
@@ -355,6 +495,16 @@ static double *field_ptr(gn::Engine &E, int field, size_t &n) {
     case GN_F_PHI: n = 2 * V; return E.phi();
     case GN_F_X: n = 2 * V; return E.X();
     case GN_F_Y: n = 2 * V; return E.Y();
+    default: break;
+  }
+  if (!E.u1()) throw gn::GnError(GN_ERR_ARG, "unknown field (U(1) fields need gn_load_pi first)");
+  switch (field) {
+    case GN_F_PI_P: n = V; return E.Ppi();
+    case GN_F_PI_F: n = V; return E.Fpi();
+    case GN_F_CHI_C: n = 4 * V; return E.chi_c();
+    case GN_F_PHI_C: n = 4 * V; return E.phi_c();
+    case GN_F_X_C: n = 4 * V; return E.X_c();
+    case GN_F_Y_C: n = 4 * V; return E.Y_c();
     default: throw gn::GnError(GN_ERR_ARG, "unknown field");
   }
 }
@@ -394,6 +544,8 @@ double *gn_field_ptr(gn_context *ctx, int field) {
   gn::Engine &E = *ctx->eng;
   if (field == GN_F_SIGMA) return E.sigma();
   if (field == GN_F_SM) return E.sm();
+  if (field == GN_F_PI) return E.u1() ? E.pi() : nullptr;
+  if (field == GN_F_PM) return E.u1() ? E.pm() : nullptr;
   try {
     size_t n = 0;
     return field_ptr(E, field, n);

@@ -56,6 +56,7 @@ struct CgArgs {
   T *p0[kMaxRhs];
   T *p1[kMaxRhs];
   T *t[kMaxRhs];
+  const T *pm;  // U(1) model: the pi mass of the complex diagonal (CM solves only)
   int nrhs;
   int variant;  // 0: test the incoming x first (START_X0_NULL form); 1: x = 0
   int rel;      // 0: stop at |r| < tol; 1: stop at |r| < tol |b|
@@ -128,7 +129,12 @@ struct CgShared {
 // One solve by a team (all its threads call it; a.bar, a.partials and a.err
 // are not used: the team's own are).  NR: right-hand-side slots unrolled
 // (>= nrhs); W: sites per item (divides L/2).
-template <typename T, int NC, int NR, int W>
+//
+// CM (NC = 2): the U(1) model's complex mass sm + i eps pm (rowvec.cuh), the
+// two planes of a system coupled through it; the CG formulas are the same,
+// with the global sums running over both planes (the real form of the
+// reference's complex CG).
+template <typename T, int NC, int NR, int W, bool CM = false>
 __device__ __forceinline__ void cg_solve(const CgArgs<T> &a, Team &team, SyncShared &sh, CgShared &cs) {
   double *const s_val = sh.val;
   double *const s_alpha = cs.alpha, *const s_beta = cs.beta, *const s_rr = cs.rr, *const s_tau = cs.tau;
@@ -141,6 +147,7 @@ __device__ __forceinline__ void cg_solve(const CgArgs<T> &a, Team &team, SyncSha
   const uint32_t V = uint32_t(g.V);
   const uint32_t NI = row_items<W>(g);
   const T *__restrict__ sm = a.sm;
+  static_assert(!CM || NC == 2, "the complex mass couples the two planes of a system");
 
   if (threadIdx.x < kMaxRhs) {
     const int k = threadIdx.x;
@@ -173,13 +180,24 @@ __device__ __forceinline__ void cg_solve(const CgArgs<T> &a, Team &team, SyncSha
       vload<T, W>(sm + it.own, smi);
       const T *xk = pick<NR>(a.x, k);
       T *tk = pick<NR>(a.t, k);
+      if constexpr (CM) {
+        Nb<T> nr[W], ni[W];
+        T b[W], o_r[W], o_i[W];
+        gather_item<T, W>(it, xk, nr);
+        gather_item<T, W>(it, xk + V, ni);
+        item_eps_pm<T, W>(g, it, a.pm, b);
+        item_Mt_cm<T, W>(it, smi, b, nr, ni, o_r, o_i);
+        vstore<T, W>(tk + it.own, o_r);
+        vstore<T, W>(tk + V + it.own, o_i);
+      } else {
 #pragma unroll
-      for (int c = 0; c < NC; c++) {
-        Nb<T> n[W];
-        T o[W];
-        gather_item<T, W>(it, xk + size_t(c) * V, n);
-        item_Mt<T, W>(it, smi, n, o);
-        vstore<T, W>(tk + size_t(c) * V + it.own, o);
+        for (int c = 0; c < NC; c++) {
+          Nb<T> n[W];
+          T o[W];
+          gather_item<T, W>(it, xk + size_t(c) * V, n);
+          item_Mt<T, W>(it, smi, n, o);
+          vstore<T, W>(tk + size_t(c) * V + it.own, o);
+        }
       }
     });
     zero_acc();
@@ -194,25 +212,51 @@ __device__ __forceinline__ void cg_solve(const CgArgs<T> &a, Team &team, SyncSha
         const T *tk = pick<NR>(a.t, k);
         const T *bk = pick<NR>(a.b, k);
         T *rk = pick<NR>(a.r, k);
+        if constexpr (CM) {
+          Nb<T> nr[W], ni[W];
+          T b[W], br[W], bim[W], rr[W], rim[W];
+          gather_item<T, W>(it, tk, nr);
+          gather_item<T, W>(it, tk + V, ni);
+          item_eps_pm<T, W>(g, it, a.pm, b);
+          vload<T, W>(bk + it.own, br);
+          vload<T, W>(bk + V + it.own, bim);
 #pragma unroll
-        for (int c = 0; c < NC; c++) {
-          const size_t off = size_t(c) * V + it.own;
-          Nb<T> n[W];
-          T bi[W], ri[W];
-          gather_item<T, W>(it, tk + size_t(c) * V, n);
-          vload<T, W>(bk + off, bi);
-#pragma unroll
-          for (int e = 0; e < W; e++) ri[e] = bi[e];
-          item_sub_M<T, W>(it, smi, n, ri);
-          vstore<T, W>(rk + off, ri);
+          for (int e = 0; e < W; e++) {
+            rr[e] = br[e];
+            rim[e] = bim[e];
+          }
+          item_sub_M_cm<T, W>(it, smi, b, nr, ni, rr, rim);
+          vstore<T, W>(rk + it.own, rr);
+          vstore<T, W>(rk + V + it.own, rim);
           double sr = 0.0, sb = 0.0;
 #pragma unroll
           for (int e = 0; e < W; e++) {
-            sr += double(ri[e]) * double(ri[e]);
-            sb += double(bi[e]) * double(bi[e]);
+            sr += double(rr[e]) * double(rr[e]) + double(rim[e]) * double(rim[e]);
+            sb += double(br[e]) * double(br[e]) + double(bim[e]) * double(bim[e]);
           }
           acc_add<NR>(acc, k, sr);
           acc_add<NR>(acc, NR + k, sb);
+        } else {
+#pragma unroll
+          for (int c = 0; c < NC; c++) {
+            const size_t off = size_t(c) * V + it.own;
+            Nb<T> n[W];
+            T bi[W], ri[W];
+            gather_item<T, W>(it, tk + size_t(c) * V, n);
+            vload<T, W>(bk + off, bi);
+#pragma unroll
+            for (int e = 0; e < W; e++) ri[e] = bi[e];
+            item_sub_M<T, W>(it, smi, n, ri);
+            vstore<T, W>(rk + off, ri);
+            double sr = 0.0, sb = 0.0;
+#pragma unroll
+            for (int e = 0; e < W; e++) {
+              sr += double(ri[e]) * double(ri[e]);
+              sb += double(bi[e]) * double(bi[e]);
+            }
+            acc_add<NR>(acc, k, sr);
+            acc_add<NR>(acc, NR + k, sb);
+          }
         }
       });
     }
@@ -302,37 +346,74 @@ __device__ __forceinline__ void cg_solve(const CgArgs<T> &a, Team &team, SyncSha
       const T *const po = odd ? pick<NR>(a.p0, k) : pick<NR>(a.p1, k);
       const T *rk = pick<NR>(a.r, k);
       T *tk = pick<NR>(a.t, k);
+      if constexpr (CM) {
+        Nb<T> n[2][W];
 #pragma unroll
-      for (int c = 0; c < NC; c++) {
-        const size_t off = size_t(c) * V;
-        Nb<T> n[W];
-        if (it == 0) {
-          gather_item<T, W>(ri, pn + off, n);
-        } else {
-          const T *rv = rk + off;
-          const T *pov = po + off;
-          gather_item<T, W>(
-              ri, n,
-              [&](uint32_t i, T(&v)[W]) {
-                T rr[W], pp[W];
-                vload<T, W>(rv + i, rr);
-                vload<T, W>(pov + i, pp);
+        for (int c = 0; c < 2; c++) {
+          const size_t off = size_t(c) * V;
+          if (it == 0) {
+            gather_item<T, W>(ri, pn + off, n[c]);
+          } else {
+            const T *rv = rk + off;
+            const T *pov = po + off;
+            gather_item<T, W>(
+                ri, n[c],
+                [&](uint32_t i, T(&v)[W]) {
+                  T rr[W], pp[W];
+                  vload<T, W>(rv + i, rr);
+                  vload<T, W>(pov + i, pp);
 #pragma unroll
-                for (int e = 0; e < W; e++) v[e] = rr[e] + beta * pp[e];
-              },
-              [&](uint32_t i) { return rv[i] + beta * pov[i]; });
-          T pc[W];
+                  for (int e = 0; e < W; e++) v[e] = rr[e] + beta * pp[e];
+                },
+                [&](uint32_t i) { return rv[i] + beta * pov[i]; });
+            T pc[W];
 #pragma unroll
-          for (int e = 0; e < W; e++) pc[e] = n[e].c;
-          vstore<T, W>(pn + off + ri.own, pc);
+            for (int e = 0; e < W; e++) pc[e] = n[c][e].c;
+            vstore<T, W>(pn + off + ri.own, pc);
+          }
         }
-        T ti[W];
-        item_Mt<T, W>(ri, smi, n, ti);
-        vstore<T, W>(tk + off + ri.own, ti);
+        T b[W], t_r[W], t_i[W];
+        item_eps_pm<T, W>(g, ri, a.pm, b);
+        item_Mt_cm<T, W>(ri, smi, b, n[0], n[1], t_r, t_i);
+        vstore<T, W>(tk + ri.own, t_r);
+        vstore<T, W>(tk + V + ri.own, t_i);
         double st = 0.0;
 #pragma unroll
-        for (int e = 0; e < W; e++) st += double(ti[e]) * double(ti[e]);
+        for (int e = 0; e < W; e++) st += double(t_r[e]) * double(t_r[e]) + double(t_i[e]) * double(t_i[e]);
         acc_add<NR>(acc, k, st);
+      } else {
+#pragma unroll
+        for (int c = 0; c < NC; c++) {
+          const size_t off = size_t(c) * V;
+          Nb<T> n[W];
+          if (it == 0) {
+            gather_item<T, W>(ri, pn + off, n);
+          } else {
+            const T *rv = rk + off;
+            const T *pov = po + off;
+            gather_item<T, W>(
+                ri, n,
+                [&](uint32_t i, T(&v)[W]) {
+                  T rr[W], pp[W];
+                  vload<T, W>(rv + i, rr);
+                  vload<T, W>(pov + i, pp);
+#pragma unroll
+                  for (int e = 0; e < W; e++) v[e] = rr[e] + beta * pp[e];
+                },
+                [&](uint32_t i) { return rv[i] + beta * pov[i]; });
+            T pc[W];
+#pragma unroll
+            for (int e = 0; e < W; e++) pc[e] = n[e].c;
+            vstore<T, W>(pn + off + ri.own, pc);
+          }
+          T ti[W];
+          item_Mt<T, W>(ri, smi, n, ti);
+          vstore<T, W>(tk + off + ri.own, ti);
+          double st = 0.0;
+#pragma unroll
+          for (int e = 0; e < W; e++) st += double(ti[e]) * double(ti[e]);
+          acc_add<NR>(acc, k, st);
+        }
       }
     });
     ok = end_phase<NR>(acc, sh, team);
@@ -354,26 +435,53 @@ __device__ __forceinline__ void cg_solve(const CgArgs<T> &a, Team &team, SyncSha
       const T *tk = pick<NR>(a.t, k);
       T *xk = pick<NR>(a.x, k);
       T *rk = pick<NR>(a.r, k);
-#pragma unroll
-      for (int c = 0; c < NC; c++) {
-        const size_t off = size_t(c) * V;
-        Nb<T> n[W];
-        T ap[W], pv[W], xv[W], rv[W];
-        gather_item<T, W>(ri, tk + off, n);
-        vload<T, W>(pn + off + ri.own, pv);
-        vload<T, W>(xk + off + ri.own, xv);
-        vload<T, W>(rk + off + ri.own, rv);
-        item_M<T, W>(ri, smi, n, ap);
+      if constexpr (CM) {
+        Nb<T> nr[W], ni[W];
+        T b[W], ap[2][W];
+        gather_item<T, W>(ri, tk, nr);
+        gather_item<T, W>(ri, tk + V, ni);
+        item_eps_pm<T, W>(g, ri, a.pm, b);
+        item_M_cm<T, W>(ri, smi, b, nr, ni, ap[0], ap[1]);
         double sr = 0.0;
 #pragma unroll
-        for (int e = 0; e < W; e++) {
-          xv[e] = xv[e] + alpha * pv[e];
-          rv[e] = rv[e] + malpha * ap[e];
-          sr += double(rv[e]) * double(rv[e]);
+        for (int c = 0; c < 2; c++) {
+          const size_t off = size_t(c) * V;
+          T pv[W], xv[W], rv[W];
+          vload<T, W>(pn + off + ri.own, pv);
+          vload<T, W>(xk + off + ri.own, xv);
+          vload<T, W>(rk + off + ri.own, rv);
+#pragma unroll
+          for (int e = 0; e < W; e++) {
+            xv[e] = xv[e] + alpha * pv[e];
+            rv[e] = rv[e] + malpha * ap[c][e];
+            sr += double(rv[e]) * double(rv[e]);
+          }
+          vstore<T, W>(xk + off + ri.own, xv);
+          vstore<T, W>(rk + off + ri.own, rv);
         }
         acc_add<NR>(acc, k, sr);
-        vstore<T, W>(xk + off + ri.own, xv);
-        vstore<T, W>(rk + off + ri.own, rv);
+      } else {
+#pragma unroll
+        for (int c = 0; c < NC; c++) {
+          const size_t off = size_t(c) * V;
+          Nb<T> n[W];
+          T ap[W], pv[W], xv[W], rv[W];
+          gather_item<T, W>(ri, tk + off, n);
+          vload<T, W>(pn + off + ri.own, pv);
+          vload<T, W>(xk + off + ri.own, xv);
+          vload<T, W>(rk + off + ri.own, rv);
+          item_M<T, W>(ri, smi, n, ap);
+          double sr = 0.0;
+#pragma unroll
+          for (int e = 0; e < W; e++) {
+            xv[e] = xv[e] + alpha * pv[e];
+            rv[e] = rv[e] + malpha * ap[e];
+            sr += double(rv[e]) * double(rv[e]);
+          }
+          acc_add<NR>(acc, k, sr);
+          vstore<T, W>(xk + off + ri.own, xv);
+          vstore<T, W>(rk + off + ri.own, rv);
+        }
       }
     });
     ok = end_phase<NR>(acc, sh, team, abort_req);
@@ -421,12 +529,12 @@ __device__ __forceinline__ void cg_solve(const CgArgs<T> &a, Team &team, SyncSha
 }
 
 // The single-lattice solve: the whole cooperative grid is the team.
-template <typename T, int NC, int NR, int BS, int W>
+template <typename T, int NC, int NR, int BS, int W, bool CM = false>
 __global__ void __launch_bounds__(BS, 1) cg_kernel(CgArgs<T> a) {
   __shared__ SyncShared sh;
   __shared__ CgShared cs;
   Team team = grid_team(a.bar, a.partials, a.err);
-  cg_solve<T, NC, NR, W>(a, team, sh, cs);
+  cg_solve<T, NC, NR, W, CM>(a, team, sh, cs);
 }
 
 }  // namespace gn

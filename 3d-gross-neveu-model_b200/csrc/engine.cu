@@ -14,7 +14,6 @@
 
 namespace gn {
 
-constexpr int kNumWorkVecs = 4;  // r, p0, p1, t per right-hand side
 
 void Engine::check(cudaError_t e, const char *what) {
   if (e != cudaSuccess) {
@@ -87,7 +86,7 @@ Engine::~Engine() {
   if (stream_) cudaStreamDestroy(stream_);
 }
 
-static int op_blocks(int64_t V, int num_sms) {
+int op_blocks(int64_t V, int num_sms) {
   int64_t b = (V + kOpThreads - 1) / kOpThreads;
   int64_t cap = int64_t(num_sms) * (2048 / kOpThreads);
   return int(b < cap ? b : cap);
@@ -294,7 +293,7 @@ int Engine::finish_solve(int nrhs, SolveInfo *info) {
 // ------------------------------------------------------------------ trajectory
 // kit->iterations / kit->CG_call bookkeeping of a flavour loop that stops at
 // the first failure (moleculardynamics.c:593-597).
-static void count_flavours(const SolveInfo *info, int n, double &iters, long long &calls, long long &inner,
+void count_flavours(const SolveInfo *info, int n, double &iters, long long &calls, long long &inner,
                            long long &rel) {
   for (int k = 0; k < n; k++) {
     if (info[k].status == kCgConverged) {
@@ -311,6 +310,7 @@ int Engine::trajectory(const gn_hmc_params &hp, double (*gauss)(void), double (*
                        const double *pre_chi, gn_traj_result *res) {
   if (hp.steps < 1) throw GnError(GN_ERR_ARG, "steps must be >= 1");
   if (hp.integrator < 0 || hp.integrator > 2) throw GnError(GN_ERR_ARG, "unknown integrator");
+  if (u1_) return trajectory_u1(hp, gauss, uniform, pre_P, pre_chi, res);
   const size_t V = size_t(V_);
   memset(res, 0, sizeof *res);
   struct ExactScope {  // parity mode for the trajectory's operators, restored on every exit

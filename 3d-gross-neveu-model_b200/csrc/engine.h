@@ -15,6 +15,8 @@
 
 namespace gn {
 
+constexpr int kNumWorkVecs = 4;  // FP64 solver vectors r, p0, p1, t per right-hand side
+
 struct DevBuf {
   void *p = nullptr;
   size_t bytes = 0;
@@ -91,6 +93,36 @@ class Engine {
   int condensate(const double *sm, double tol, double *target, double *D, double (*uniform)(void), double out[11],
                  double *iterations, long long *calls, int precision);
 
+  // ---- the U(1) model (PI_INTERACTION), u1.cu; its state is allocated on
+  // first use.  Complex fields are two planes (real, imaginary); a field of
+  // both flavours is four planes (flavour f: planes 2f, 2f + 1).
+  bool u1() const { return u1_; }
+  void set_u1(bool on);  // allocates and zeroes pi on first use
+  double *pi() { return pi_[pcur_]; }
+  double *pi_alt() { return pi_[pcur_ ^ 1]; }
+  void swap_pi() { pcur_ ^= 1; }
+  double *pm() { return pm_; }
+  double *Ppi() { return Ppi_; }
+  double *Fpi() { return Fpi_; }
+  double *chi_c() { return chi_c_; }
+  double *phi_c() { return phi_c_; }
+  double *X_c() { return X_c_; }
+  double *Y_c() { return Y_c_; }
+  // M, M^dagger or out - M psi with the complex mass on nsys complex systems
+  void dirac_cm(const double *sm, const double *pm, const double *in, double *out, int nsys, int op);
+  // CG on M M^dagger (FP64) for nrhs complex systems (b[k], x[k]: 2V each)
+  int solve_cm(const double *sm, const double *pm, const double *const *b, double *const *x, int nrhs, double tol,
+               int variant, int rel, long long max_iter, SolveInfo *info);
+  // fermion force of sigma (pi = false) or pi (pi = true) from complex X, Y
+  // (4V each), minus gcoef * field, with the fused step P += pcoef F if P
+  void force_cm(bool pi, const double *X, const double *Y, const double *field, double gcoef, double *F, double *P,
+                double pcoef);
+  // (sum P^2/2, sum_f 1/2 Re(conj phi_f X_f), sum field^2); synchronises
+  void energy_cm(const double *P, const double *phi, const double *X, const double *field, double out[3]);
+  // LeapFrog2Pi (moleculardynamics.c:1743-1870) on the resident sigma, pi
+  int trajectory_pi(const gn_hmc_params &hp, void (*gauss_pair)(double *, double *), double (*gauss)(void),
+                    double (*uniform)(void), gn_traj_result *res);
+
   // host staging (pinned), at least 4*V doubles
   double *host_stage() { return h_stage_; }
   int *abort_flag_host() { return h_abort_; }
@@ -111,6 +143,8 @@ class Engine {
                   int variant, int rel, long long max_iter, SolveInfo *info);
   void *alloc(size_t bytes);
   int cg_blocks(int ncomp, int nrhs, bool mixed, int w);
+  int trajectory_u1(const gn_hmc_params &hp, double (*gauss)(void), double (*uniform)(void), const double *pre_P,
+                    const double *pre_chi, gn_traj_result *res);
 
   int L_, device_;
   int64_t V_;
@@ -140,9 +174,20 @@ class Engine {
   double *h_stage_ = nullptr;
   int max_blocks_ = 0;
   int cg_blocks_cache_[2][2][kMaxRhs][3] = {};  // [mixed][ncomp-1][nrhs-1][log2 w]
+  // U(1) model
+  bool u1_ = false;
+  double *pi_[2] = {nullptr, nullptr};
+  int pcur_ = 0;
+  double *pm_ = nullptr, *Ppi_ = nullptr, *Fpi_ = nullptr;
+  double *chi_c_ = nullptr, *phi_c_ = nullptr, *X_c_ = nullptr, *Y_c_ = nullptr;
 };
 
 // Host-side compensated sum of (hi, lo) block partials.
 double sum_partials(const double *part, int nb, int q);
+// Blocks of the elementwise kernels.
+int op_blocks(int64_t V, int num_sms);
+// kit->iterations / kit->CG_call bookkeeping of a flavour loop that stops at
+// the first failure (moleculardynamics.c:593-597).
+void count_flavours(const SolveInfo *info, int n, double &iters, long long &calls, long long &inner, long long &rel);
 
 }  // namespace gn

@@ -238,6 +238,107 @@ static __global__ void __launch_bounds__(kOpThreads) cond_fill_kernel(Geom g, in
 }
 
 
+// ------------------------------------------------------------------ U(1) model
+// M, M^dagger or out - M psi with the complex mass sm + i eps pm (rowvec.cuh)
+// on complex fields of two planes each: system y = blockIdx.y uses planes 2y
+// (real) and 2y + 1 (imaginary).
+template <int W, int OP>
+__global__ void __launch_bounds__(kOpThreads) dirac_cm_kernel(Geom g, const double *__restrict__ sm,
+                                                             const double *__restrict__ pm,
+                                                             const double *__restrict__ in, double *__restrict__ out) {
+  const uint32_t V = uint32_t(g.V);
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= row_items<W>(g)) return;
+  const double *pr = in + size_t(2 * blockIdx.y) * V, *pi = pr + V;
+  double *orr = out + size_t(2 * blockIdx.y) * V, *oi = orr + V;
+  const RowItem it = make_item<W>(g, j);
+  Nb<double> nr[W], ni[W];
+  gather_item<double, W>(it, pr, nr);
+  gather_item<double, W>(it, pi, ni);
+  double smv[W], b[W], o_r[W], o_i[W];
+  vload<double, W>(sm + it.own, smv);
+  item_eps_pm<double, W>(g, it, pm, b);
+  if (OP == 0) {
+    item_M_cm<double, W>(it, smv, b, nr, ni, o_r, o_i);
+  } else if (OP == 1) {
+    item_Mt_cm<double, W>(it, smv, b, nr, ni, o_r, o_i);
+  } else {
+    vload<double, W>(orr + it.own, o_r);
+    vload<double, W>(oi + it.own, o_i);
+    item_sub_M_cm<double, W>(it, smv, b, nr, ni, o_r, o_i);
+  }
+  vstore<double, W>(orr + it.own, o_r);
+  vstore<double, W>(oi + it.own, o_i);
+}
+
+// The fermion forces of the U(1) model on complex X_f, Y_f (flavour f: planes
+// 2f, 2f + 1), over the corners of force_site in its order, flavour 0 first:
+//   sigma: F += 1/8 Re(conj X Y)           (moleculardynamics.c:590-622)
+//   pi:    F += 1/8 Re(i eps conj X Y)     (moleculardynamics.c:695-733)
+// then F -= gcoef field (the quadratic terms, :576-581 / :681-686), and the
+// momentum step P += pcoef F when P is given.  C forms Re(conj X Y) as
+// Xr Yr - (-Xi) Yi and Re(i eps conj X Y) as (eps Xi) Yr - (eps Xr) Yi.
+template <bool PI>
+__global__ void __launch_bounds__(kOpThreads) force_cm_kernel(Geom g, const double *__restrict__ X,
+                                                             const double *__restrict__ Y,
+                                                             const double *__restrict__ field, double gcoef,
+                                                             double *__restrict__ F, double *P, double pcoef) {
+  const uint32_t V = uint32_t(g.V);
+  const int off[8][3] = {{0, 0, 0}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 1, 1}};
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x) {
+    uint32_t x0, x1, x2, par, row, k;
+    site_coords(g, i, x0, x1, x2, par, row, k);
+    uint32_t cj[8];
+#pragma unroll
+    for (int c = 0; c < 8; c++) cj[c] = site_index(g, int(x0) + off[c][0], int(x1) + off[c][1], int(x2) + off[c][2]);
+    double f = 0.0;
+#pragma unroll
+    for (int fl = 0; fl < 2; fl++) {
+      const double *Xr = X + size_t(2 * fl) * V, *Xi = Xr + V;
+      const double *Yr = Y + size_t(2 * fl) * V, *Yi = Yr + V;
+#pragma unroll
+      for (int c = 0; c < 8; c++) {
+        const uint32_t j = cj[c];
+        const double xr = __ldg(Xr + j), xi = __ldg(Xi + j), yr = __ldg(Yr + j), yi = __ldg(Yi + j);
+        double t;
+        if constexpr (PI) {
+          const double e = j >= uint32_t(g.half) ? -1.0 : 1.0;
+          t = (e * xi) * yr - (e * xr) * yi;
+        } else {
+          t = xr * yr - (-xi) * yi;
+        }
+        f = f + 0.125 * t;
+      }
+    }
+    f = f - gcoef * __ldg(field + i);
+    F[i] = f;
+    if (P != nullptr) P[i] = P[i] + f * pcoef;
+  }
+}
+
+// Energy terms with complex phi_f, X_f (planes 2f, 2f + 1):
+//   q0 = sum P^2 / 2, q1 = sum_f sum 1/2 Re(conj phi_f X_f), q2 = sum field^2
+// (ComputeFullEnergyForSigma / ForPi, moleculardynamics.c:299-319, :349-369).
+static __global__ void __launch_bounds__(kOpThreads) energy_cm_kernel(uint32_t V, const double *__restrict__ P,
+                                                              const double *__restrict__ phi,
+                                                              const double *__restrict__ X,
+                                                              const double *__restrict__ field, double *part) {
+  double hi[3] = {0, 0, 0}, lo[3] = {0, 0, 0};
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x) {
+    const double p = P[i];
+    neumaier(hi[0], lo[0], p * p / 2.0);
+#pragma unroll
+    for (int fl = 0; fl < 2; fl++) {
+      const double pr = phi[size_t(2 * fl) * V + i], pim = phi[size_t(2 * fl + 1) * V + i];
+      const double xr = X[size_t(2 * fl) * V + i], xi = X[size_t(2 * fl + 1) * V + i];
+      neumaier(hi[1], lo[1], 0.5 * (pr * xr - (-pim) * xi));
+    }
+    const double s = field[i];
+    neumaier(hi[2], lo[2], s * s);
+  }
+  publish_compensated<3>(hi, lo, part);
+}
+
 // ------------------------------------------------------------------ sigma observables
 // CondensateSigmaPi (observables.c:323-369, the Z2 model): with t = sigma(x) / V,
 //   s0 = sum_x t,   s1+2d + i s2+2d = sum_x exp(i P_MIN x_d) t   (d = 0, 1, 2),

@@ -219,4 +219,88 @@ __device__ __forceinline__ void item_sub_M(const RowItem &it, const T (&sm)[W], 
   }
 }
 
+// ------------------------------------------------------------------ U(1) model
+// The complex mass of the U(1) Gross-Neveu model (PI_INTERACTION): the
+// diagonal of M is sm + i eps(x) pm (dirac.c:65-69), of M^dagger sm - i eps pm
+// (dirac.c:106-109), with eps = +1 on even and -1 on odd sites (the item's
+// parity) and pm the pi field's mass.  A complex field is two planes (real,
+// imaginary).  The mass product is formed as C forms (a + ib)(c + id):
+// (ac - bd) + i(ad + bc); the hopping terms are added to each plane in the
+// order of the real stencils.  b = eps pm is exact (eps = +-1).
+template <typename T, int W>
+__device__ __forceinline__ void item_eps_pm(const Geom &g, const RowItem &it, const T *pm, T (&b)[W]) {
+  vload<T, W>(pm + it.own, b);
+  if (it.own >= uint32_t(g.half)) {
+#pragma unroll
+    for (int e = 0; e < W; e++) b[e] = -b[e];
+  }
+}
+
+template <typename T, int W>
+__device__ __forceinline__ void item_M_cm(const RowItem &it, const T (&sm)[W], const T (&b)[W],
+                                          const Nb<T> (&nr)[W], const Nb<T> (&ni)[W], T (&out_r)[W],
+                                          T (&out_i)[W]) {
+#pragma unroll
+  for (int e = 0; e < W; e++) {
+    const uint32_t neg = item_neg<W>(it, e);
+    T tr = sm[e] * nr[e].c - b[e] * ni[e].c;
+    T ti = sm[e] * ni[e].c + b[e] * nr[e].c;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      tr = hop_add(tr, nr[e].up[d], neg, d);
+      tr = hop_sub(tr, nr[e].dn[d], neg, 3 + d);
+      ti = hop_add(ti, ni[e].up[d], neg, d);
+      ti = hop_sub(ti, ni[e].dn[d], neg, 3 + d);
+    }
+    out_r[e] = tr;
+    out_i[e] = ti;
+  }
+}
+
+// M^dagger: the mass sm - i b, formed as (sm c - (-b) d) + i(sm d + (-b) c)
+template <typename T, int W>
+__device__ __forceinline__ void item_Mt_cm(const RowItem &it, const T (&sm)[W], const T (&b)[W],
+                                           const Nb<T> (&nr)[W], const Nb<T> (&ni)[W], T (&out_r)[W],
+                                           T (&out_i)[W]) {
+#pragma unroll
+  for (int e = 0; e < W; e++) {
+    const uint32_t neg = item_neg<W>(it, e);
+    const T mb = -b[e];
+    T tr = sm[e] * nr[e].c - mb * ni[e].c;
+    T ti = sm[e] * ni[e].c + mb * nr[e].c;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      tr = hop_sub(tr, nr[e].up[d], neg, d);
+      tr = hop_add(tr, nr[e].dn[d], neg, 3 + d);
+      ti = hop_sub(ti, ni[e].up[d], neg, d);
+      ti = hop_add(ti, ni[e].dn[d], neg, 3 + d);
+    }
+    out_r[e] = tr;
+    out_i[e] = ti;
+  }
+}
+
+// out <- out - M psi (SubtractDiracFermion with the complex mass, dirac.c:213-247:
+// the mass product first, then the hopping terms)
+template <typename T, int W>
+__device__ __forceinline__ void item_sub_M_cm(const RowItem &it, const T (&sm)[W], const T (&b)[W],
+                                              const Nb<T> (&nr)[W], const Nb<T> (&ni)[W], T (&out_r)[W],
+                                              T (&out_i)[W]) {
+#pragma unroll
+  for (int e = 0; e < W; e++) {
+    const uint32_t neg = item_neg<W>(it, e);
+    T tr = out_r[e] - (sm[e] * nr[e].c - b[e] * ni[e].c);
+    T ti = out_i[e] - (sm[e] * ni[e].c + b[e] * nr[e].c);
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      tr = hop_sub(tr, nr[e].up[d], neg, d);
+      tr = hop_add(tr, nr[e].dn[d], neg, 3 + d);
+      ti = hop_sub(ti, ni[e].up[d], neg, d);
+      ti = hop_add(ti, ni[e].dn[d], neg, 3 + d);
+    }
+    out_r[e] = tr;
+    out_i[e] = ti;
+  }
+}
+
 }  // namespace gn

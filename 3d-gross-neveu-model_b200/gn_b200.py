@@ -33,6 +33,7 @@ STATUS_NAMES = {0: "GN_OK", 1: "GN_NOT_CONVERGED", -1: "GN_ERR_ARG", -2: "GN_ERR
 SIGMA_OBSERVABLES = ("condensate_sigma", "condensate_sigma_abs", "mu2", "mu4", "chi", "chip", "chip_pbc1",
                      "chip_pbc2")
 DRAW_FN = C.CFUNCTYPE(C.c_double)
+PAIR_FN = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.POINTER(C.c_double))
 
 
 class GnError(RuntimeError):
@@ -195,6 +196,18 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
         "gn_ensemble_checkpoint_load": ([v, C.c_int, C.c_char_p, C.c_char_p, C.POINTER(HmcCounters)], C.c_int),
         "gn_format_measure_line": ([C.c_char_p, C.c_size_t, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                     C.c_double, C.c_double, _dp, _dp], C.c_int),
+        "gn_load_pi": ([v, _dp], C.c_int),
+        "gn_store_pi": ([v, _dp, _dp], C.c_int),
+        "gn_set_u1": ([v, C.c_int], C.c_int),
+        "gn_dirac_u1": ([v, _dp, _dp, _dp, _dp, C.c_int, C.c_int], C.c_int),
+        "gn_cg_u1": ([v, _dp, _dp, _dp, _dp, C.c_int, C.c_double, C.c_int, C.c_int, C.c_longlong, C.POINTER(CgInfo)],
+                     C.c_int),
+        "gn_sigma_force_u1": ([v, C.c_double, _dp, _dp, _dp, _dp, _dp, _dp, C.c_double, _dp, C.POINTER(CgInfo)],
+                              C.c_int),
+        "gn_pi_force": ([v, C.c_double, _dp, _dp, _dp, _dp, _dp, _dp, C.c_double, _dp, C.POINTER(CgInfo)], C.c_int),
+        "gn_energy_u1": ([v, C.c_int, C.c_double, _dp, _dp, _dp, _dp, _dp], C.c_int),
+        "gn_trajectory_pi": ([v, C.POINTER(HmcParams), C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(TrajResult)],
+                             C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -480,6 +493,95 @@ class Lattice:
 
     def flush_l2(self):
         self._check(self.lib.gn_flush_l2(self.ctx))
+
+    # ---- the U(1) model (complex fields as numpy complex128, shape (nsys, V))
+    @staticmethod
+    def _cplanes(a):
+        a = np.asarray(a, np.complex128)
+        a = a[None] if a.ndim == 1 else a
+        return np.ascontiguousarray(np.concatenate([np.concatenate([r.real, r.imag]) for r in a])), a.shape[0]
+
+    def _uncplanes(self, p, n):
+        p = p.reshape(n, 2, self.V)
+        return p[:, 0] + 1j * p[:, 1]
+
+    def load_pi(self, pi):
+        """The resident pi (and pimass); the context switches to the U(1) model."""
+        self._check(self.lib.gn_load_pi(self.ctx, _p(np.ascontiguousarray(pi, np.float64))))
+
+    def store_pi(self):
+        pi, pm = np.empty(self.V), np.empty(self.V)
+        self._check(self.lib.gn_store_pi(self.ctx, _p(pi), _p(pm)))
+        return pi, pm
+
+    def set_u1(self, on=True):
+        self._check(self.lib.gn_set_u1(self.ctx, int(on)))
+
+    def dirac_u1(self, sm, pm, psi, op=GN_OP_M, out=None):
+        """M, M^dagger or out - M psi with the complex mass; psi complex (V,) or (nsys, V)."""
+        single = np.asarray(psi).ndim == 1
+        inp, n = self._cplanes(psi)
+        o = self._cplanes(out)[0].copy() if op == GN_OP_SUB_M else np.zeros_like(inp)
+        self._check(self.lib.gn_dirac_u1(self.ctx, _p(np.ascontiguousarray(sm, np.float64)),
+                                         _p(np.ascontiguousarray(pm, np.float64)), _p(inp), _p(o), n, op))
+        r = self._uncplanes(o, n)
+        return r[0] if single else r
+
+    def cg_u1(self, sm, pm, b, x0=None, tol=1e-9, variant=0, relative=False, max_iter=0):
+        single = np.asarray(b).ndim == 1
+        bp, n = self._cplanes(b)
+        xp = np.zeros_like(bp) if x0 is None else self._cplanes(x0)[0].copy()
+        infos = (CgInfo * n)()
+        st = self._check(self.lib.gn_cg_u1(self.ctx, _p(np.ascontiguousarray(sm, np.float64)),
+                                           _p(np.ascontiguousarray(pm, np.float64)), _p(bp), _p(xp), n, tol,
+                                           variant, int(relative), max_iter, infos),
+                         allow=(GN_OK, GN_NOT_CONVERGED))
+        x = self._uncplanes(xp, n)
+        return (x[0] if single else x), [i.as_dict() for i in infos], st
+
+    def _force_u1(self, fn, beta_s, fld, sm, pm, phi, X, tol):
+        php, _ = self._cplanes(phi)
+        Xp = self._cplanes(X)[0].copy()
+        Y = np.zeros(4 * self.V)
+        F = np.zeros(self.V)
+        infos = (CgInfo * 2)()
+        st = self._check(fn(self.ctx, beta_s, _p(np.ascontiguousarray(fld, np.float64)),
+                            _p(np.ascontiguousarray(sm, np.float64)), _p(np.ascontiguousarray(pm, np.float64)),
+                            _p(php), _p(Xp), _p(Y), tol, _p(F), infos), allow=(GN_OK, GN_NOT_CONVERGED))
+        return F, self._uncplanes(Xp, 2), self._uncplanes(Y, 2), [i.as_dict() for i in infos], st
+
+    def sigma_force_u1(self, beta_s, sigma, sm, pm, phi, X, tol):
+        """ComputeSigmaForce in the U(1) model: (F, X, Y, infos, status); phi, X complex (2, V)."""
+        return self._force_u1(self.lib.gn_sigma_force_u1, beta_s, sigma, sm, pm, phi, X, tol)
+
+    def pi_force(self, beta_s, pi, sm, pm, phi, X, tol):
+        """ComputePiForce: (F, X, Y, infos, status); phi, X complex (2, V)."""
+        return self._force_u1(self.lib.gn_pi_force, beta_s, pi, sm, pm, phi, X, tol)
+
+    def energy_u1(self, which, beta_s, field, P, phi, X):
+        """which 0: ComputeFullEnergyForSigma, 1: ComputeFullEnergyForPi (phi, X complex (2, V))."""
+        H = C.c_double()
+        self._check(self.lib.gn_energy_u1(self.ctx, which, beta_s, _p(np.ascontiguousarray(field, np.float64)),
+                                          _p(np.ascontiguousarray(P, np.float64)), _p(self._cplanes(phi)[0]),
+                                          _p(self._cplanes(X)[0]), C.byref(H)))
+        return H.value
+
+    def trajectory_pi(self, beta_s, eps, steps, gauss_pair=None, gauss=None, uniform=None, tol_high=1e-9,
+                      relative=False):
+        """LeapFrog2Pi on the resident sigma and pi.  gauss_pair(a, b) fills two
+        N(0, 1) values (the reference's Gauss2MeanVariance(a, b, 0, 1)): an int
+        address, a PAIR_FN or a Python callable taking two POINTER(c_double)."""
+        hp = HmcParams(beta_s, eps, steps, 0, tol_high, tol_high, int(relative), GN_PREC_FP64)
+        res = TrajResult()
+        if gauss_pair is not None and not isinstance(gauss_pair, (int, C._CFuncPtr)):
+            gauss_pair = PAIR_FN(gauss_pair)
+        keep = gauss_pair  # the callback must outlive the call
+        pair = None if gauss_pair is None else (gauss_pair if isinstance(gauss_pair, int)
+                                                else C.cast(gauss_pair, C.c_void_p).value)
+        self._check(self.lib.gn_trajectory_pi(self.ctx, C.byref(hp), pair, fn_address(gauss), fn_address(uniform),
+                                              C.byref(res)), allow=(GN_OK, GN_NOT_CONVERGED))
+        del keep
+        return res.as_dict()
 
     # ---- observables and checkpoints
     def condensate_sigma(self, sigma=None):

@@ -172,6 +172,58 @@ GN_API int gn_condensate_sigma(gn_context *ctx, const double *sigma, double *out
 /* The same for a device sigma (V doubles). */
 GN_API int gn_condensate_sigma_device(gn_context *ctx, const double *sigma, double *out);
 
+/* ---- the U(1) model (the reference's PI_INTERACTION) --------------------
+ * M = D + sigmamass + i eps(x) pimass (dirac.c:65-69; eps = +1 on even, -1 on
+ * odd sites), M^dagger = -D + sigmamass - i eps pimass.  Fermion fields are
+ * complex: two planes (real, imaginary) per system; a field of both flavours
+ * is four planes (flavour f: planes 2f, 2f + 1).  FP64 only.
+ *
+ * gn_load_pi sets the resident pi (V doubles, fermion order; pimass =
+ * ComputeFullPiMass, pi.c:44-60) and switches the context to the U(1) model:
+ * gn_trajectory then runs the sigma integrators with this M on complex
+ * fields.  gn_set_u1(ctx, 0) switches back to the Z2 model (real fields). */
+GN_API int gn_load_pi(gn_context *ctx, const double *pi);
+GN_API int gn_store_pi(gn_context *ctx, double *pi, double *pimass);
+GN_API int gn_set_u1(gn_context *ctx, int on);
+
+/* gn_dirac with the complex mass: in/out hold nsys complex systems (2 nsys V). */
+GN_API int gn_dirac_u1(gn_context *ctx, const double *sigmamass, const double *pimass, const double *in, double *out,
+                       int nsys, int op);
+/* CG on M M^dagger for nrhs (1 or 2) complex systems (b, x: 2 nrhs V; x in/out),
+ * variant / relative / max_iter as gn_cg; FP64.  info[nrhs] may be NULL. */
+GN_API int gn_cg_u1(gn_context *ctx, const double *sigmamass, const double *pimass, const double *b, double *x,
+                    int nrhs, double tol, int variant, int relative, long long max_iter, gn_cg_info *info);
+/* ComputeSigmaForce (moleculardynamics.c:631-647) and ComputePiForce
+ * (:736-752) in the U(1) model: X_f = (M M^dagger)^-1 phi_f by variant-0 CG
+ * from the incoming X_f (tolerance tol), Y_f = M^dagger X_f, then
+ *   sigma: F = sum_f 1/8 sum_corners Re(conj X_f Y_f) - (N_f beta_s / 2) sigma
+ *   pi:    F = sum_f 1/8 sum_corners Re(i eps conj X_f Y_f) - (N_f beta_s / 4) pi
+ * phi, X, Y: 4V (X in/out); field = sigma or pi (V); force out (V). */
+GN_API int gn_sigma_force_u1(gn_context *ctx, double beta_s, const double *sigma, const double *sigmamass,
+                             const double *pimass, const double *phi, double *X, double *Y, double tol, double *force,
+                             gn_cg_info *info);
+GN_API int gn_pi_force(gn_context *ctx, double beta_s, const double *pi, const double *sigmamass,
+                       const double *pimass, const double *phi, double *X, double *Y, double tol, double *force,
+                       gn_cg_info *info);
+/* ComputeFullEnergyForSigma (which = 0, moleculardynamics.c:299-319) or
+ * ComputeFullEnergyForPi (which = 1, :349-369) with complex phi, X (4V):
+ *   H = 1/2 sum P^2 + 1/2 sum_f Re(conj phi_f X_f) + c beta_s-term,
+ * c = N_f beta_s / 4 times sum sigma^2, or N_f beta_s / 8 times sum pi^2. */
+GN_API int gn_energy_u1(gn_context *ctx, int which, double beta_s, const double *field, const double *P,
+                        const double *phi, const double *X, double *H);
+/* LeapFrog2Pi (moleculardynamics.c:1743-1870) on the resident sigma and pi.
+ * Draws as the reference: the pi momenta in pairs, gauss_pair(&P[x],
+ * &P[x + V/2]) for x < V/2 (DrawPiMomentaFromGaussianDistribution calls
+ * Gauss2MeanVariance(.., 0, 1), random.c:129), then chi_0, chi_1 from gauss()
+ * (Gauss1); phi_f = M chi_f; every inversion a variant-0 CG at
+ * params->tol_high; the Metropolis test with uniform().  pi is restored on
+ * reject or on a failed solve (res->ok = 0).  params->eps and ->steps are the
+ * pi step (epsilon_pi_HMC, steps_pi_HMC); integrator and tol_medium are not
+ * used; precision GN_PREC_FP64.  gauss_pair and gauss NULL: P_pi (GN_F_PI_P)
+ * and the real parts of GN_F_CHI_C as they are. */
+GN_API int gn_trajectory_pi(gn_context *ctx, const gn_hmc_params *params, void (*gauss_pair)(double *, double *),
+                            double (*gauss)(void), double (*uniform)(void), gn_traj_result *res);
+
 /* ---- checkpoints: the reference's lattice file ------------------------- */
 
 /* The HMC bookkeeping the file carries (simulation.c:162-178, struct Info
@@ -255,8 +307,11 @@ GN_API int gn_trajectory(gn_context *ctx, const gn_hmc_params *params, double (*
 GN_API void *gn_stream(gn_context *ctx);
 
 /* Device pointer of a resident field: GN_F_* above, or GN_F_SIGMA / GN_F_SM
- * (the current sigma and sigmamass, V doubles each). */
-enum { GN_F_SIGMA = 6, GN_F_SM = 7 };
+ * (the current sigma and sigmamass, V doubles each).  U(1) model: GN_F_PI /
+ * GN_F_PM (pi, pimass), and for gn_read_state / gn_write_state too the pi
+ * momenta and force (V) and the complex chi, phi, X, Y of both flavours (4V). */
+enum { GN_F_SIGMA = 6, GN_F_SM = 7, GN_F_PI_P = 8, GN_F_PI_F = 9, GN_F_CHI_C = 10, GN_F_PHI_C = 11, GN_F_X_C = 12,
+       GN_F_Y_C = 13, GN_F_PI = 14, GN_F_PM = 15 };
 GN_API double *gn_field_ptr(gn_context *ctx, int field);
 
 /* gn_dirac on device pointers; asynchronous on gn_stream(ctx). */

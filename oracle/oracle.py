@@ -249,6 +249,13 @@ class Ref:
         lib.gnref_write_lattice.argtypes = [C.c_char_p, C.c_char_p, _dp, _ip]
         lib.gnref_read_lattice.argtypes = [C.c_char_p, C.c_char_p, _dp, _ip]
         lib.gnref_read_lattice.restype = C.c_double
+        for name in ("gnref_set_pi", "gnref_get_pi", "gnref_get_pimass", "gnref_set_pi_momenta",
+                     "gnref_get_pi_momenta", "gnref_get_pi_force"):
+            getattr(lib, name).argtypes = [_dp]
+        lib.gnref_set_pi_params.argtypes = [C.c_double, C.c_int]
+        lib.gnref_energy_pi.restype = C.c_double
+        lib.gnref_trajectory_pi.argtypes = [C.c_char_p, _ip]
+        lib.gnref_gauss2.argtypes = [_dp, _dp]
 
     def init(self, seed=1231, beta_s=0.85, eps=0.2, steps=2):
         self.lib.gnref_init(seed, beta_s, eps, steps)
@@ -378,3 +385,56 @@ class Ref:
         counters = {"epsilon_link": float(eps[0]), "epsilon_pi": float(eps[1])}
         counters.update({k: int(ints[i]) for i, k in enumerate(self.COUNTER_INTS)})
         return self.sigma(), counters, check
+
+    # ---- the U(1) model (a build with extra_defs=("-DPI_INTERACTION",)) ----
+    def _getv(self, name):
+        v = np.empty(self.V)
+        getattr(self.lib, name)(_p(v))
+        return v
+
+    def gauss2(self, npairs):
+        """npairs Gauss2MeanVariance(.., 0, 1) pairs, as the pi momenta draw them: (npairs, 2)."""
+        out = np.empty((npairs, 2))
+        a, b = C.c_double(), C.c_double()
+        for i in range(npairs):
+            self.lib.gnref_gauss2(C.byref(a), C.byref(b))
+            out[i] = (a.value, b.value)
+        return out
+
+    def set_pi(self, pi):
+        self.lib.gnref_set_pi(_p(np.ascontiguousarray(pi, np.float64)))
+
+    def pi(self):
+        return self._getv("gnref_get_pi")
+
+    def pimass(self):
+        return self._getv("gnref_get_pimass")
+
+    def set_pi_momenta(self, P):
+        self.lib.gnref_set_pi_momenta(_p(np.ascontiguousarray(P, np.float64)))
+
+    def pi_momenta(self):
+        return self._getv("gnref_get_pi_momenta")
+
+    def pi_force_buf(self):
+        return self._getv("gnref_get_pi_force")
+
+    def set_pi_params(self, eps, steps):
+        self.lib.gnref_set_pi_params(eps, steps)
+
+    def pi_force(self):
+        return bool(self.lib.gnref_pi_force())
+
+    def energy_pi(self):
+        return self.lib.gnref_energy_pi()
+
+    def trajectory_pi(self, accfile: str):
+        """LeapFrog2Pi; returns (ok, accepted, dH parsed from the acceptance line)."""
+        acc = C.c_int(0)
+        ok = self.lib.gnref_trajectory_pi(accfile.encode(), C.byref(acc))
+        dH = None
+        if ok:
+            with open(accfile) as fh:
+                last = fh.read().strip().splitlines()[-1]
+            dH = float(last.split("\t")[11])
+        return bool(ok), bool(acc.value), dH

@@ -397,3 +397,63 @@ double gnref_read_lattice(const char *path, const char *copy, double *eps, int *
     ints[9] = sim.info.measure;
     return TestWriteReadLattice(&sim);
 }
+
+/* ---- the U(1) model (meaningful in a build with -DPI_INTERACTION) ---------- */
+static struct Forcepi g_force_pi;
+static struct Momentapi g_mom_pi;
+static int g_pi_ready = 0;
+
+static void pi_ready(void)
+{
+    if (!g_pi_ready) {
+        AllocateForcePi(&g_force_pi);
+        AllocateMomentaPi(&g_mom_pi);
+        g_pi_ready = 1;
+    }
+}
+
+/* one Gauss2MeanVariance(.., 0, 1) pair (random.c:129), as the pi momenta draw it */
+void gnref_gauss2(double *a, double *b) { Gauss2MeanVariance(a, b, 0.0, 1.0); }
+
+/* pi and its mass (ComputeFullPiMass, pi.c:44) */
+void gnref_set_pi(const double *pi)
+{
+    memcpy(g_lat.pi, pi, sizeof(double) * VOLUME);
+    ComputeFullPiMass(&g_lat, &g_fcor, g_lat.pimass);
+}
+void gnref_get_pi(double *pi) { memcpy(pi, g_lat.pi, sizeof(double) * VOLUME); }
+void gnref_get_pimass(double *pm) { memcpy(pm, g_lat.pimass, sizeof(double) * VOLUME); }
+void gnref_set_pi_momenta(const double *p) { pi_ready(); memcpy(g_mom_pi.momenta, p, sizeof(double) * VOLUME); }
+void gnref_get_pi_momenta(double *p) { pi_ready(); memcpy(p, g_mom_pi.momenta, sizeof(double) * VOLUME); }
+void gnref_get_pi_force(double *f) { pi_ready(); memcpy(f, g_force_pi.force, sizeof(double) * VOLUME); }
+void gnref_set_pi_params(double eps, int steps)
+{
+    g_info.epsilon_pi_HMC = eps;
+    g_info.steps_pi_HMC = steps;
+    g_info.distance_pi_HMC = eps * steps;
+}
+
+/* ComputePiForce (moleculardynamics.c:736) into the harness force buffer */
+int gnref_pi_force(void)
+{
+    pi_ready();
+    return ComputePiForce(&g_lat, &g_info, &g_fcor, &g_force_pi, &g_kit) ? 1 : 0;
+}
+
+/* ComputeFullEnergyForPi (moleculardynamics.c:349) */
+double gnref_energy_pi(void)
+{
+    pi_ready();
+    return ComputeFullEnergyForPi(&g_lat, &g_info, &g_fcor, &g_mom_pi, &g_kit);
+}
+
+/* LeapFrog2Pi (moleculardynamics.c:1743) with the epsilon / steps of gnref_set_pi_params */
+int gnref_trajectory_pi(const char *accfile, int *accepted)
+{
+    pi_ready();
+    int before = g_info.hybrid_accepted_pi;
+    bool ok = LeapFrog2Pi(&g_lat, &g_info, &g_force_pi, &g_mom_pi, &g_fcor, &g_kit, g_info.epsilon_pi_HMC,
+                          g_info.steps_pi_HMC, accfile);
+    *accepted = g_info.hybrid_accepted_pi - before;
+    return ok ? 1 : 0;
+}
