@@ -25,6 +25,9 @@ GN_OP_M, GN_OP_MT, GN_OP_SUB_M = 0, 1, 2
 GN_PREC_FP64, GN_PREC_MIXED, GN_PREC_FP64_EXACT = 0, 1, 2
 GN_LFMN2VF, GN_LF2, GN_LFMN2 = 0, 1, 2
 GN_F_P, GN_F_F, GN_F_CHI, GN_F_PHI, GN_F_X, GN_F_Y, GN_F_SIGMA, GN_F_SM = range(8)
+# the U(1) model's resident fields: pi momenta and force (V), complex chi, phi,
+# X, Y of both flavours (4V), and for field_ptr pi and pimass
+GN_F_PI_P, GN_F_PI_F, GN_F_CHI_C, GN_F_PHI_C, GN_F_X_C, GN_F_Y_C, GN_F_PI, GN_F_PM = range(8, 16)
 GN_ERR_IO, GN_ERR_NOT_FOUND, GN_ERR_FORMAT = -6, -7, -8
 STATUS_NAMES = {0: "GN_OK", 1: "GN_NOT_CONVERGED", -1: "GN_ERR_ARG", -2: "GN_ERR_CUDA", -3: "GN_ERR_TIMEOUT",
                 -4: "GN_ERR_ABORTED", -5: "GN_ERR_NO_DEVICE", -6: "GN_ERR_IO", -7: "GN_ERR_NOT_FOUND",
@@ -434,10 +437,15 @@ class Lattice:
         return s, sm
 
     def read_state(self, field):
-        n = self.V if field in (GN_F_P, GN_F_F) else 2 * self.V
+        if field in (GN_F_P, GN_F_F, GN_F_PI_P, GN_F_PI_F):
+            n = self.V
+        elif field in (GN_F_CHI_C, GN_F_PHI_C, GN_F_X_C, GN_F_Y_C):
+            n = 4 * self.V
+        else:
+            n = 2 * self.V
         a = np.empty(n)
         self._check(self.lib.gn_read_state(self.ctx, field, _p(a)))
-        return a if n == self.V else a.reshape(2, self.V)
+        return a if n == self.V else a.reshape(n // self.V, self.V)
 
     def write_state(self, field, a):
         self._check(self.lib.gn_write_state(self.ctx, field, _p(np.ascontiguousarray(a, np.float64).reshape(-1))))

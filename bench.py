@@ -66,7 +66,8 @@ def parse():
     ap.add_argument("--eps", type=float, default=0.05)
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--case", choices=["cg64", "dirac128", "dirac256", "traj64", "cgscan", "batched", "serve", "l128"], default=None,
+    ap.add_argument("--case", choices=["cg64", "dirac128", "dirac256", "traj64", "cgscan", "batched", "serve", "l128",
+                                       "u1"], default=None,
                     help="run one small case for a profiler instead of the benchmark")
     return ap.parse_args()
 
@@ -360,6 +361,7 @@ def run_ours(a, world, rank, local):
                            if k in ("value", "ms_per_ensemble_trajectory", "cg_iterations_per_chain_trajectory",
                                     "solver_gbs")}
     l128 = l128_case(G, dev) if world == 1 else None
+    u1 = u1_case(G, dev) if world == 1 else None
     serving = None
     if world == 1:
         serving = serve_bench(G)
@@ -399,7 +401,8 @@ def run_ours(a, world, rank, local):
             "gpu_launches": int(round(mixed["launches"] * a.steps)),
             "batched": batched,
             "serving": serving,
-            "mixed_precision_L128": l128}
+            "mixed_precision_L128": l128,
+            "u1_model_L64": u1}
     if rank == 0:
         print(json.dumps(line), flush=True)
     lat.close()
@@ -560,6 +563,64 @@ def serve_bench(G, nreq=600, rate=200.0, warm=24, seed=5, precision=None):
     return out
 
 
+def u1_case(G, dev, L=64, md_steps=10, eps=0.05, pi_steps=10, tol=1e-10, reps=2):
+    """The U(1) model (PI_INTERACTION) in FP64 at L = 64: ms per sigma trajectory
+    (LFMN2VF md_steps x eps with the complex M, every solve to a true relative
+    residual of tol) and per LeapFrog2Pi (pi_steps x eps), against the Z2
+    model's FP64 trajectory on the same sigma and draws.  Draws resident on
+    the device (gn_trajectory_device; P_pi and chi written before the pi
+    trajectory), CUDA events around each trajectory, `reps` after one warm-up."""
+    import torch
+    V = L ** 3
+    rng = np.random.default_rng(64)
+    sigma = rng.normal(0.0, np.sqrt(2.0 / (NFLAV * BETA_S)), V)
+    pi = rng.normal(0.0, np.sqrt(2.0 / (NFLAV * BETA_S)), V)
+    draws = torch.tensor(rng.normal(size=3 * V), dtype=torch.float64, device=dev)
+    chi_c = np.zeros(4 * V)
+    chi_c[0:V], chi_c[2 * V:3 * V] = rng.normal(size=V), rng.normal(size=V)
+    ppi = rng.normal(size=V)
+    out = {"L": L, "precision": "fp64"}
+    lat = G.Lattice(L, dev.index)
+    stream = torch.cuda.ExternalStream(lat.stream, device=dev)
+
+    def timed(run):
+        ts, res = [], None
+        for rep in range(reps + 1):
+            e0, e1 = cuda_events()
+            e0.record(stream)
+            res = run()
+            e1.record(stream)
+            e1.synchronize()
+            if rep > 0:
+                ts.append(e0.elapsed_time(e1))
+        return min(ts), res
+
+    params = dict(tol_medium=tol, tol_high=tol, relative=True)
+    for name, u1 in (("z2_sigma_trajectory", False), ("u1_sigma_trajectory", True)):
+        def run():
+            lat.load_sigma(sigma)
+            if u1:
+                lat.load_pi(pi)
+            else:
+                lat.set_u1(False)
+            base = draws.data_ptr()
+            return lat.trajectory_device(base, base + 8 * V, BETA_S, eps, md_steps, None, precision=G.GN_PREC_FP64,
+                                         **params)
+        ms, r = timed(run)
+        out[name] = {"ms": round(ms, 2), "cg_iterations": r["cg_iterations"], "dH": r["dH"]}
+
+    def run_pi():
+        lat.load_sigma(sigma)
+        lat.load_pi(pi)
+        lat.write_state(G.GN_F_PI_P, ppi)
+        lat.write_state(G.GN_F_CHI_C, chi_c)
+        return lat.trajectory_pi(BETA_S, eps, pi_steps, None, None, None, tol_high=tol, relative=True)
+    ms, r = timed(run_pi)
+    out["u1_pi_trajectory"] = {"ms": round(ms, 2), "cg_iterations": r["cg_iterations"], "dH": r["dH"]}
+    lat.close()
+    return out
+
+
 def l128_case(G, dev, betas=(0.7, 0.85, 1.0), L=128, md_steps=10, eps=0.05, tol=1e-10, reliable=50):
     """Mixed precision at L = 128 (V = 2,097,152): FP32 fields and inner CG,
     FP64 reliable updates at least every `reliable` iterations, FP64 dH and
@@ -674,6 +735,9 @@ def run_case(a):
         return
     if a.case == "l128":
         print(json.dumps(l128_case(G, dev)))
+        return
+    if a.case == "u1":
+        print(json.dumps(u1_case(G, dev)))
         return
     if a.case == "batched":
         r = batched_bench(G, dev)
