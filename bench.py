@@ -204,6 +204,26 @@ def _port_solve(L, tol, seed):
     return time.perf_counter() - t0, it
 
 
+def _u1_ref_solve(L, tol, seed=0):
+    """One complex CG solve of the reference built with PI_INTERACTION
+    (ConjugateGradient..., conjugategradient.c:115, from x = 0) at L on
+    b = M chi, to the absolute tolerance tol * |b|: (seconds, iterations)."""
+    sys.path.insert(0, str(ROOT))
+    from oracle import build_ref
+    from oracle.oracle import Ref
+    ref = Ref(L, 0, build=False, tag=build_ref.PI_TAG)
+    ref.init(1231, BETA_S, 0.05, 10)
+    rng = np.random.default_rng(seed)
+    V = L ** 3
+    ref.set_sigma(rng.normal(0.0, np.sqrt(2.0 / (NFLAV * BETA_S)), V))
+    ref.set_pi(rng.normal(0.0, np.sqrt(2.0 / (NFLAV * BETA_S)), V))
+    b = ref.dirac(rng.normal(size=V).astype(complex), 0)
+    t0 = time.perf_counter()
+    _, ok = ref.cg(b, None, tol * float(np.linalg.norm(b)), 1)
+    dt = time.perf_counter() - t0
+    return dt, ref.counters()[0]
+
+
 def reference_available(L):
     from oracle import build_ref
     return build_ref.lib_path(L, 0).exists()
@@ -618,6 +638,15 @@ def u1_case(G, dev, L=64, md_steps=10, eps=0.05, pi_steps=10, tol=1e-10, reps=2)
     ms, r = timed(run_pi)
     out["u1_pi_trajectory"] = {"ms": round(ms, 2), "cg_iterations": r["cg_iterations"], "dH": r["dH"]}
     lat.close()
+    # the reference's own complex solve on one host core, beside ours
+    nsol = solves_per_trajectory(md_steps)
+    out["gpu_ms_per_solve"] = round(out["u1_sigma_trajectory"]["ms"] / nsol, 3)
+    from oracle import build_ref
+    if build_ref.lib_path(L, 0, build_ref.PI_TAG).exists():
+        t, it = _u1_ref_solve(L, tol)
+        out["cpu_reference_one_solve"] = {"s": round(t, 3), "iterations": it, "cores": 1,
+                                          "kind": "reference (PI_INTERACTION build)",
+                                          "sample": f"one two-plane CG solve from x=0 at L={L} to |r| < {tol:g}|b|"}
     return out
 
 

@@ -29,6 +29,7 @@ OUT = HERE / "_ref"
 REF_DIR = Path(os.environ.get("GN_REFERENCE_DIR", "/root/reference"))
 
 DEFAULT_L = (4, 6, 8, 12, 16, 24, 32, 48, 64)
+PI_DEFS, PI_TAG = ("-DPI_INTERACTION",), "_pi"  # the U(1) model's build
 CFLAGS = ["-O3", "-fcommon", "-fPIC", "-w"]
 
 
@@ -81,6 +82,9 @@ def build_all(Ls=DEFAULT_L, integrators=(0,)) -> list[Path]:
     for L in (4, 8):
         for i in (1, 2):
             built.append(build(L, i))
+    # the U(1) model (PI_INTERACTION): the test sizes and the benchmark's L = 64
+    for L in (4, 8, 64):
+        built.append(build(L, 0, PI_DEFS, PI_TAG))
     return built
 
 
