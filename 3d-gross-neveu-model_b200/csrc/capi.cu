@@ -278,7 +278,7 @@ int gn_condensate_sigma(gn_context *ctx, const double *sigma, double *out) {
       up(E, ctx->io, sigma, size_t(E.V()));
       d = ctx->io;
     }
-    E.sigma_observables(d, out);
+    E.sigma_observables(d, E.u1() ? E.pi() : nullptr, out);
     return GN_OK;
   });
 }
@@ -286,7 +286,7 @@ int gn_condensate_sigma(gn_context *ctx, const double *sigma, double *out) {
 int gn_condensate_sigma_device(gn_context *ctx, const double *sigma, double *out) {
   if (!sigma || !out) return fail(GN_ERR_ARG, "null pointer");
   return guarded(ctx, [&](gn::Engine &E) {
-    E.sigma_observables(sigma, out);
+    E.sigma_observables(sigma, E.u1() ? E.pi() : nullptr, out);
     return GN_OK;
   });
 }
@@ -375,9 +375,11 @@ int gn_dirac_u1(gn_context *ctx, const double *sigmamass, const double *pimass, 
 }
 
 int gn_cg_u1(gn_context *ctx, const double *sigmamass, const double *pimass, const double *b, double *x, int nrhs,
-             double tol, int variant, int relative, long long max_iter, gn_cg_info *info) {
+             double tol, int variant, int relative, long long max_iter, int precision, gn_cg_info *info) {
   if (!sigmamass || !pimass || !b || !x) return fail(GN_ERR_ARG, "null pointer");
   if (nrhs < 1 || nrhs > 2) return fail(GN_ERR_ARG, "nrhs must be 1 or 2");
+  if (variant < 0 || variant > 1) return fail(GN_ERR_ARG, "bad variant");
+  if (precision != GN_PREC_FP64 && precision != GN_PREC_MIXED) return fail(GN_ERR_ARG, "precision: FP64 or MIXED");
   return guarded(ctx, [&](gn::Engine &E) {
     const size_t V = size_t(E.V());
     double *d_sm = ctx->io, *d_pm = d_sm + V, *d_b = d_pm + V, *d_x = d_b + 4 * V;
@@ -388,7 +390,7 @@ int gn_cg_u1(gn_context *ctx, const double *sigmamass, const double *pimass, con
     const double *bs[2] = {d_b, d_b + 2 * V};
     double *xs[2] = {d_x, d_x + 2 * V};
     gn::SolveInfo si[2];
-    const int st = E.solve_cm(d_sm, d_pm, bs, xs, nrhs, tol, variant, relative, max_iter, si);
+    const int st = E.solve_cm(d_sm, d_pm, bs, xs, nrhs, tol, variant, relative, max_iter, si, precision);
     down(E, x, d_x, 2 * size_t(nrhs) * V);
     sync(E);
     if (info)

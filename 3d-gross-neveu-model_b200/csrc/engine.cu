@@ -173,9 +173,9 @@ void Engine::cond_dots(const double *v, const double *D, double out[3]) {
   for (int q = 0; q < 3; q++) out[q] = sum_partials(h_partials_, nb, q);
 }
 
-void Engine::sigma_observables(const double *sigma, double out[8]) {
+void Engine::sigma_observables(const double *sigma, const double *pi, double out[8]) {
   const int nb = op_blocks(V_, num_sms_);
-  sigma_obs_kernel<<<nb, kOpThreads, 0, stream_>>>(g_, sigma, partials_);
+  sigma_obs_kernel<<<nb, kOpThreads, 0, stream_>>>(g_, sigma, pi, partials_);
   check(cudaGetLastError(), "sigma_obs_kernel");
   launches++;
   check(cudaMemcpyAsync(h_partials_, partials_, sizeof(double) * 2 * kSigmaObsSums * nb, cudaMemcpyDeviceToHost,

@@ -52,9 +52,9 @@ class Engine {
   void energy_terms(const double *P, const double *phi, const double *X, const double *sigma, double out[3]);
   // sum Re(conj v D)/V, sum Re(conj v D), sum Im(conj v D); synchronises.
   void cond_dots(const double *v, const double *D, double out[3]);
-  // CondensateSigmaPi of a device sigma (fermion order): the 8 outputs in the
-  // reference's argument order
-  void sigma_observables(const double *sigma, double out[8]);
+  // CondensateSigmaPi of a device sigma (fermion order), of |(sigma, pi)| when
+  // pi is given (the U(1) model): the 8 outputs in the reference's argument order
+  void sigma_observables(const double *sigma, const double *pi, double out[8]);
   void cond_fill(int mode, const signed char *signs, const double *table, const double *sm, double *v);
 
   // CG on M M^T for nrhs right-hand sides of ncomp planes each (b[k], x[k] are
@@ -110,9 +110,10 @@ class Engine {
   double *Y_c() { return Y_c_; }
   // M, M^dagger or out - M psi with the complex mass on nsys complex systems
   void dirac_cm(const double *sm, const double *pm, const double *in, double *out, int nsys, int op);
-  // CG on M M^dagger (FP64) for nrhs complex systems (b[k], x[k]: 2V each)
+  // CG on M M^dagger for nrhs complex systems (b[k], x[k]: 2V each);
+  // precision GN_PREC_FP64 or GN_PREC_MIXED
   int solve_cm(const double *sm, const double *pm, const double *const *b, double *const *x, int nrhs, double tol,
-               int variant, int rel, long long max_iter, SolveInfo *info);
+               int variant, int rel, long long max_iter, SolveInfo *info, int precision = GN_PREC_FP64);
   // fermion force of sigma (pi = false) or pi (pi = true) from complex X, Y
   // (4V each), minus gcoef * field, with the fused step P += pcoef F if P
   void force_cm(bool pi, const double *X, const double *Y, const double *field, double gcoef, double *F, double *P,
@@ -139,8 +140,9 @@ class Engine {
   void mixed_init();
   const void *mixed_kernel_ptr(int ncomp, int nrhs, int w);
   const void *fp64_kernel_ptr(int ncomp, int nrhs, int w);
+  // pm != nullptr: the U(1) model's complex mass (ncomp = 2)
   int solve_mixed(const double *sm, const double *const *b, double *const *x, int nrhs, int ncomp, double tol,
-                  int variant, int rel, long long max_iter, SolveInfo *info);
+                  int variant, int rel, long long max_iter, SolveInfo *info, const double *pm = nullptr);
   void *alloc(size_t bytes);
   int cg_blocks(int ncomp, int nrhs, bool mixed, int w);
   int trajectory_u1(const gn_hmc_params &hp, double (*gauss)(void), double (*uniform)(void), const double *pre_P,
@@ -163,6 +165,7 @@ class Engine {
   double *cg_work_ = nullptr;  // kMaxRhs * 4 vectors * 2 planes * V
   float *mx_work_ = nullptr;   // mixed precision: kMaxRhs * 5 vectors * 2 planes * V
   float *sm32_ = nullptr;
+  float *pm32_ = nullptr;  // the U(1) model: FP32 copy of the pi mass
   double *partials_ = nullptr;
   double *h_partials_ = nullptr;
   PhaseBar *bar_ = nullptr;

@@ -17,6 +17,7 @@ void Engine::mixed_init() {
   const size_t V = size_t(V_);
   mx_work_ = (float *)alloc(size_t(kMaxRhs) * kMixedVecs * 2 * V * sizeof(float));
   sm32_ = (float *)alloc(V * sizeof(float));
+  pm32_ = (float *)alloc(V * sizeof(float));
 }
 
 template <int W>
@@ -31,6 +32,14 @@ static const void *mixed_kernel(int ncomp, int nr) {
   throw GnError(GN_ERR_ARG, "complex systems: at most 2 right-hand sides per solve");
 }
 
+// the U(1) model: complex mass, one or two complex systems
+template <int W>
+static const void *mixed_cm_kernel(int nr) {
+  if (nr == 1) return (const void *)cg_mixed_kernel<2, 1, kSolverThreads, W, true>;
+  if (nr == 2) return (const void *)cg_mixed_kernel<2, 2, kSolverThreads, W, true>;
+  throw GnError(GN_ERR_ARG, "complex systems: at most 2 right-hand sides per solve");
+}
+
 // w: sites per item of the FP32 sweeps (1, 2 or 4)
 const void *Engine::mixed_kernel_ptr(int ncomp, int nrhs, int w) {
   const int nr = rhs_slots(nrhs);
@@ -40,13 +49,16 @@ const void *Engine::mixed_kernel_ptr(int ncomp, int nrhs, int w) {
 }
 
 int Engine::solve_mixed(const double *sm, const double *const *b, double *const *x, int nrhs, int ncomp, double tol,
-                        int variant, int rel, long long max_iter, SolveInfo *info) {
+                        int variant, int rel, long long max_iter, SolveInfo *info, const double *pm) {
+  if (pm != nullptr && ncomp != 2) throw GnError(GN_ERR_ARG, "the complex mass needs complex systems");
   const size_t V = size_t(V_);
   MixedArgs a;
   memset(&a, 0, sizeof a);
   a.g = g_;
   a.sm = sm;
   a.sm32 = sm32_;
+  a.pm = pm;
+  a.pm32 = pm32_;
   for (int k = 0; k < nrhs; k++) {
     float *w = mx_work_ + size_t(k) * kMixedVecs * 2 * V;
     a.b[k] = b[k];
@@ -75,15 +87,21 @@ int Engine::solve_mixed(const double *sm, const double *const *b, double *const 
   check(cudaMemsetAsync(err_, 0, sizeof(int), stream_), "memset");
   // FP32 sweeps in items of up to 4 sites (float4) when the caller's FP64
   // arrays allow the 2-site FP64 sweeps, else one site per item throughout
-  const void *ptrs[2 * kMaxRhs + 1] = {sm};
+  const void *ptrs[2 * kMaxRhs + 2] = {sm, pm != nullptr ? pm : sm};
   for (int k = 0; k < nrhs; k++) {
-    ptrs[1 + 2 * k] = b[k];
-    ptrs[2 + 2 * k] = x[k];
+    ptrs[2 + 2 * k] = b[k];
+    ptrs[3 + 2 * k] = x[k];
   }
-  const int w = fp64_width(L_, ptrs, 1 + 2 * nrhs) == 2 ? row_width(L_, 4) : 1;
+  const int w = fp64_width(L_, ptrs, 2 + 2 * nrhs) == 2 ? row_width(L_, 4) : 1;
   const int nb = cg_blocks(ncomp, nrhs, true, w);
-  check(launch_solver(mixed_kernel_ptr(ncomp, nrhs, w), nb, threads_for(ncomp, nrhs), a, stream_),
-        "cg_mixed_kernel launch");
+  const void *fn;
+  if (pm != nullptr) {
+    const int nr = rhs_slots(nrhs);
+    fn = w == 4 ? mixed_cm_kernel<4>(nr) : w == 2 ? mixed_cm_kernel<2>(nr) : mixed_cm_kernel<1>(nr);
+  } else {
+    fn = mixed_kernel_ptr(ncomp, nrhs, w);
+  }
+  check(launch_solver(fn, nb, threads_for(ncomp, nrhs), a, stream_), "cg_mixed_kernel launch");
   launches++;
   return finish_solve(nrhs, info);
 }

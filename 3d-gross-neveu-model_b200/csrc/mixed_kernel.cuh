@@ -65,6 +65,8 @@ struct MixedArgs {
   Geom g;
   const double *sm;
   float *sm32;
+  const double *pm;  // U(1) model (CM solves): the pi mass, and its FP32 copy
+  float *pm32;
   const double *b[kMaxRhs];
   double *x[kMaxRhs];
   double *t64[kMaxRhs];
@@ -99,8 +101,12 @@ struct MixedShared {
 
 // One mixed-precision solve by a team (all its threads call it; a.bar,
 // a.partials and a.err are not used: the team's own are).
-template <int NC, int NR, int W>
+//
+// CM (NC = 2): the U(1) model's complex mass sm + i eps pm, as in cg_solve;
+// always the split inner iteration.
+template <int NC, int NR, int W, bool CM = false>
 __device__ __forceinline__ void mixed_solve(const MixedArgs &a, Team &team, SyncShared &sh, MixedShared &ms) {
+  static_assert(!CM || NC == 2, "the complex mass couples the two planes of a system");
   constexpr int W64 = W >= 2 ? 2 : 1;
   double *const s_val = sh.val;
   double *const s_alpha = ms.alpha, *const s_beta = ms.beta, *const s_rr = ms.rr, *const s_tau = ms.tau;
@@ -150,13 +156,24 @@ __device__ __forceinline__ void mixed_solve(const MixedArgs &a, Team &team, Sync
       vload<double, W64>(sm + it.own, smi);
       const double *xk = pick<NR>(a.x, k);
       double *tk = pick<NR>(a.t64, k);
+      if constexpr (CM) {
+        Nb<double> nr[W64], ni[W64];
+        double b[W64], o_r[W64], o_i[W64];
+        gather_item<double, W64>(it, xk, nr);
+        gather_item<double, W64>(it, xk + V, ni);
+        item_eps_pm<double, W64>(g, it, a.pm, b);
+        item_Mt_cm<double, W64>(it, smi, b, nr, ni, o_r, o_i);
+        vstore<double, W64>(tk + it.own, o_r);
+        vstore<double, W64>(tk + V + it.own, o_i);
+      } else {
 #pragma unroll
-      for (int c = 0; c < NC; c++) {
-        Nb<double> n[W64];
-        double o[W64];
-        gather_item<double, W64>(it, xk + size_t(c) * V, n);
-        item_Mt<double, W64>(it, smi, n, o);
-        vstore<double, W64>(tk + size_t(c) * V + it.own, o);
+        for (int c = 0; c < NC; c++) {
+          Nb<double> n[W64];
+          double o[W64];
+          gather_item<double, W64>(it, xk + size_t(c) * V, n);
+          item_Mt<double, W64>(it, smi, n, o);
+          vstore<double, W64>(tk + size_t(c) * V + it.own, o);
+        }
       }
     });
     zero_acc();
@@ -169,23 +186,47 @@ __device__ __forceinline__ void mixed_solve(const MixedArgs &a, Team &team, Sync
         vload<double, W64>(sm + it.own, smi);
         const double *tk = pick<NR>(a.t64, k);
         const double *bk = pick<NR>(a.b, k);
+        if constexpr (CM) {
+          Nb<double> nr[W64], ni[W64];
+          double b[W64], br[W64], bim[W64], rr[W64], rim[W64];
+          gather_item<double, W64>(it, tk, nr);
+          gather_item<double, W64>(it, tk + V, ni);
+          item_eps_pm<double, W64>(g, it, a.pm, b);
+          vload<double, W64>(bk + it.own, br);
+          vload<double, W64>(bk + V + it.own, bim);
 #pragma unroll
-        for (int c = 0; c < NC; c++) {
-          Nb<double> n[W64];
-          double bi[W64], ri[W64];
-          gather_item<double, W64>(it, tk + size_t(c) * V, n);
-          vload<double, W64>(bk + size_t(c) * V + it.own, bi);
-#pragma unroll
-          for (int e = 0; e < W64; e++) ri[e] = bi[e];
-          item_sub_M<double, W64>(it, smi, n, ri);
+          for (int e = 0; e < W64; e++) {
+            rr[e] = br[e];
+            rim[e] = bim[e];
+          }
+          item_sub_M_cm<double, W64>(it, smi, b, nr, ni, rr, rim);
           double sr = 0.0, sb = 0.0;
 #pragma unroll
           for (int e = 0; e < W64; e++) {
-            sr += ri[e] * ri[e];
-            sb += bi[e] * bi[e];
+            sr += rr[e] * rr[e] + rim[e] * rim[e];
+            sb += br[e] * br[e] + bim[e] * bim[e];
           }
           acc_add<NR>(acc, k, sr);
           acc_add<NR>(acc, NR + k, sb);
+        } else {
+#pragma unroll
+          for (int c = 0; c < NC; c++) {
+            Nb<double> n[W64];
+            double bi[W64], ri[W64];
+            gather_item<double, W64>(it, tk + size_t(c) * V, n);
+            vload<double, W64>(bk + size_t(c) * V + it.own, bi);
+#pragma unroll
+            for (int e = 0; e < W64; e++) ri[e] = bi[e];
+            item_sub_M<double, W64>(it, smi, n, ri);
+            double sr = 0.0, sb = 0.0;
+#pragma unroll
+            for (int e = 0; e < W64; e++) {
+              sr += ri[e] * ri[e];
+              sb += bi[e] * bi[e];
+            }
+            acc_add<NR>(acc, k, sr);
+            acc_add<NR>(acc, NR + k, sb);
+          }
         }
       });
     }
@@ -207,7 +248,7 @@ __device__ __forceinline__ void mixed_solve(const MixedArgs &a, Team &team, Sync
     if (threadIdx.x == 0) sys_list_from(s_run, s_active, a.nrhs);
     __syncthreads();
   }
-  const bool split = a.scheme == kMixedSplit;
+  const bool split = CM || a.scheme == kMixedSplit;
   // x = 0, x^ = 0, r^ = (float) b, p^ = (float) b (two-phase) or 0 (split),
   // a^ = 0, sm32 = (float) sm; sums r^2 (FP32 values), b^2
   zero_acc();
@@ -220,6 +261,12 @@ __device__ __forceinline__ void mixed_solve(const MixedArgs &a, Team &team, Sync
 #pragma unroll
       for (int e = 0; e < W64; e++) s32[e] = float(s64[e]);
       vstore<float, W64>(a.sm32 + own, s32);
+      if constexpr (CM) {
+        vload<double, W64>(a.pm + own, s64);
+#pragma unroll
+        for (int e = 0; e < W64; e++) s32[e] = float(s64[e]);
+        vstore<float, W64>(a.pm32 + own, s32);
+      }
     }
     for_units(NI64, s_run, team, [&](int k, uint32_t j) {
       const uint32_t own = make_item<W64>(g, j).own;
@@ -290,22 +337,41 @@ __device__ __forceinline__ void mixed_solve(const MixedArgs &a, Team &team, Sync
         vload<float, W>(a.sm32 + ri.own, smi);
         const float *rk = pick<NR>(a.rh, k);
         float *uk = pick<NR>(a.uh, k);
-#pragma unroll
-        for (int c = 0; c < NC; c++) {
-          const size_t off = size_t(c) * V;
-          Nb<float> n[W];
-          float u[W];
-          gather_item<float, W>(ri, rk + off, n);
-          item_Mt<float, W>(ri, smi, n, u);
-          vstore<float, W>(uk + off + ri.own, u);
+        if constexpr (CM) {
+          Nb<float> nr[W], ni[W];
+          float b[W], u_r[W], u_i[W];
+          gather_item<float, W>(ri, rk, nr);
+          gather_item<float, W>(ri, rk + V, ni);
+          item_eps_pm<float, W>(g, ri, a.pm32, b);
+          item_Mt_cm<float, W>(ri, smi, b, nr, ni, u_r, u_i);
+          vstore<float, W>(uk + ri.own, u_r);
+          vstore<float, W>(uk + V + ri.own, u_i);
           double sg = 0.0, sd = 0.0;
 #pragma unroll
           for (int e = 0; e < W; e++) {
-            sg += double(n[e].c) * double(n[e].c);
-            sd += double(u[e]) * double(u[e]);
+            sg += double(nr[e].c) * double(nr[e].c) + double(ni[e].c) * double(ni[e].c);
+            sd += double(u_r[e]) * double(u_r[e]) + double(u_i[e]) * double(u_i[e]);
           }
           acc_add<NR>(acc, k, sg);
           acc_add<NR>(acc, NR + k, sd);
+        } else {
+#pragma unroll
+          for (int c = 0; c < NC; c++) {
+            const size_t off = size_t(c) * V;
+            Nb<float> n[W];
+            float u[W];
+            gather_item<float, W>(ri, rk + off, n);
+            item_Mt<float, W>(ri, smi, n, u);
+            vstore<float, W>(uk + off + ri.own, u);
+            double sg = 0.0, sd = 0.0;
+#pragma unroll
+            for (int e = 0; e < W; e++) {
+              sg += double(n[e].c) * double(n[e].c);
+              sd += double(u[e]) * double(u[e]);
+            }
+            acc_add<NR>(acc, k, sg);
+            acc_add<NR>(acc, NR + k, sd);
+          }
         }
       });
       ok = end_phase<2 * NR>(acc, sh, team, abort_req);
@@ -461,26 +527,51 @@ __device__ __forceinline__ void mixed_solve(const MixedArgs &a, Team &team, Sync
         const double *xk = pick<NR>(a.x, k);
         const float *xhk = pick<NR>(a.xh, k);
         double *tk = pick<NR>(a.t64, k);
+        if constexpr (CM) {
+          Nb<double> n[2][W64];
 #pragma unroll
-        for (int c = 0; c < NC; c++) {
-          const size_t off = size_t(c) * V;
-          const double *xv = xk + off;
-          const float *xhv = xhk + off;
-          Nb<double> n[W64];
-          gather_item<double, W64>(
-              it, n,
-              [&](uint32_t i, double(&v)[W64]) {
-                double xx[W64];
-                float hh[W64];
-                vload<double, W64>(xv + i, xx);
-                vload<float, W64>(xhv + i, hh);
+          for (int c = 0; c < 2; c++) {
+            const double *xv = xk + size_t(c) * V;
+            const float *xhv = xhk + size_t(c) * V;
+            gather_item<double, W64>(
+                it, n[c],
+                [&](uint32_t i, double(&v)[W64]) {
+                  double xx[W64];
+                  float hh[W64];
+                  vload<double, W64>(xv + i, xx);
+                  vload<float, W64>(xhv + i, hh);
 #pragma unroll
-                for (int e = 0; e < W64; e++) v[e] = xx[e] + double(hh[e]);
-              },
-              [&](uint32_t i) { return xv[i] + double(xhv[i]); });
-          double o[W64];
-          item_Mt<double, W64>(it, smi, n, o);
-          vstore<double, W64>(tk + off + it.own, o);
+                  for (int e = 0; e < W64; e++) v[e] = xx[e] + double(hh[e]);
+                },
+                [&](uint32_t i) { return xv[i] + double(xhv[i]); });
+          }
+          double b[W64], o_r[W64], o_i[W64];
+          item_eps_pm<double, W64>(g, it, a.pm, b);
+          item_Mt_cm<double, W64>(it, smi, b, n[0], n[1], o_r, o_i);
+          vstore<double, W64>(tk + it.own, o_r);
+          vstore<double, W64>(tk + V + it.own, o_i);
+        } else {
+#pragma unroll
+          for (int c = 0; c < NC; c++) {
+            const size_t off = size_t(c) * V;
+            const double *xv = xk + off;
+            const float *xhv = xhk + off;
+            Nb<double> n[W64];
+            gather_item<double, W64>(
+                it, n,
+                [&](uint32_t i, double(&v)[W64]) {
+                  double xx[W64];
+                  float hh[W64];
+                  vload<double, W64>(xv + i, xx);
+                  vload<float, W64>(xhv + i, hh);
+#pragma unroll
+                  for (int e = 0; e < W64; e++) v[e] = xx[e] + double(hh[e]);
+                },
+                [&](uint32_t i) { return xv[i] + double(xhv[i]); });
+            double o[W64];
+            item_Mt<double, W64>(it, smi, n, o);
+            vstore<double, W64>(tk + off + it.own, o);
+          }
         }
       });
       zero_acc();
@@ -497,32 +588,69 @@ __device__ __forceinline__ void mixed_solve(const MixedArgs &a, Team &team, Sync
         double *xk = pick<NR>(a.x, k);
         float *xhk = pick<NR>(a.xh, k);
         float *rhk = pick<NR>(a.rh, k);
+        if constexpr (CM) {
+          Nb<double> nr[W64], ni[W64];
+          double b[W64], rv[2][W64];
+          gather_item<double, W64>(it, tk, nr);
+          gather_item<double, W64>(it, tk + V, ni);
+          item_eps_pm<double, W64>(g, it, a.pm, b);
 #pragma unroll
-        for (int c = 0; c < NC; c++) {
-          const size_t off = size_t(c) * V + it.own;
-          double xx[W64], ri[W64];
-          float hh[W64], z32[W64], rf[W64];
-          vload<double, W64>(xk + off, xx);
-          vload<float, W64>(xhk + off, hh);
+          for (int c = 0; c < 2; c++) {
+            const size_t off = size_t(c) * V + it.own;
+            double xx[W64];
+            float hh[W64], z32[W64];
+            vload<double, W64>(xk + off, xx);
+            vload<float, W64>(xhk + off, hh);
 #pragma unroll
-          for (int e = 0; e < W64; e++) {
-            xx[e] = xx[e] + double(hh[e]);
-            z32[e] = 0.f;
+            for (int e = 0; e < W64; e++) {
+              xx[e] = xx[e] + double(hh[e]);
+              z32[e] = 0.f;
+            }
+            vstore<double, W64>(xk + off, xx);
+            vstore<float, W64>(xhk + off, z32);
+            vload<double, W64>(bk + off, rv[c]);
           }
-          vstore<double, W64>(xk + off, xx);
-          vstore<float, W64>(xhk + off, z32);
-          Nb<double> n[W64];
-          gather_item<double, W64>(it, tk + size_t(c) * V, n);
-          vload<double, W64>(bk + off, ri);
-          item_sub_M<double, W64>(it, smi, n, ri);
+          item_sub_M_cm<double, W64>(it, smi, b, nr, ni, rv[0], rv[1]);
           double sr = 0.0;
 #pragma unroll
-          for (int e = 0; e < W64; e++) {
-            rf[e] = float(ri[e]);
-            sr += ri[e] * ri[e];
+          for (int c = 0; c < 2; c++) {
+            float rf[W64];
+#pragma unroll
+            for (int e = 0; e < W64; e++) {
+              rf[e] = float(rv[c][e]);
+              sr += rv[c][e] * rv[c][e];
+            }
+            vstore<float, W64>(rhk + size_t(c) * V + it.own, rf);
           }
           acc_add<NR>(acc, k, sr);
-          vstore<float, W64>(rhk + off, rf);
+        } else {
+#pragma unroll
+          for (int c = 0; c < NC; c++) {
+            const size_t off = size_t(c) * V + it.own;
+            double xx[W64], ri[W64];
+            float hh[W64], z32[W64], rf[W64];
+            vload<double, W64>(xk + off, xx);
+            vload<float, W64>(xhk + off, hh);
+#pragma unroll
+            for (int e = 0; e < W64; e++) {
+              xx[e] = xx[e] + double(hh[e]);
+              z32[e] = 0.f;
+            }
+            vstore<double, W64>(xk + off, xx);
+            vstore<float, W64>(xhk + off, z32);
+            Nb<double> n[W64];
+            gather_item<double, W64>(it, tk + size_t(c) * V, n);
+            vload<double, W64>(bk + off, ri);
+            item_sub_M<double, W64>(it, smi, n, ri);
+            double sr = 0.0;
+#pragma unroll
+            for (int e = 0; e < W64; e++) {
+              rf[e] = float(ri[e]);
+              sr += ri[e] * ri[e];
+            }
+            acc_add<NR>(acc, k, sr);
+            vstore<float, W64>(rhk + off, rf);
+          }
         }
       });
       ok = end_phase<NR>(acc, sh, team);
@@ -557,33 +685,66 @@ __device__ __forceinline__ void mixed_solve(const MixedArgs &a, Team &team, Sync
         vload<float, W>(a.sm32 + ri.own, smi);
         const float alpha = float(s_alpha[k]), beta = float(s_beta[k]);
         const float *uk = pick<NR>(a.uh, k);
+        if constexpr (CM) {
+          Nb<float> nr[W], ni[W];
+          float b[W], w[2][W];
+          gather_item<float, W>(ri, uk, nr);
+          gather_item<float, W>(ri, uk + V, ni);
+          item_eps_pm<float, W>(g, ri, a.pm32, b);
+          item_M_cm<float, W>(ri, smi, b, nr, ni, w[0], w[1]);
 #pragma unroll
-        for (int c = 0; c < NC; c++) {
-          const size_t off = size_t(c) * V;
-          const size_t o = off + ri.own;
-          Nb<float> n[W];
-          float w[W], av[W], pv[W], xv[W], rv[W];
-          gather_item<float, W>(ri, uk + off, n);
-          float *const ak = pick<NR>(a.ah, k) + o;
-          float *const pk = pick<NR>(a.ph, k) + o;
-          float *const xk = pick<NR>(a.xh, k) + o;
-          float *const rk = pick<NR>(a.rh, k) + o;
-          vload<float, W>(ak, av);
-          vload<float, W>(pk, pv);
-          vload<float, W>(xk, xv);
-          vload<float, W>(rk, rv);
-          item_M<float, W>(ri, smi, n, w);
+          for (int c = 0; c < 2; c++) {
+            const size_t o = size_t(c) * V + ri.own;
+            float av[W], pv[W], xv[W], rv[W];
+            float *const ak = pick<NR>(a.ah, k) + o;
+            float *const pk = pick<NR>(a.ph, k) + o;
+            float *const xk = pick<NR>(a.xh, k) + o;
+            float *const rk = pick<NR>(a.rh, k) + o;
+            vload<float, W>(ak, av);
+            vload<float, W>(pk, pv);
+            vload<float, W>(xk, xv);
+            vload<float, W>(rk, rv);
 #pragma unroll
-          for (int e = 0; e < W; e++) {
-            av[e] = fmaf(beta, av[e], w[e]);
-            pv[e] = fmaf(beta, pv[e], rv[e]);
-            xv[e] = fmaf(alpha, pv[e], xv[e]);
-            rv[e] = fmaf(-alpha, av[e], rv[e]);
+            for (int e = 0; e < W; e++) {
+              av[e] = fmaf(beta, av[e], w[c][e]);
+              pv[e] = fmaf(beta, pv[e], rv[e]);
+              xv[e] = fmaf(alpha, pv[e], xv[e]);
+              rv[e] = fmaf(-alpha, av[e], rv[e]);
+            }
+            vstore<float, W>(ak, av);
+            vstore<float, W>(pk, pv);
+            vstore<float, W>(xk, xv);
+            vstore<float, W>(rk, rv);
           }
-          vstore<float, W>(ak, av);
-          vstore<float, W>(pk, pv);
-          vstore<float, W>(xk, xv);
-          vstore<float, W>(rk, rv);
+        } else {
+#pragma unroll
+          for (int c = 0; c < NC; c++) {
+            const size_t off = size_t(c) * V;
+            const size_t o = off + ri.own;
+            Nb<float> n[W];
+            float w[W], av[W], pv[W], xv[W], rv[W];
+            gather_item<float, W>(ri, uk + off, n);
+            float *const ak = pick<NR>(a.ah, k) + o;
+            float *const pk = pick<NR>(a.ph, k) + o;
+            float *const xk = pick<NR>(a.xh, k) + o;
+            float *const rk = pick<NR>(a.rh, k) + o;
+            vload<float, W>(ak, av);
+            vload<float, W>(pk, pv);
+            vload<float, W>(xk, xv);
+            vload<float, W>(rk, rv);
+            item_M<float, W>(ri, smi, n, w);
+#pragma unroll
+            for (int e = 0; e < W; e++) {
+              av[e] = fmaf(beta, av[e], w[e]);
+              pv[e] = fmaf(beta, pv[e], rv[e]);
+              xv[e] = fmaf(alpha, pv[e], xv[e]);
+              rv[e] = fmaf(-alpha, av[e], rv[e]);
+            }
+            vstore<float, W>(ak, av);
+            vstore<float, W>(pk, pv);
+            vstore<float, W>(xk, xv);
+            vstore<float, W>(rk, rv);
+          }
         }
       });
       ok = team_barrier(sh, team);
@@ -609,12 +770,12 @@ __device__ __forceinline__ void mixed_solve(const MixedArgs &a, Team &team, Sync
 }
 
 // The single-lattice solve: the whole cooperative grid is the team.
-template <int NC, int NR, int BS, int W>
+template <int NC, int NR, int BS, int W, bool CM = false>
 __global__ void __launch_bounds__(BS, 1) cg_mixed_kernel(MixedArgs a) {
   __shared__ SyncShared sh;
   __shared__ MixedShared ms;
   Team team = grid_team(a.bar, a.partials, a.err);
-  mixed_solve<NC, NR, W>(a, team, sh, ms);
+  mixed_solve<NC, NR, W, CM>(a, team, sh, ms);
 }
 
 }  // namespace gn

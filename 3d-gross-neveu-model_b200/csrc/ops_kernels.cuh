@@ -350,11 +350,13 @@ constexpr double kPi = 3.14159265358979323846;
 constexpr int kSigmaObsSums = 7;
 constexpr int kSigmaObs = 8;
 
+// pi != null: the U(1) model's order parameter |(sigma, pi)| = pow(sigma^2 +
+// pi^2, 0.5) in place of sigma (observables.c:354-357).
 __device__ __forceinline__ void sigma_obs_site(const Geom &g, uint32_t i, const double *__restrict__ sigma,
-                                               double (&v)[kSigmaObsSums]) {
+                                               double (&v)[kSigmaObsSums], const double *__restrict__ pi = nullptr) {
   uint32_t x[3], par, row, k;
   site_coords(g, i, x[0], x[1], x[2], par, row, k);
-  const double t = sigma[i] / double(g.V);
+  const double t = (pi == nullptr ? sigma[i] : sqrt(sigma[i] * sigma[i] + pi[i] * pi[i])) / double(g.V);
   const double pmin = (2 * kPi) / double(g.L);
   v[0] = t;
 #pragma unroll
@@ -379,14 +381,14 @@ __host__ __device__ inline void sigma_obs_finish(const double (&s)[kSigmaObsSums
 }
 
 static __global__ void __launch_bounds__(kOpThreads) sigma_obs_kernel(Geom g, const double *__restrict__ sigma,
-                                                                      double *part) {
+                                                                      const double *__restrict__ pi, double *part) {
   double hi[kSigmaObsSums], lo[kSigmaObsSums];
 #pragma unroll
   for (int q = 0; q < kSigmaObsSums; q++) hi[q] = lo[q] = 0.0;
   const uint32_t V = uint32_t(g.V);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x) {
     double v[kSigmaObsSums];
-    sigma_obs_site(g, i, sigma, v);
+    sigma_obs_site(g, i, sigma, v, pi);
 #pragma unroll
     for (int q = 0; q < kSigmaObsSums; q++) neumaier(hi[q], lo[q], v[q]);
   }

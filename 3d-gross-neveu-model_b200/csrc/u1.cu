@@ -60,9 +60,12 @@ static const void *cm_kernel(int nr) {
 }
 
 int Engine::solve_cm(const double *sm, const double *pm, const double *const *b, double *const *x, int nrhs,
-                     double tol, int variant, int rel, long long max_iter, SolveInfo *info) {
+                     double tol, int variant, int rel, long long max_iter, SolveInfo *info, int precision) {
   if (nrhs < 1 || nrhs > 2) throw GnError(GN_ERR_ARG, "the U(1) solve takes 1 or 2 systems");
+  if (precision != GN_PREC_FP64 && precision != GN_PREC_MIXED)
+    throw GnError(GN_ERR_ARG, "the U(1) model solves in FP64 or mixed precision");
   if (max_iter <= 0) max_iter = V_ + 1;  // MAX_CONJUGATE_GRADIENT_ITERATION, macro.h:134
+  if (precision == GN_PREC_MIXED) return solve_mixed(sm, b, x, nrhs, 2, tol, variant, rel, max_iter, info, pm);
   const size_t V = size_t(V_);
   CgArgs<double> a;
   memset(&a, 0, sizeof a);
@@ -149,7 +152,8 @@ void load_chi(Engine &E, const double *host_chi, const double *dev_chi) {
 // The sigma integrators (the schedules of schedule.h) with the complex M.
 int Engine::trajectory_u1(const gn_hmc_params &hp, double (*gauss)(void), double (*uniform)(void), const double *pre_P,
                           const double *pre_chi, gn_traj_result *res) {
-  if (hp.precision != GN_PREC_FP64) throw GnError(GN_ERR_ARG, "the U(1) model runs in FP64");
+  if (hp.precision != GN_PREC_FP64 && hp.precision != GN_PREC_MIXED)
+    throw GnError(GN_ERR_ARG, "the U(1) model runs in FP64 or mixed precision");
   const size_t V = size_t(V_);
   memset(res, 0, sizeof *res);
   // draws: P, chi_0, chi_1 (moleculardynamics.c:1240-1247)
@@ -187,7 +191,7 @@ int Engine::trajectory_u1(const gn_hmc_params &hp, double (*gauss)(void), double
     finish(0);
     return GN_NOT_CONVERGED;
   };
-  int st = solve_cm(sm_, pm_, phis, Xs, 2, hp.tol_high, 1, hp.relative, 0, info);
+  int st = solve_cm(sm_, pm_, phis, Xs, 2, hp.tol_high, 1, hp.relative, 0, info, hp.precision);
   count_flavours(info, 2, iters, calls, inner, rel);
   if (st != GN_OK) return fail();
   const double ccoef = (4 * hp.beta_s / 4.0);  // (NFLAV * beta_scalar / 4.0), moleculardynamics.c:316
@@ -200,7 +204,7 @@ int Engine::trajectory_u1(const gn_hmc_params &hp, double (*gauss)(void), double
     const Op &o = ops[k];
     if (o.op == OP_F_MED || o.op == OP_F_HIGH) {
       const double tol = o.op == OP_F_MED ? hp.tol_medium : hp.tol_high;
-      st = solve_cm(sm_, pm_, phis, Xs, 2, tol, 0, hp.relative, 0, info);
+      st = solve_cm(sm_, pm_, phis, Xs, 2, tol, 0, hp.relative, 0, info, hp.precision);
       count_flavours(info, 2, iters, calls, inner, rel);
       if (st != GN_OK) return fail();
       dirac_cm(sm_, pm_, X_c_, Y_c_, 2, GN_OP_MT);
@@ -218,7 +222,7 @@ int Engine::trajectory_u1(const gn_hmc_params &hp, double (*gauss)(void), double
       distance += o.c;
       res->distance += o.c;
     } else {
-      st = solve_cm(sm_, pm_, phis, Xs, 2, hp.tol_high, 1, hp.relative, 0, info);
+      st = solve_cm(sm_, pm_, phis, Xs, 2, hp.tol_high, 1, hp.relative, 0, info, hp.precision);
       count_flavours(info, 2, iters, calls, inner, rel);
       if (st != GN_OK) return fail();
     }
@@ -246,7 +250,8 @@ int Engine::trajectory_pi(const gn_hmc_params &hp, void (*gauss_pair)(double *, 
                           double (*uniform)(void), gn_traj_result *res) {
   if (!u1_) throw GnError(GN_ERR_ARG, "the context is not in the U(1) model (load pi first)");
   if (hp.steps < 1) throw GnError(GN_ERR_ARG, "steps must be >= 1");
-  if (hp.precision != GN_PREC_FP64) throw GnError(GN_ERR_ARG, "the U(1) model runs in FP64");
+  if (hp.precision != GN_PREC_FP64 && hp.precision != GN_PREC_MIXED)
+    throw GnError(GN_ERR_ARG, "the U(1) model runs in FP64 or mixed precision");
   const size_t V = size_t(V_);
   memset(res, 0, sizeof *res);
   double *h = h_stage_;
@@ -286,7 +291,7 @@ int Engine::trajectory_pi(const gn_hmc_params &hp, void (*gauss_pair)(double *, 
   const double ecoef = (4 * hp.beta_s / 8.0);  // (NFLAV * beta_scalar / 8.0), moleculardynamics.c:365
   const double gcoef = (4 * hp.beta_s / 4.0);  // (NFLAV * beta_scalar / 4.0), moleculardynamics.c:685
   auto pi_force = [&](double pcoef) {  // ComputePiForce, then P_pi += pcoef F_pi
-    const int s = solve_cm(sm_, pm_, phis, Xs, 2, hp.tol_high, 0, hp.relative, 0, info);
+    const int s = solve_cm(sm_, pm_, phis, Xs, 2, hp.tol_high, 0, hp.relative, 0, info, hp.precision);
     count_flavours(info, 2, iters, calls, inner, rel);
     if (s != GN_OK) return false;
     dirac_cm(sm_, pm_, X_c_, Y_c_, 2, GN_OP_MT);
@@ -297,7 +302,7 @@ int Engine::trajectory_pi(const gn_hmc_params &hp, void (*gauss_pair)(double *, 
     sigma_mass(pi(), Ppi_, eps, pi_alt(), pm_);
     swap_pi();
   };
-  int st = solve_cm(sm_, pm_, phis, Xs, 2, hp.tol_high, 0, hp.relative, 0, info);
+  int st = solve_cm(sm_, pm_, phis, Xs, 2, hp.tol_high, 0, hp.relative, 0, info, hp.precision);
   count_flavours(info, 2, iters, calls, inner, rel);
   if (st != GN_OK) return fail();
   double e[3];

@@ -203,7 +203,8 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
         "gn_store_pi": ([v, _dp, _dp], C.c_int),
         "gn_set_u1": ([v, C.c_int], C.c_int),
         "gn_dirac_u1": ([v, _dp, _dp, _dp, _dp, C.c_int, C.c_int], C.c_int),
-        "gn_cg_u1": ([v, _dp, _dp, _dp, _dp, C.c_int, C.c_double, C.c_int, C.c_int, C.c_longlong, C.POINTER(CgInfo)],
+        "gn_cg_u1": ([v, _dp, _dp, _dp, _dp, C.c_int, C.c_double, C.c_int, C.c_int, C.c_longlong, C.c_int,
+                      C.POINTER(CgInfo)],
                      C.c_int),
         "gn_sigma_force_u1": ([v, C.c_double, _dp, _dp, _dp, _dp, _dp, _dp, C.c_double, _dp, C.POINTER(CgInfo)],
                               C.c_int),
@@ -535,14 +536,14 @@ class Lattice:
         r = self._uncplanes(o, n)
         return r[0] if single else r
 
-    def cg_u1(self, sm, pm, b, x0=None, tol=1e-9, variant=0, relative=False, max_iter=0):
+    def cg_u1(self, sm, pm, b, x0=None, tol=1e-9, variant=0, relative=False, max_iter=0, precision=GN_PREC_FP64):
         single = np.asarray(b).ndim == 1
         bp, n = self._cplanes(b)
         xp = np.zeros_like(bp) if x0 is None else self._cplanes(x0)[0].copy()
         infos = (CgInfo * n)()
         st = self._check(self.lib.gn_cg_u1(self.ctx, _p(np.ascontiguousarray(sm, np.float64)),
                                            _p(np.ascontiguousarray(pm, np.float64)), _p(bp), _p(xp), n, tol,
-                                           variant, int(relative), max_iter, infos),
+                                           variant, int(relative), max_iter, precision, infos),
                          allow=(GN_OK, GN_NOT_CONVERGED))
         x = self._uncplanes(xp, n)
         return (x[0] if single else x), [i.as_dict() for i in infos], st
@@ -575,11 +576,11 @@ class Lattice:
         return H.value
 
     def trajectory_pi(self, beta_s, eps, steps, gauss_pair=None, gauss=None, uniform=None, tol_high=1e-9,
-                      relative=False):
+                      relative=False, precision=GN_PREC_FP64):
         """LeapFrog2Pi on the resident sigma and pi.  gauss_pair(a, b) fills two
         N(0, 1) values (the reference's Gauss2MeanVariance(a, b, 0, 1)): an int
         address, a PAIR_FN or a Python callable taking two POINTER(c_double)."""
-        hp = HmcParams(beta_s, eps, steps, 0, tol_high, tol_high, int(relative), GN_PREC_FP64)
+        hp = HmcParams(beta_s, eps, steps, 0, tol_high, tol_high, int(relative), precision)
         res = TrajResult()
         if gauss_pair is not None and not isinstance(gauss_pair, (int, C._CFuncPtr)):
             gauss_pair = PAIR_FN(gauss_pair)

@@ -167,7 +167,9 @@ GN_API int gn_condensate(gn_context *ctx, const double *sigmamass, double tol, d
  * sigma (V doubles, fermion order) on the host, or NULL for the resident
  * sigma (no transfer of the field).  out[8] = condensate_sigma,
  * |condensate_sigma|, mu2, mu4, chi, chip, chip_pbc1, chip_pbc2, the
- * reference's argument order.  The sums run on the device. */
+ * reference's argument order.  The sums run on the device.  In the U(1) model
+ * (after gn_load_pi) the order parameter is |(sigma, pi)| with the resident
+ * pi, as under PI_INTERACTION (observables.c:354-357). */
 GN_API int gn_condensate_sigma(gn_context *ctx, const double *sigma, double *out);
 /* The same for a device sigma (V doubles). */
 GN_API int gn_condensate_sigma_device(gn_context *ctx, const double *sigma, double *out);
@@ -190,9 +192,12 @@ GN_API int gn_set_u1(gn_context *ctx, int on);
 GN_API int gn_dirac_u1(gn_context *ctx, const double *sigmamass, const double *pimass, const double *in, double *out,
                        int nsys, int op);
 /* CG on M M^dagger for nrhs (1 or 2) complex systems (b, x: 2 nrhs V; x in/out),
- * variant / relative / max_iter as gn_cg; FP64.  info[nrhs] may be NULL. */
+ * variant / relative / max_iter as gn_cg; precision GN_PREC_FP64 or
+ * GN_PREC_MIXED (FP32 inner iterations, FP64 reliable updates, the same
+ * true-residual test).  info[nrhs] may be NULL. */
 GN_API int gn_cg_u1(gn_context *ctx, const double *sigmamass, const double *pimass, const double *b, double *x,
-                    int nrhs, double tol, int variant, int relative, long long max_iter, gn_cg_info *info);
+                    int nrhs, double tol, int variant, int relative, long long max_iter, int precision,
+                    gn_cg_info *info);
 /* ComputeSigmaForce (moleculardynamics.c:631-647) and ComputePiForce
  * (:736-752) in the U(1) model: X_f = (M M^dagger)^-1 phi_f by variant-0 CG
  * from the incoming X_f (tolerance tol), Y_f = M^dagger X_f, then
@@ -219,7 +224,7 @@ GN_API int gn_energy_u1(gn_context *ctx, int which, double beta_s, const double 
  * params->tol_high; the Metropolis test with uniform().  pi is restored on
  * reject or on a failed solve (res->ok = 0).  params->eps and ->steps are the
  * pi step (epsilon_pi_HMC, steps_pi_HMC); integrator and tol_medium are not
- * used; precision GN_PREC_FP64.  gauss_pair and gauss NULL: P_pi (GN_F_PI_P)
+ * used; precision GN_PREC_FP64 or GN_PREC_MIXED.  gauss_pair and gauss NULL: P_pi (GN_F_PI_P)
  * and the real parts of GN_F_CHI_C as they are. */
 GN_API int gn_trajectory_pi(gn_context *ctx, const gn_hmc_params *params, void (*gauss_pair)(double *, double *),
                             double (*gauss)(void), double (*uniform)(void), gn_traj_result *res);

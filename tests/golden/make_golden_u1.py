@@ -47,7 +47,8 @@ def fixture(L):
     sigma, pi = field(L, 11 + L), field(L, 13 + L)
     ref.set_sigma(sigma)
     ref.set_pi(pi)
-    d = dict(L=L, beta_s=BETA_S, sigma=sigma, pi=pi, sm=ref.sigmamass(), pm=ref.pimass())
+    d = dict(L=L, beta_s=BETA_S, sigma=sigma, pi=pi, sm=ref.sigmamass(), pm=ref.pimass(),
+             sigma_obs=ref.condensate_sigma())  # CondensateSigmaPi of |(sigma, pi)|
     # operators on a complex field
     psi, out0 = cplx(rng, V), cplx(rng, V)
     d.update(psi=psi, M_psi=ref.dirac(psi, 0), Mt_psi=ref.dirac(psi, 1), sub_out0=out0,

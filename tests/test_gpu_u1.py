@@ -32,6 +32,8 @@ def test_u1_operators_solve_forces_energies(golden, L):
         lat.load_pi(g["pi"])
         _, pm = lat.store_pi()
         assert np.array_equal(pm, g["pm"])
+        # CondensateSigmaPi of the U(1) order parameter |(sigma, pi)|
+        np.testing.assert_allclose(lat.condensate_sigma(), g["sigma_obs"], rtol=1e-12, atol=1e-16)
         sm = g["sm"]
         assert np.array_equal(lat.dirac_u1(sm, pm, g["psi"], G.GN_OP_M), g["M_psi"])
         assert rel(lat.dirac_u1(sm, pm, g["psi"], G.GN_OP_MT), g["Mt_psi"]) < 1e-15
@@ -103,3 +105,77 @@ def test_u1_switch_back(golden):
         lat.load_sigma(g["sigma0"])
         r = lat.trajectory(float(g["beta_s"]), float(g["eps"]), int(g["steps"]), None, None)
         assert r["ok"] == 1
+
+
+def _u1_fields(L, seed):
+    rng = np.random.default_rng(seed)
+    s = np.sqrt(2.0 / (4 * 0.85))
+    return rng, rng.normal(0, s, L ** 3), rng.normal(0, s, L ** 3)
+
+
+@pytest.mark.parametrize("L", [6, 16])
+def test_u1_mixed_precision_solver(L):
+    """The mixed solver with the complex mass (FP32 inner iterations, FP64
+    reliable updates) meets the FP64 stopping rule on the true residual,
+    checked with the FP64 operators, for one and two systems and both start
+    variants."""
+    import gn_b200 as G
+    rng, sigma, pi = _u1_fields(L, 40 + L)
+    V = L ** 3
+    with G.Lattice(L) as lat:
+        lat.load_sigma(sigma)
+        lat.load_pi(pi)
+        _, pm = lat.store_pi()
+        _, sm = lat.store_sigma()
+        b = np.stack([rng.normal(size=V) + 1j * rng.normal(size=V) for _ in range(2)])
+        x0 = 0.1 * (rng.normal(size=(2, V)) + 1j * rng.normal(size=(2, V)))
+        for variant in (0, 1):
+            for nsys in (1, 2):
+                nb = b[0] if nsys == 1 else b
+                start = None if variant == 1 else (x0[0] if nsys == 1 else x0)
+                x64, i64, st = lat.cg_u1(sm, pm, nb, start, 1e-10, variant=variant, relative=True)
+                xm, im, st2 = lat.cg_u1(sm, pm, nb, start, 1e-10, variant=variant, relative=True,
+                                        precision=G.GN_PREC_MIXED)
+                assert st == G.GN_OK and st2 == G.GN_OK
+                bs, xs = np.atleast_2d(nb), np.atleast_2d(xm)
+                for k in range(bs.shape[0]):
+                    y = lat.dirac_u1(sm, pm, xs[k], G.GN_OP_MT)
+                    r = bs[k] - lat.dirac_u1(sm, pm, y, G.GN_OP_M)
+                    assert np.linalg.norm(r) < 1e-10 * np.linalg.norm(bs[k]) * 1.01
+                    assert im[k]["reliable_updates"] >= 1
+                    assert im[k]["iterations"] <= 1.1 * i64[k]["iterations"] + 20
+                assert rel(np.asarray(xm), np.asarray(x64)) < 1e-7
+
+
+def test_u1_mixed_precision_trajectories(port):
+    """Mixed-precision solves inside the U(1) sigma and pi trajectories: dH and
+    the evolved fields agree with the FP64 path to the solver tolerance."""
+    import gn_b200 as G
+    L = 16
+    V = L ** 3
+    rng, sigma0, pi0 = _u1_fields(L, 91)
+    gauss = rng.normal(size=3 * V)
+    pairs = rng.normal(size=(V // 2, 2))
+    unif = np.array([0.5])
+    res = {}
+    for prec in (G.GN_PREC_FP64, G.GN_PREC_MIXED):
+        with G.Lattice(L) as lat:
+            lat.load_sigma(sigma0)
+            lat.load_pi(pi0)
+            gp, up = port.replay(gauss, unif)
+            r = lat.trajectory(0.85, 0.05, 4, gp, up, tol_medium=1e-10, tol_high=1e-10, relative=True,
+                               precision=prec)
+            it = iter(pairs)
+
+            def pair(a, b):
+                a[0], b[0] = next(it)
+            gp, up = port.replay(gauss, unif)
+            rp = lat.trajectory_pi(0.85, 0.05, 4, pair, gp, up, tol_high=1e-10, relative=True, precision=prec)
+            res[prec] = (r, rp, lat.store_sigma()[0], lat.store_pi()[0])
+    a, b = res[G.GN_PREC_FP64], res[G.GN_PREC_MIXED]
+    for q in (0, 1):
+        assert a[q]["ok"] and b[q]["ok"]
+        assert abs(a[q]["dH"] - b[q]["dH"]) < 1e-6
+        assert a[q]["accepted"] == b[q]["accepted"]
+        assert b[q]["reliable_updates"] > 0
+    assert rel(b[2], a[2]) < 1e-8 and rel(b[3], a[3]) < 1e-8
