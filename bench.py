@@ -584,12 +584,14 @@ def serve_bench(G, nreq=600, rate=200.0, warm=24, seed=5, precision=None):
 
 
 def u1_case(G, dev, L=64, md_steps=10, eps=0.05, pi_steps=10, tol=1e-10, reps=2):
-    """The U(1) model (PI_INTERACTION) in FP64 at L = 64: ms per sigma trajectory
+    """The U(1) model (PI_INTERACTION) at L = 64: ms per sigma trajectory
     (LFMN2VF md_steps x eps with the complex M, every solve to a true relative
-    residual of tol) and per LeapFrog2Pi (pi_steps x eps), against the Z2
-    model's FP64 trajectory on the same sigma and draws.  Draws resident on
-    the device (gn_trajectory_device; P_pi and chi written before the pi
-    trajectory), CUDA events around each trajectory, `reps` after one warm-up."""
+    residual of tol) and per LeapFrog2Pi (pi_steps x eps), in FP64 and in
+    mixed precision (FP32 inner iterations, FP64 reliable updates, dH in
+    FP64), against the Z2 model's FP64 trajectory on the same sigma and draws.
+    Draws resident on the device (gn_trajectory_device; P_pi and chi written
+    before the pi trajectory), CUDA events around each trajectory, `reps`
+    after one warm-up."""
     import torch
     V = L ** 3
     rng = np.random.default_rng(64)
@@ -599,7 +601,7 @@ def u1_case(G, dev, L=64, md_steps=10, eps=0.05, pi_steps=10, tol=1e-10, reps=2)
     chi_c = np.zeros(4 * V)
     chi_c[0:V], chi_c[2 * V:3 * V] = rng.normal(size=V), rng.normal(size=V)
     ppi = rng.normal(size=V)
-    out = {"L": L, "precision": "fp64"}
+    out = {"L": L}
     lat = G.Lattice(L, dev.index)
     stream = torch.cuda.ExternalStream(lat.stream, device=dev)
 
@@ -616,7 +618,9 @@ def u1_case(G, dev, L=64, md_steps=10, eps=0.05, pi_steps=10, tol=1e-10, reps=2)
         return min(ts), res
 
     params = dict(tol_medium=tol, tol_high=tol, relative=True)
-    for name, u1 in (("z2_sigma_trajectory", False), ("u1_sigma_trajectory", True)):
+    cases = (("z2_sigma_trajectory", False, G.GN_PREC_FP64), ("u1_sigma_trajectory", True, G.GN_PREC_FP64),
+             ("u1_sigma_trajectory_mixed", True, G.GN_PREC_MIXED))
+    for name, u1, prec in cases:
         def run():
             lat.load_sigma(sigma)
             if u1:
@@ -624,20 +628,25 @@ def u1_case(G, dev, L=64, md_steps=10, eps=0.05, pi_steps=10, tol=1e-10, reps=2)
             else:
                 lat.set_u1(False)
             base = draws.data_ptr()
-            return lat.trajectory_device(base, base + 8 * V, BETA_S, eps, md_steps, None, precision=G.GN_PREC_FP64,
-                                         **params)
+            return lat.trajectory_device(base, base + 8 * V, BETA_S, eps, md_steps, None, precision=prec, **params)
         ms, r = timed(run)
         out[name] = {"ms": round(ms, 2), "cg_iterations": r["cg_iterations"], "dH": r["dH"]}
 
-    def run_pi():
-        lat.load_sigma(sigma)
-        lat.load_pi(pi)
-        lat.write_state(G.GN_F_PI_P, ppi)
-        lat.write_state(G.GN_F_CHI_C, chi_c)
-        return lat.trajectory_pi(BETA_S, eps, pi_steps, None, None, None, tol_high=tol, relative=True)
-    ms, r = timed(run_pi)
-    out["u1_pi_trajectory"] = {"ms": round(ms, 2), "cg_iterations": r["cg_iterations"], "dH": r["dH"]}
+    for name, prec in (("u1_pi_trajectory", G.GN_PREC_FP64), ("u1_pi_trajectory_mixed", G.GN_PREC_MIXED)):
+        def run_pi():
+            lat.load_sigma(sigma)
+            lat.load_pi(pi)
+            lat.write_state(G.GN_F_PI_P, ppi)
+            lat.write_state(G.GN_F_CHI_C, chi_c)
+            return lat.trajectory_pi(BETA_S, eps, pi_steps, None, None, None, tol_high=tol, relative=True,
+                                     precision=prec)
+        ms, r = timed(run_pi)
+        out[name] = {"ms": round(ms, 2), "cg_iterations": r["cg_iterations"], "dH": r["dH"]}
     lat.close()
+    for kind in ("sigma", "pi"):
+        a, b = out[f"u1_{kind}_trajectory"], out[f"u1_{kind}_trajectory_mixed"]
+        out[f"u1_{kind}_mixed_speedup"] = round(a["ms"] / b["ms"], 3)
+        out[f"u1_{kind}_mixed_abs_ddH"] = abs(a["dH"] - b["dH"])
     # the reference's own complex solve on one host core, beside ours
     nsol = solves_per_trajectory(md_steps)
     out["gpu_ms_per_solve"] = round(out["u1_sigma_trajectory"]["ms"] / nsol, 3)
