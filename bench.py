@@ -126,7 +126,7 @@ class Clocks:
             os.close(fd)
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-i", str(self.device), "-lms", "200"], stdout=self.fh,
+                                          "-i", str(self.device), "-lms", "50"], stdout=self.fh,
                                          stderr=subprocess.DEVNULL)
             # wait for the first sample: the sampler's start-up (NVML initialisation)
             # must not fall inside a timed region

@@ -114,3 +114,37 @@ def test_mixed_trajectory_matches_fp64(port):
     assert abs(r64["dH"] - rmx["dH"]) < 1e-6
     assert rel(smx, s64) < 1e-8
     assert rmx["reliable_updates"] > 0
+
+
+@pytest.mark.parametrize("name", ["readme", "reject"])
+def test_reference_chains(golden, name):
+    """The reference's own chains at L = 8 (tests/golden/make_chain.py): 1000
+    trajectories at the README configuration and 500 at eps = 1.0, where a
+    quarter are rejected.  The GPU chain draws from the same reference build's
+    dSFMT stream (Gauss1, Casuale), seeded the same way, so every accept
+    decision is the same, dH agrees per trajectory (the chain carries the
+    sum-order differences of the solves forward: 1e-8 absolute), and the
+    final sigma to 1e-8."""
+    import gn_b200 as G
+    from oracle import build_ref
+    from oracle.oracle import Ref
+    g = golden("golden_L8_chains.npz")
+    L = int(g["L"])
+    if not build_ref.lib_path(L).exists() and not build_ref.available():
+        pytest.skip("no compiled reference harness")
+    eps, steps = float(g[f"{name}_eps"]), int(g[f"{name}_steps"])
+    ref = Ref(L)
+    ref.init(int(g["seed"]), float(g["beta_s"]), eps, steps)
+    gp, up = ref.fn_ptrs()
+    dH, acc = g[f"{name}_dH"], g[f"{name}_accepted"]
+    with G.Lattice(L) as lat:
+        lat.load_sigma(g[f"{name}_sigma0"])
+        worst = 0.0
+        for t in range(len(dH)):
+            r = lat.trajectory(float(g["beta_s"]), eps, steps, gp, up)
+            assert r["ok"] == int(g[f"{name}_ok"][t]), t
+            assert r["accepted"] == int(acc[t]), t
+            worst = max(worst, abs(r["dH"] - dH[t]))
+        s, _ = lat.store_sigma()
+    assert worst < 1e-8, worst
+    assert rel(s, g[f"{name}_sigma_final"]) < 1e-8
