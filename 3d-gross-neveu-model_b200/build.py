@@ -2,7 +2,9 @@
 
 Compiles csrc/*.cu with nvcc into lib/libgn_b200.so (the C-ABI of
 include/gn_b200.h) and csrc/dropin.cpp into lib/libgn_dropin.so (the
-reference-signature layer of include/gn_dropin.h).  The FP64 translation unit
+reference-signature layer of include/gn_dropin.h) and, with GN_DROPIN_PI, into
+lib/libgn_dropin_pi.so (the same layer for the PI_INTERACTION build,
+include/gn_dropin_pi.h).  The FP64 translation unit
 engine.cu is compiled with --fmad=false so that the FP64 kernels round like the
 reference's x86-64 build (multiply, then add).
 
@@ -38,6 +40,7 @@ UNITS = {
 }
 CORE_LIB = LIB / "libgn_b200.so"
 DROPIN_LIB = LIB / "libgn_dropin.so"
+DROPIN_PI_LIB = LIB / "libgn_dropin_pi.so"  # the same source with GN_DROPIN_PI: the U(1) (PI_INTERACTION) build
 
 
 def _nvcc() -> str:
@@ -75,9 +78,10 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     if force or _stale(CORE_LIB, objs):
         subprocess.run([_nvcc(), *ARCH, "-shared", "-o", str(CORE_LIB), *map(str, objs), "-lcudart"], check=True)
     dropin = CSRC / "dropin.cpp"
-    if dropin.exists() and (force or _stale(DROPIN_LIB, [dropin, CORE_LIB, *headers])):
-        subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", f"-I{INCLUDE}", "-o", str(DROPIN_LIB),
-                        str(dropin), f"-L{LIB}", "-lgn_b200", "-Wl,-rpath,$ORIGIN", "-ldl"], check=True)
+    for lib, defs in ((DROPIN_LIB, []), (DROPIN_PI_LIB, ["-DGN_DROPIN_PI"])):
+        if dropin.exists() and (force or _stale(lib, [dropin, CORE_LIB, *headers])):
+            subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-Wall", *defs, f"-I{INCLUDE}", "-o",
+                            str(lib), str(dropin), f"-L{LIB}", "-lgn_b200", "-Wl,-rpath,$ORIGIN", "-ldl"], check=True)
     return CORE_LIB
 
 

@@ -593,6 +593,18 @@ int gn_trajectory_device(gn_context *ctx, const gn_hmc_params *params, const dou
   return guarded(ctx, [&](gn::Engine &E) { return E.trajectory(*params, nullptr, uniform, P, chi, res); });
 }
 
+int gn_md_evolve(gn_context *ctx, const gn_hmc_params *params, gn_traj_result *res) {
+  if (!params || !res) return fail(GN_ERR_ARG, "null pointer");
+  return guarded(ctx, [&](gn::Engine &E) {
+    struct KeepPhi {  // restored on every exit
+      bool &flag;
+      explicit KeepPhi(bool &f) : flag(f) { flag = true; }
+      ~KeepPhi() { flag = false; }
+    } keep(E.keep_phi);
+    return E.trajectory(*params, nullptr, nullptr, nullptr, nullptr, res);
+  });
+}
+
 long long gn_launch_count(gn_context *ctx) { return (ctx && ctx->eng) ? ctx->eng->launches : 0; }
 
 int gn_flush_l2(gn_context *ctx) {

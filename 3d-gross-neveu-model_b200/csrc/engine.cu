@@ -329,7 +329,7 @@ int Engine::trajectory(const gn_hmc_params &hp, double (*gauss)(void), double (*
     if (pre_chi)
       check(cudaMemcpyAsync(chi_, pre_chi, 2 * V * sizeof(double), cudaMemcpyDeviceToDevice, stream_), "copy chi");
   }
-  dirac(sm_, chi_, phi_, 2, GN_OP_M);  // phi_f = M chi_f (both flavours as planes)
+  if (!keep_phi) dirac(sm_, chi_, phi_, 2, GN_OP_M);  // phi_f = M chi_f (both flavours as planes)
   double *sigma_copy = scratch_[3];
   check(cudaMemcpyAsync(sigma_copy, sigma(), V * sizeof(double), cudaMemcpyDeviceToDevice, stream_), "copy sigma");
   auto restore = [&]() {

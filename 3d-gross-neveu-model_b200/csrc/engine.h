@@ -83,6 +83,9 @@ class Engine {
   // energy and the condensate (set by gn_set_parity_mode and by the
   // operations run with precision GN_PREC_FP64_EXACT).
   bool exact = false;
+  // trajectories run the MD alone on the resident P and phi (phi is not
+  // formed from chi), as the reference's EvolveSigmaInTime* helpers
+  bool keep_phi = false;
   int reliable_every = 100;  // mixed precision: a reliable update at least every this many iterations
 
   // One trajectory on the resident state; see gn_trajectory in gn_b200.h.

@@ -166,7 +166,7 @@ int Engine::trajectory_u1(const gn_hmc_params &hp, double (*gauss)(void), double
     if (pre_P) check(cudaMemcpyAsync(P_, pre_P, V * sizeof(double), cudaMemcpyDeviceToDevice, stream_), "copy P");
     if (pre_chi) load_chi(*this, nullptr, pre_chi);
   }
-  dirac_cm(sm_, pm_, chi_c_, phi_c_, 2, GN_OP_M);
+  if (!keep_phi) dirac_cm(sm_, pm_, chi_c_, phi_c_, 2, GN_OP_M);
   double *sigma_copy = scratch_[3];
   check(cudaMemcpyAsync(sigma_copy, sigma(), V * sizeof(double), cudaMemcpyDeviceToDevice, stream_), "copy sigma");
   auto restore = [&]() {

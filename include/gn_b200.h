@@ -305,6 +305,18 @@ GN_API int gn_write_state(gn_context *ctx, int field, const double *in);
 GN_API int gn_trajectory(gn_context *ctx, const gn_hmc_params *params, double (*gauss)(void), double (*uniform)(void),
                   gn_traj_result *res);
 
+/* The molecular dynamics of one trajectory without draws and without the
+ * Metropolis test, as the reference's EvolveSigmaInTimeLF2 /
+ * ...MinimumNormLF2 / ...MinimumNormSigmaVelocityFirst helpers
+ * (moleculardynamics.c:1460-1625, used by its DEBUG_LF2_SIGMA reversibility
+ * check): from the resident sigma, P (GN_F_P) and phi (GN_F_PHI; in the U(1)
+ * model GN_F_PHI_C), with params->integrator's schedule as gn_trajectory runs
+ * it.  phi is not formed from chi.  res->H0, H1, dH are the energies before
+ * and after; sigma and P are left evolved (res->accepted = 1), or restored
+ * when a solve fails (GN_NOT_CONVERGED).  Flipping P and evolving again
+ * retraces the trajectory. */
+GN_API int gn_md_evolve(gn_context *ctx, const gn_hmc_params *params, gn_traj_result *res);
+
 /* ---- device-resident entry points ------------------------------------- */
 
 /* The context's CUDA stream (a cudaStream_t); every device-pointer call below

@@ -324,6 +324,19 @@ int gnref_layout(long *out)
     out[n++] = sizeof(struct Forcesigma);
     out[n++] = sizeof(struct Momentasigma);
     out[n++] = sizeof(struct RandomVec);
+    /* the U(1) model's members and structs */
+    out[n++] = offsetof(struct Lattice, pi);
+    out[n++] = offsetof(struct Lattice, epsilon_pi);
+    out[n++] = offsetof(struct Lattice, pimass);
+    out[n++] = offsetof(struct Lattice, distance_pi);
+    out[n++] = offsetof(struct Lattice, done_pi);
+    out[n++] = offsetof(struct Info, epsilon_pi_HMC);
+    out[n++] = offsetof(struct Info, steps_pi_HMC);
+    out[n++] = offsetof(struct Info, hybrid_accepted_pi);
+    out[n++] = offsetof(struct Info, hybrid_done_acceptance_pi);
+    out[n++] = offsetof(struct Info, story_pi);
+    out[n++] = sizeof(struct Forcepi);
+    out[n++] = sizeof(struct Momentapi);
     return n;
 }
 

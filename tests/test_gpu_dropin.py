@@ -60,3 +60,47 @@ def test_dropin_exact_mode_is_bit_identical():
     assert [tuple(c) for c in out["counters"]] == [tuple(c) for c in g["counters"]]
     c = dict(np.load(GOLD / "golden_L8_cond.npz"))
     assert out["condensate"] == [float(v) for v in c["out"]]
+
+
+@pytest.mark.parametrize("L", [4, 8])
+def test_dropin_pi_under_reference_harness(L):
+    """libgn_dropin_pi.so under the reference's PI_INTERACTION build: the
+    reference's harness calls its own U(1) functions by name and gets the
+    GPU's, with the reference's RNG.  Results against the fixtures the
+    reference made alone, to the tolerances of tests/test_gpu_u1.py."""
+    from oracle import build_ref
+    if not build_ref.lib_path(L, 0, build_ref.PI_TAG).exists():
+        pytest.skip("reference PI build not present")
+    gold = GOLD / f"golden_L{L}_u1.npz"
+    r = subprocess.run([sys.executable, str(ROOT / "tests" / "dropin_driver_pi.py"), str(gold)], capture_output=True,
+                       text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = [ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1]
+    out = json.loads(line)
+    g = dict(np.load(gold))
+    cx = lambda a: np.array(a[0]) + 1j * np.array(a[1])  # noqa: E731
+
+    def rel(a, b):
+        return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
+    assert np.array_equal(np.array(out["pm"]), g["pm"])
+    np.testing.assert_allclose(out["sigma_obs"], g["sigma_obs"], rtol=1e-12, atol=1e-16)
+    assert np.array_equal(cx(out["M_psi"]), g["M_psi"])
+    assert rel(cx(out["Mt_psi"]), g["Mt_psi"]) < 1e-15
+    assert np.array_equal(cx(out["sub_res"]), g["sub_res"])
+    assert out["cg_ok"] and tuple(out["cg_counters"]) == tuple(g["cg_counters"])
+    assert rel(cx(out["cg_x"]), g["cg_x"]) < 1e-11
+    assert out["force_ok"] and tuple(out["force_counters"]) == tuple(g["force_counters"])
+    assert rel(np.array(out["force_F"]), g["force_F"]) < 1e-11
+    assert rel(np.stack([cx(v) for v in out["force_X"]]), g["force_X"]) < 1e-11
+    assert out["piforce_ok"]
+    assert rel(np.array(out["piforce_F"]), g["piforce_F"]) < 1e-11
+    assert rel(np.stack([cx(v) for v in out["piforce_Y"]]), g["piforce_Y"]) < 1e-11
+    assert abs(out["energy_H"] - g["energy_H"]) < 1e-13 * abs(g["energy_H"])
+    assert abs(out["energy_Hpi"] - g["energy_Hpi"]) < 1e-13 * abs(g["energy_Hpi"])
+    for name in ("traj", "trajpi"):
+        assert out[f"{name}_ok"]
+        assert abs(out[f"{name}_dH"] - float(g[f"{name}_dH"])) < 1e-10
+        assert out[f"{name}_accepted"] == int(g[f"{name}_accepted"])
+        assert tuple(out[f"{name}_counters"]) == tuple(g[f"{name}_counters"])
+        assert rel(np.array(out[f"{name}_sigma"]), g[f"{name}_sigma"]) < 1e-11
+        assert rel(np.array(out[f"{name}_pi"]), g[f"{name}_pi"]) < 1e-11

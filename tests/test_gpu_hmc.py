@@ -148,3 +148,65 @@ def test_reference_chains(golden, name):
         s, _ = lat.store_sigma()
     assert worst < 1e-8, worst
     assert rel(s, g[f"{name}_sigma_final"]) < 1e-8
+
+
+@pytest.mark.parametrize("L", [8, 16])
+def test_chi_identity(port, L):
+    """phi^T (M M^T)^-1 phi = chi^T chi for phi = M chi (the reference's
+    DEBUG_STARTING_ENERGY_HMC check, moleculardynamics.c:1273-1275 with
+    ComputeFullEnergyForSigmaWithChi :324-344): the starting energy of a
+    trajectory equals sum P^2/2 + sum chi^2/2 + (N_f beta_s/4) sum sigma^2 to
+    the tolerance of its first solve."""
+    import gn_b200 as G
+    V = L ** 3
+    rng = np.random.default_rng(300 + L)
+    sigma = rng.normal(0, np.sqrt(2 / (4 * 0.85)), V)
+    draws = rng.normal(size=3 * V)
+    gp, _ = port.replay(draws, np.zeros(0))
+    with G.Lattice(L) as lat:
+        lat.load_sigma(sigma)
+        r = lat.trajectory(0.85, 0.05, 2, gp, None, tol_medium=1e-12, tol_high=1e-12, relative=True)
+    P, chi = draws[:V], draws[V:]
+    h0 = (0.5 * np.dot(P, P) + 0.5 * np.dot(chi, chi)) + 0.85 * np.dot(sigma, sigma)
+    assert r["ok"] == 1
+    assert abs(r["H0"] - h0) < 1e-10 * abs(h0)
+
+
+@pytest.mark.parametrize("model", ["z2", "u1"])
+@pytest.mark.parametrize("integrator", [0, 1, 2])
+def test_md_reversibility(port, model, integrator):
+    """The reference's DEBUG_LF2_SIGMA check (moleculardynamics.c:1371-1382):
+    evolve (sigma, P) with phi fixed, flip P, evolve again: sigma and -P come
+    back, and the two energy changes cancel, to the tolerance of the solves
+    (true relative residual 1e-12)."""
+    import gn_b200 as G
+    L = 8
+    V = L ** 3
+    rng = np.random.default_rng(40 + integrator)
+    sigma0 = rng.normal(0, np.sqrt(2 / (4 * 0.85)), V)
+    pi0 = rng.normal(0, np.sqrt(2 / (4 * 0.85)), V)
+    P0 = rng.normal(size=V)
+    chi = rng.normal(size=(2, V))
+    kw = dict(integrator=integrator, tol_medium=1e-12, tol_high=1e-12, relative=True)
+    with G.Lattice(L) as lat:
+        lat.load_sigma(sigma0)
+        sm = lat.store_sigma()[1]
+        if model == "u1":
+            lat.load_pi(pi0)
+            phi = lat.dirac_u1(sm, lat.store_pi()[1], chi.astype(complex), G.GN_OP_M)
+            lat.write_state(G.GN_F_PHI_C, G.Lattice._cplanes(phi)[0])
+        else:
+            lat.write_state(G.GN_F_PHI, np.stack([port.dirac(L, sm, chi[f], 0) for f in range(2)]))
+        lat.write_state(G.GN_F_P, P0)
+        r1 = lat.md_evolve(0.85, 0.1, 4, **kw)
+        s1 = lat.store_sigma()[0]
+        lat.write_state(G.GN_F_P, -lat.read_state(G.GN_F_P))
+        r2 = lat.md_evolve(0.85, 0.1, 4, **kw)
+        s2 = lat.store_sigma()[0]
+        P2 = lat.read_state(G.GN_F_P)
+    assert r1["ok"] == 1 and r2["ok"] == 1 and r1["accepted"] == 1
+    assert rel(s1, sigma0) > 1e-3  # it moved
+    assert rel(s2, sigma0) < 1e-9
+    assert rel(-P2, P0) < 1e-9
+    assert abs(r1["dH"] + r2["dH"]) < 1e-9
+    assert abs(r2["H1"] - r1["H0"]) < 1e-9 * abs(r1["H0"])
