@@ -176,8 +176,7 @@ __device__ __forceinline__ void mixed_solve(const MixedArgs &a, Team &team, Sync
         }
       }
     });
-    zero_acc();
-    ok = end_phase<1>(acc, sh, team);
+    ok = team_barrier(sh, team);  // t is complete: no sums needed
     zero_acc();
     if (ok) {
       for_units(NI64, s_every, team, [&](int k, uint32_t j) {
@@ -386,7 +385,11 @@ __device__ __forceinline__ void mixed_solve(const MixedArgs &a, Team &team, Sync
           s_r2[k] = gn;
           if (rn > s_rmax[k]) s_rmax[k] = rn;
           if (rn < s_tau[k] || rn < a.delta * s_rmax[k] || s_since[k] >= a.n_ru || !(rn == rn)) {
-            s_ru[k] = 1;  // the true residual replaces r^; a later S1 takes the step
+            // the true residual replaces r^; a later S1 takes the step.  (A step
+            // in this pass, from u^ of the drifted r^, would leave a^ != A p^ by
+            // A (r - r^), an error that a^ and p^ carry on and that grows from
+            // one refresh to the next.)
+            s_ru[k] = 1;
           } else {
             double bt = 0.0, den = dn;
             if (!s_first[k]) {
@@ -574,8 +577,7 @@ __device__ __forceinline__ void mixed_solve(const MixedArgs &a, Team &team, Sync
           }
         }
       });
-      zero_acc();
-      ok = end_phase<1>(acc, sh, team);
+      ok = team_barrier(sh, team);  // t is complete: no sums needed
       if (!ok) break;
       // D: x += x^, x^ = 0, r = b - M t, r^ = (float) r
       zero_acc();
