@@ -384,11 +384,11 @@ __device__ __forceinline__ void mixed_solve(const MixedArgs &a, Team &team, Sync
           const double rn = sqrt(gn);
           s_r2[k] = gn;
           if (rn > s_rmax[k]) s_rmax[k] = rn;
-          if (rn < s_tau[k] || rn < a.delta * s_rmax[k] || s_since[k] >= a.n_ru || !(rn == rn)) {
-            // the true residual replaces r^; a later S1 takes the step.  (A step
-            // in this pass, from u^ of the drifted r^, would leave a^ != A p^ by
-            // A (r - r^), an error that a^ and p^ carry on and that grows from
-            // one refresh to the next.)
+          if (rn < s_tau[k] || !(rn == rn)) {
+            // r^ says converged (or is not finite): the true residual decides,
+            // and this pass takes no step.  (A step from u^ of the drifted r^
+            // after the refresh would leave a^ != A p^ by A (r - r^), an error
+            // that a^ and p^ carry on and that grows from one refresh to the next.)
             s_ru[k] = 1;
           } else {
             double bt = 0.0, den = dn;
@@ -406,6 +406,9 @@ __device__ __forceinline__ void mixed_solve(const MixedArgs &a, Team &team, Sync
             s_rr[k] = gn;
             s_since[k]++;
             s_step[k] = 1;
+            // a scheduled refresh runs after this pass's step (S2 comes before
+            // C, D in the split scheme), so the next S1 starts from the true r
+            if (rn < a.delta * s_rmax[k] || s_since[k] >= a.n_ru) s_ru[k] = 1;
           }
         }
       }
@@ -520,6 +523,79 @@ __device__ __forceinline__ void mixed_solve(const MixedArgs &a, Team &team, Sync
       if (threadIdx.x == 0 && team.brank == 0) atomicExch(team.err, 2);
       ok = false;
       break;
+    }
+    if (split && s_stp.n > 0) {
+      // S2: a^ = M u^ + beta a^, p^ = r^ + beta p^, x^ += alpha p^, r^ -= alpha a^
+      for_units(NI, s_stp, team, [&](int k, uint32_t j) {
+        const RowItem ri = make_item<W>(g, j);
+        float smi[W];
+        vload<float, W>(a.sm32 + ri.own, smi);
+        const float alpha = float(s_alpha[k]), beta = float(s_beta[k]);
+        const float *uk = pick<NR>(a.uh, k);
+        if constexpr (CM) {
+          Nb<float> nr[W], ni[W];
+          float b[W], w[2][W];
+          gather_item<float, W>(ri, uk, nr);
+          gather_item<float, W>(ri, uk + V, ni);
+          item_eps_pm<float, W>(g, ri, a.pm32, b);
+          item_M_cm<float, W>(ri, smi, b, nr, ni, w[0], w[1]);
+#pragma unroll
+          for (int c = 0; c < 2; c++) {
+            const size_t o = size_t(c) * V + ri.own;
+            float av[W], pv[W], xv[W], rv[W];
+            float *const ak = pick<NR>(a.ah, k) + o;
+            float *const pk = pick<NR>(a.ph, k) + o;
+            float *const xk = pick<NR>(a.xh, k) + o;
+            float *const rk = pick<NR>(a.rh, k) + o;
+            vload<float, W>(ak, av);
+            vload<float, W>(pk, pv);
+            vload<float, W>(xk, xv);
+            vload<float, W>(rk, rv);
+#pragma unroll
+            for (int e = 0; e < W; e++) {
+              av[e] = fmaf(beta, av[e], w[c][e]);
+              pv[e] = fmaf(beta, pv[e], rv[e]);
+              xv[e] = fmaf(alpha, pv[e], xv[e]);
+              rv[e] = fmaf(-alpha, av[e], rv[e]);
+            }
+            vstore<float, W>(ak, av);
+            vstore<float, W>(pk, pv);
+            vstore<float, W>(xk, xv);
+            vstore<float, W>(rk, rv);
+          }
+        } else {
+#pragma unroll
+          for (int c = 0; c < NC; c++) {
+            const size_t off = size_t(c) * V;
+            const size_t o = off + ri.own;
+            Nb<float> n[W];
+            float w[W], av[W], pv[W], xv[W], rv[W];
+            gather_item<float, W>(ri, uk + off, n);
+            float *const ak = pick<NR>(a.ah, k) + o;
+            float *const pk = pick<NR>(a.ph, k) + o;
+            float *const xk = pick<NR>(a.xh, k) + o;
+            float *const rk = pick<NR>(a.rh, k) + o;
+            vload<float, W>(ak, av);
+            vload<float, W>(pk, pv);
+            vload<float, W>(xk, xv);
+            vload<float, W>(rk, rv);
+            item_M<float, W>(ri, smi, n, w);
+#pragma unroll
+            for (int e = 0; e < W; e++) {
+              av[e] = fmaf(beta, av[e], w[e]);
+              pv[e] = fmaf(beta, pv[e], rv[e]);
+              xv[e] = fmaf(alpha, pv[e], xv[e]);
+              rv[e] = fmaf(-alpha, av[e], rv[e]);
+            }
+            vstore<float, W>(ak, av);
+            vstore<float, W>(pk, pv);
+            vstore<float, W>(xk, xv);
+            vstore<float, W>(rk, rv);
+          }
+        }
+      });
+      ok = team_barrier(sh, team);
+      if (!ok) break;
     }
     if (s_upd.n > 0) {
       // C: t = M^T (x + x^) in FP64
@@ -678,79 +754,6 @@ __device__ __forceinline__ void mixed_solve(const MixedArgs &a, Team &team, Sync
       __syncthreads();
       if (threadIdx.x == 0) sys_list_from(s_run, s_active, a.nrhs);
       __syncthreads();
-    }
-    if (split && s_stp.n > 0) {
-      // S2: a^ = M u^ + beta a^, p^ = r^ + beta p^, x^ += alpha p^, r^ -= alpha a^
-      for_units(NI, s_stp, team, [&](int k, uint32_t j) {
-        const RowItem ri = make_item<W>(g, j);
-        float smi[W];
-        vload<float, W>(a.sm32 + ri.own, smi);
-        const float alpha = float(s_alpha[k]), beta = float(s_beta[k]);
-        const float *uk = pick<NR>(a.uh, k);
-        if constexpr (CM) {
-          Nb<float> nr[W], ni[W];
-          float b[W], w[2][W];
-          gather_item<float, W>(ri, uk, nr);
-          gather_item<float, W>(ri, uk + V, ni);
-          item_eps_pm<float, W>(g, ri, a.pm32, b);
-          item_M_cm<float, W>(ri, smi, b, nr, ni, w[0], w[1]);
-#pragma unroll
-          for (int c = 0; c < 2; c++) {
-            const size_t o = size_t(c) * V + ri.own;
-            float av[W], pv[W], xv[W], rv[W];
-            float *const ak = pick<NR>(a.ah, k) + o;
-            float *const pk = pick<NR>(a.ph, k) + o;
-            float *const xk = pick<NR>(a.xh, k) + o;
-            float *const rk = pick<NR>(a.rh, k) + o;
-            vload<float, W>(ak, av);
-            vload<float, W>(pk, pv);
-            vload<float, W>(xk, xv);
-            vload<float, W>(rk, rv);
-#pragma unroll
-            for (int e = 0; e < W; e++) {
-              av[e] = fmaf(beta, av[e], w[c][e]);
-              pv[e] = fmaf(beta, pv[e], rv[e]);
-              xv[e] = fmaf(alpha, pv[e], xv[e]);
-              rv[e] = fmaf(-alpha, av[e], rv[e]);
-            }
-            vstore<float, W>(ak, av);
-            vstore<float, W>(pk, pv);
-            vstore<float, W>(xk, xv);
-            vstore<float, W>(rk, rv);
-          }
-        } else {
-#pragma unroll
-          for (int c = 0; c < NC; c++) {
-            const size_t off = size_t(c) * V;
-            const size_t o = off + ri.own;
-            Nb<float> n[W];
-            float w[W], av[W], pv[W], xv[W], rv[W];
-            gather_item<float, W>(ri, uk + off, n);
-            float *const ak = pick<NR>(a.ah, k) + o;
-            float *const pk = pick<NR>(a.ph, k) + o;
-            float *const xk = pick<NR>(a.xh, k) + o;
-            float *const rk = pick<NR>(a.rh, k) + o;
-            vload<float, W>(ak, av);
-            vload<float, W>(pk, pv);
-            vload<float, W>(xk, xv);
-            vload<float, W>(rk, rv);
-            item_M<float, W>(ri, smi, n, w);
-#pragma unroll
-            for (int e = 0; e < W; e++) {
-              av[e] = fmaf(beta, av[e], w[e]);
-              pv[e] = fmaf(beta, pv[e], rv[e]);
-              xv[e] = fmaf(alpha, pv[e], xv[e]);
-              rv[e] = fmaf(-alpha, av[e], rv[e]);
-            }
-            vstore<float, W>(ak, av);
-            vstore<float, W>(pk, pv);
-            vstore<float, W>(xk, xv);
-            vstore<float, W>(rk, rv);
-          }
-        }
-      });
-      ok = team_barrier(sh, team);
-      if (!ok) break;
     }
   }
   // ---------------------------------------------------------------- results
