@@ -37,6 +37,7 @@ UNITS = {
     "serve.cu": ["--fmad=false"],
     "checkpoint.cu": [],
     "u1.cu": ["--fmad=false"],
+    "selftest.cu": [],
 }
 CORE_LIB = LIB / "libgn_b200.so"
 DROPIN_LIB = LIB / "libgn_dropin.so"

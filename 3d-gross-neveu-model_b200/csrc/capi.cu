@@ -115,6 +115,10 @@ void gn_request_abort(gn_context *ctx, int on) {
   if (ctx && ctx->eng) *(volatile int *)ctx->eng->abort_flag_host() = on;
 }
 
+int gn_selftest_wait_timeout(gn_context *ctx) {
+  return guarded(ctx, [&](gn::Engine &E) { return E.selftest_wait_timeout(); });
+}
+
 int gn_sigma_mass(gn_context *ctx, const double *sigma, double *sigmamass) {
   if (!sigma || !sigmamass) return fail(GN_ERR_ARG, "null pointer");
   return guarded(ctx, [&](gn::Engine &E) {

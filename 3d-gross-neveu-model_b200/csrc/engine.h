@@ -127,6 +127,10 @@ class Engine {
   int trajectory_pi(const gn_hmc_params &hp, void (*gauss_pair)(double *, double *), double (*gauss)(void),
                     double (*uniform)(void), gn_traj_result *res);
 
+  // failure-detection self-test: a team barrier whose partner block never
+  // arrives runs out of polls; returns GN_ERR_TIMEOUT (selftest.cu)
+  int selftest_wait_timeout();
+
   // host staging (pinned), at least 4*V doubles
   double *host_stage() { return h_stage_; }
   int *abort_flag_host() { return h_abort_; }

@@ -28,6 +28,7 @@ GN_F_P, GN_F_F, GN_F_CHI, GN_F_PHI, GN_F_X, GN_F_Y, GN_F_SIGMA, GN_F_SM = range(
 # the U(1) model's resident fields: pi momenta and force (V), complex chi, phi,
 # X, Y of both flavours (4V), and for field_ptr pi and pimass
 GN_F_PI_P, GN_F_PI_F, GN_F_CHI_C, GN_F_PHI_C, GN_F_X_C, GN_F_Y_C, GN_F_PI, GN_F_PM = range(8, 16)
+GN_ERR_ARG, GN_ERR_CUDA, GN_ERR_TIMEOUT, GN_ERR_ABORTED, GN_ERR_NO_DEVICE = -1, -2, -3, -4, -5
 GN_ERR_IO, GN_ERR_NOT_FOUND, GN_ERR_FORMAT = -6, -7, -8
 STATUS_NAMES = {0: "GN_OK", 1: "GN_NOT_CONVERGED", -1: "GN_ERR_ARG", -2: "GN_ERR_CUDA", -3: "GN_ERR_TIMEOUT",
                 -4: "GN_ERR_ABORTED", -5: "GN_ERR_NO_DEVICE", -6: "GN_ERR_IO", -7: "GN_ERR_NOT_FOUND",
@@ -135,6 +136,7 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
         "gn_last_error": ([], C.c_char_p),
         "gn_volume": ([v], C.c_longlong),
         "gn_request_abort": ([v, C.c_int], None),
+        "gn_selftest_wait_timeout": ([v], C.c_int),
         "gn_sigma_mass": ([v, _dp, _dp], C.c_int),
         "gn_dirac": ([v, _dp, _dp, _dp, C.c_int, C.c_int], C.c_int),
         "gn_cg": ([v, _dp, _dp, _dp, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_longlong, C.c_int,
@@ -479,6 +481,10 @@ class Lattice:
 
     def request_abort(self, on=True):
         self.lib.gn_request_abort(self.ctx, int(on))
+
+    def selftest_wait_timeout(self):
+        """Status of the failure-detection self-test (GN_ERR_TIMEOUT when the bounded wait works)."""
+        return self.lib.gn_selftest_wait_timeout(self.ctx)
 
     # ---- device-resident entry points (pointers are ints)
     @property

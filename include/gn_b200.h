@@ -98,8 +98,16 @@ GN_API int gn_create(gn_context **ctx, int L, int device);
 GN_API void gn_destroy(gn_context *ctx);
 GN_API const char *gn_last_error(void);
 GN_API long long gn_volume(const gn_context *ctx);
-/* Ask a running solve on this context to stop (from another host thread). */
+/* Ask a running solve on this context to stop (from another host thread).
+ * The solve returns GN_ERR_ABORTED within a few iterations; the flag stays
+ * set until gn_request_abort(ctx, 0). */
 GN_API void gn_request_abort(gn_context *ctx, int on);
+/* Failure-detection self-test (no counterpart in the reference): runs the
+ * library's bounded team barrier for a team of two blocks of which only one
+ * is launched, so the wait runs out after about a second, as a wait on a
+ * block or peer that has died would.  Returns GN_ERR_TIMEOUT, with the context
+ * still usable; no fault or trap is involved. */
+GN_API int gn_selftest_wait_timeout(gn_context *ctx);
 
 /* Parity mode for the operators that take no precision argument (gn_dirac's
  * M^T, gn_energy): on = the reference's exact order of operations. */
