@@ -11,6 +11,7 @@
 #include "errors.h"
 #include "launch.h"
 #include "ops_kernels.cuh"
+#include "trace.h"
 
 namespace gn {
 
@@ -128,6 +129,7 @@ void Engine::momenta(double *P, const double *F, double eps) {
 
 void Engine::force(const double *X, const double *Y, const double *sigma, double beta_s, double *F, double *P,
                    double pcoef) {
+  TraceRange tr("gn sigma force");
   const double gcoef = (4 * beta_s / 2.0);  // (NFLAV * beta_scalar / 2.0), moleculardynamics.c:580
   force_kernel<double><<<op_blocks(V_, num_sms_), kOpThreads, 0, stream_>>>(g_, X, Y, sigma, gcoef, F, P, pcoef);
   check(cudaGetLastError(), "force_kernel");
@@ -227,6 +229,7 @@ int Engine::cg_blocks(int ncomp, int nrhs, bool mixed, int w) {
 
 int Engine::solve(const double *sm, const double *const *b, double *const *x, int nrhs, int ncomp, double tol,
                   int variant, int rel, long long max_iter, int precision, SolveInfo *info) {
+  TraceRange tr(precision == GN_PREC_MIXED ? "gn cg mixed" : "gn cg fp64");
   if (nrhs < 1 || nrhs > kMaxRhs || ncomp < 1 || ncomp > 2) throw GnError(GN_ERR_ARG, "bad nrhs / ncomp");
   if (max_iter <= 0) max_iter = V_ + 1;  // MAX_CONJUGATE_GRADIENT_ITERATION, macro.h:134
   if (precision == GN_PREC_MIXED) return solve_mixed(sm, b, x, nrhs, ncomp, tol, variant, rel, max_iter, info);
@@ -308,6 +311,7 @@ void count_flavours(const SolveInfo *info, int n, double &iters, long long &call
 
 int Engine::trajectory(const gn_hmc_params &hp, double (*gauss)(void), double (*uniform)(void), const double *pre_P,
                        const double *pre_chi, gn_traj_result *res) {
+  TraceRange tr("gn trajectory");
   if (hp.steps < 1) throw GnError(GN_ERR_ARG, "steps must be >= 1");
   if (hp.integrator < 0 || hp.integrator > 2) throw GnError(GN_ERR_ARG, "unknown integrator");
   if (u1_) return trajectory_u1(hp, gauss, uniform, pre_P, pre_chi, res);
@@ -415,6 +419,7 @@ int Engine::trajectory(const gn_hmc_params &hp, double (*gauss)(void), double (*
 // ------------------------------------------------------------------ condensate
 int Engine::condensate(const double *sm, double tol, double *target, double *D, double (*uniform)(void),
                        double out[11], double *iterations, long long *calls, int precision) {
+  TraceRange tr("gn condensate");
   const size_t V = size_t(V_);
   struct ExactScope {
     bool &flag, saved;

@@ -22,6 +22,7 @@
 #include "../../include/gn_b200.h"
 #define GN_DEFINE_ENSEMBLE_KERNEL
 #include "ensemble_kernel.cuh"
+#include "trace.h"
 #include "checkpoint.h"
 #include "errors.h"
 #include "launch.h"
@@ -378,6 +379,7 @@ void Ensemble::check_err() {
 }
 
 void Ensemble::run(const gn_ens_params &p, int ntraj, bool graph) {
+  TraceRange tr("gn ensemble run");
   if (p.steps < 1 || p.integrator < 0 || p.integrator > 2 || !(p.tol > 0.0) || ntraj < 0)
     throw GnError(GN_ERR_ARG, "bad ensemble parameters");
   if (p.precision != GN_PREC_MIXED && p.precision != GN_PREC_FP64)

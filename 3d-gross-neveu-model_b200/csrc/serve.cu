@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "../../include/gn_b200.h"
+#include "trace.h"
 #include "ensemble_kernel.cuh"  // declares ens_node_kernel (defined in ensemble.cu)
 #include "errors.h"
 #include "launch.h"
@@ -395,6 +396,7 @@ void Server::admit() {
 }
 
 int Server::step() {
+  TraceRange tr("gn server step");
   admit();
   if (running_.empty()) return 0;
   // Team size of the top tier this step: the whole GPU shared among the

@@ -16,6 +16,7 @@
 #include "launch.h"
 #include "ops_kernels.cuh"
 #include "schedule.h"
+#include "trace.h"
 
 namespace gn {
 
@@ -61,6 +62,7 @@ static const void *cm_kernel(int nr) {
 
 int Engine::solve_cm(const double *sm, const double *pm, const double *const *b, double *const *x, int nrhs,
                      double tol, int variant, int rel, long long max_iter, SolveInfo *info, int precision) {
+  TraceRange tr(precision == GN_PREC_MIXED ? "gn cg u1 mixed" : "gn cg u1 fp64");
   if (nrhs < 1 || nrhs > 2) throw GnError(GN_ERR_ARG, "the U(1) solve takes 1 or 2 systems");
   if (precision != GN_PREC_FP64 && precision != GN_PREC_MIXED)
     throw GnError(GN_ERR_ARG, "the U(1) model solves in FP64 or mixed precision");
@@ -152,6 +154,7 @@ void load_chi(Engine &E, const double *host_chi, const double *dev_chi) {
 // The sigma integrators (the schedules of schedule.h) with the complex M.
 int Engine::trajectory_u1(const gn_hmc_params &hp, double (*gauss)(void), double (*uniform)(void), const double *pre_P,
                           const double *pre_chi, gn_traj_result *res) {
+  TraceRange tr("gn trajectory u1");
   if (hp.precision != GN_PREC_FP64 && hp.precision != GN_PREC_MIXED)
     throw GnError(GN_ERR_ARG, "the U(1) model runs in FP64 or mixed precision");
   const size_t V = size_t(V_);
@@ -248,6 +251,7 @@ int Engine::trajectory_u1(const gn_hmc_params &hp, double (*gauss)(void), double
 // with H = sum P^2/2 + sum_f 1/2 Re(conj phi_f X_f) + (N_f beta_s / 8) sum pi^2.
 int Engine::trajectory_pi(const gn_hmc_params &hp, void (*gauss_pair)(double *, double *), double (*gauss)(void),
                           double (*uniform)(void), gn_traj_result *res) {
+  TraceRange tr("gn trajectory pi");
   if (!u1_) throw GnError(GN_ERR_ARG, "the context is not in the U(1) model (load pi first)");
   if (hp.steps < 1) throw GnError(GN_ERR_ARG, "steps must be >= 1");
   if (hp.precision != GN_PREC_FP64 && hp.precision != GN_PREC_MIXED)
