@@ -31,6 +31,11 @@ def main():
     L = int(hmc["L"])
     drop = C.CDLL(str(ROOT / "3d-gross-neveu-model_b200" / "lib" / "libgn_dropin.so"), mode=C.RTLD_GLOBAL)
     drop.GNB200_SetLattice(L)
+    drop.GNB200_Context.restype = C.c_void_p
+    core = C.CDLL(str(ROOT / "3d-gross-neveu-model_b200" / "lib" / "libgn_b200.so"))
+    core.gn_launch_count.restype = C.c_longlong
+    core.gn_launch_count.argtypes = [C.c_void_p]
+    launches = lambda: core.gn_launch_count(drop.GNB200_Context())  # noqa: E731  (GPU kernels so far)
     if len(sys.argv) > 3 and sys.argv[3] == "exact":
         drop.GNB200_SetPrecision(2)
     from oracle import build_ref
@@ -39,9 +44,10 @@ def main():
     lib = C.CDLL(str(path), mode=C.RTLD_GLOBAL)  # the reference's code, with its Gauss1 / Casuale
     ref = Ref.__new__(Ref)
     Ref.__init__(ref, L, int(hmc["integrator"]), build=False)
-    out = {"dH": [], "accepted": [], "sigma_rel": [], "counters": []}
+    out = {"dH": [], "accepted": [], "sigma_rel": [], "counters": [], "launches": {}}
     ref.init(1231, float(hmc["beta_s"]), float(hmc["eps"]), int(hmc["steps"]))
     ref.set_sigma(hmc["sigma0"])
+    n0 = launches()
     with tempfile.TemporaryDirectory() as td:
         acc = str(Path(td) / "acc.txt")
         for t in range(len(hmc["dH"])):
@@ -52,17 +58,22 @@ def main():
             out["accepted"].append(int(accepted))
             out["sigma_rel"].append(float(np.max(np.abs(s - hmc["sigma_final"][t])) / np.max(np.abs(hmc["sigma_final"][t]))))
             out["counters"].append(list(ref.counters()))
+    out["launches"]["trajectories"] = launches() - n0
     # the condensate through the reference's ComputeCondensateDirac call site
     ref.init(1231, float(hmc["beta_s"]), 0.2, 2)
     ref.set_sigma(cond["sigma"])
     ref.kit_set("Y", 0, cond["target0"].astype(complex))
     ref.lib.gnref_reset_counters()
+    n0 = launches()
     out["condensate"] = ref.condensate(1e-9).tolist()
+    out["launches"]["condensate"] = launches() - n0
     out["condensate_counters"] = list(ref.counters())
     # Dirac and CG through their call sites
     rng = np.random.default_rng(3)
     psi = rng.normal(size=L ** 3)
+    n0 = launches()
     out["M_psi"] = ref.dirac(psi.astype(complex), 0).real.tolist()
+    out["launches"]["dirac"] = launches() - n0
     out["psi"] = psi.tolist()
     out["sm"] = ref.sigmamass().tolist()
     print(json.dumps(out))

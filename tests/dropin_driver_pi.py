@@ -31,6 +31,12 @@ def main():
     V = L ** 3
     drop = C.CDLL(str(ROOT / "3d-gross-neveu-model_b200" / "lib" / "libgn_dropin_pi.so"), mode=C.RTLD_GLOBAL)
     drop.GNB200_SetLattice(L)
+    drop.GNB200_Context.restype = C.c_void_p
+    core = C.CDLL(str(ROOT / "3d-gross-neveu-model_b200" / "lib" / "libgn_b200.so"))
+    core.gn_launch_count.restype = C.c_longlong
+    core.gn_launch_count.argtypes = [C.c_void_p]
+    launches = lambda: core.gn_launch_count(drop.GNB200_Context())  # noqa: E731  (GPU kernels so far)
+    counts = {}
     from oracle import build_ref
     from oracle.oracle import Ref
     lib = C.CDLL(str(build_ref.lib_path(L, 0, build_ref.PI_TAG)), mode=C.RTLD_GLOBAL)
@@ -41,11 +47,15 @@ def main():
     ref.set_pi(g["pi"])
     out = {"pm": ref.pimass().tolist(), "sigma_obs": ref.condensate_sigma().tolist()}
     cj = lambda z: [np.real(z).tolist(), np.imag(z).tolist()]  # noqa: E731
+    n0 = launches()
     out["M_psi"] = cj(ref.dirac(g["psi"], 0))
+    counts["dirac"] = launches() - n0
     out["Mt_psi"] = cj(ref.dirac(g["psi"], 1))
     out["sub_res"] = cj(ref.dirac(g["psi"], 2, out=g["sub_out0"]))
     ref.lib.gnref_reset_counters()
+    n0 = launches()
     x, ok = ref.cg(g["cg_b"], None, 1e-9, 1)
+    counts["cg"] = launches() - n0
     out.update(cg_x=cj(x), cg_ok=bool(ok), cg_counters=list(ref.counters()))
     for f in range(2):
         ref.kit_set("phi", f, g["force_phi"][f])
@@ -57,7 +67,9 @@ def main():
     out["force_counters"] = list(ref.counters())
     for f in range(2):
         ref.kit_set("X", f, np.zeros(V, complex))
+    n0 = launches()
     out["piforce_ok"] = bool(ref.pi_force())
+    counts["pi_force"] = launches() - n0
     out["piforce_F"] = ref.pi_force_buf().tolist()
     out["piforce_Y"] = [cj(ref.kit_get("Y", f)) for f in range(2)]
     ref.set_momenta(g["energy_P"])
@@ -68,10 +80,13 @@ def main():
         accfile = str(Path(td) / "acc.txt")
         for name, run in (("traj", ref.trajectory), ("trajpi", ref.trajectory_pi)):
             ref.lib.gnref_reset_counters()
+            n0 = launches()
             ok, accepted, dH = run(accfile)
+            counts[name] = launches() - n0
             out.update({f"{name}_ok": bool(ok), f"{name}_dH": dH, f"{name}_accepted": int(accepted),
                         f"{name}_counters": list(ref.counters()), f"{name}_sigma": ref.sigma().tolist(),
                         f"{name}_pi": ref.pi().tolist()})
+    out["launches"] = counts
     C.CDLL(None).fflush(None)  # LeapFrog2Pi's printed lines go out before the JSON line
     print(json.dumps(out))
     _ = (drop, lib)

@@ -39,6 +39,9 @@ def test_dropin_under_reference_driver(port):
     for k in range(11):
         assert abs(out["condensate"][k] - c["out"][k]) <= 1e-11 * max(abs(c["out"][k]), 1e-3)
     assert tuple(out["condensate_counters"]) == tuple(c["counters"])
+    # the replacement took effect: each phase launched the library's kernels
+    assert all(out["launches"][k] > 0 for k in ("trajectories", "condensate", "dirac")), out["launches"]
+    assert out["launches"]["trajectories"] >= 20 * 5  # 20 trajectories, each with solves, forces and steps
     # DiracFermion called by the reference's harness equals the reference's own M, bit for bit
     L = 8
     assert np.array_equal(np.array(out["M_psi"]), port.dirac(L, np.array(out["sm"]), np.array(out["psi"]), 0))
@@ -82,6 +85,8 @@ def test_dropin_pi_under_reference_harness(L):
 
     def rel(a, b):
         return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
+    # the replacement took effect: each call site launched the library's kernels
+    assert all(v > 0 for v in out["launches"].values()) and len(out["launches"]) == 5, out["launches"]
     assert np.array_equal(np.array(out["pm"]), g["pm"])
     np.testing.assert_allclose(out["sigma_obs"], g["sigma_obs"], rtol=1e-12, atol=1e-16)
     assert np.array_equal(cx(out["M_psi"]), g["M_psi"])

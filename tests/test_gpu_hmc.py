@@ -210,3 +210,27 @@ def test_md_reversibility(port, model, integrator):
     assert rel(-P2, P0) < 1e-9
     assert abs(r1["dH"] + r2["dH"]) < 1e-9
     assert abs(r2["H1"] - r1["H0"]) < 1e-9 * abs(r1["H0"])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_rerun_is_bitwise_identical(precision):
+    """Every block sums the partials of a phase in the same fixed order, so a
+    solve, and a trajectory built on solves, gives the same bits when run
+    again on the same input (here at L = 32, 128 blocks per solve)."""
+    import gn_b200 as G
+    prec = G.GN_PREC_FP64 if precision == "fp64" else G.GN_PREC_MIXED
+    L, V = 32, 32 ** 3
+    rng = np.random.default_rng(21)
+    sigma0 = rng.normal(0, np.sqrt(2 / (4 * 0.85)), V)
+    draws = rng.normal(size=3 * V)
+    runs = []
+    for _ in range(2):
+        with G.Lattice(L) as lat:
+            lat.load_sigma(sigma0)
+            it = iter(draws)
+            r = lat.trajectory(0.85, 0.05, 4, lambda: next(it), None, tol_medium=1e-10, tol_high=1e-10,
+                               relative=True, precision=prec)
+            runs.append((r["dH"], r["cg_iterations"], lat.store_sigma()[0], lat.read_state(G.GN_F_X)))
+    (d0, i0, s0, x0), (d1, i1, s1, x1) = runs
+    assert d0 == d1 and i0 == i1
+    assert np.array_equal(s0, s1) and np.array_equal(x0, x1)
