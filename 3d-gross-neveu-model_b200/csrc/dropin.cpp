@@ -472,13 +472,15 @@ bool LeapFrog2MinimumNormSigmaVelocityFirst(Lattice *lattice, Info *info, Forces
   return trajectory(lattice, info, force, momenta, kit, epsilon, step, acceptance_file, GN_LFMN2VF);
 }
 
-#ifndef GN_DROPIN_PI  // the U(1) build keeps the reference's own, whose solves run through this layer
 void ComputeCondensateDirac(const Lattice *lat, double *tr1, double *tr1_abs, double *tr2, double *tr4, double *mu2,
                             double *mu4, double *chi, double *chi_abs, double *chip, double *c12_nosigma,
                             double *c12_withsigma, RandomVec *, Fermion *target_inverted, const Info *,
                             const Fermioncoor *, double inversion_precision, Fermionkit *kit, int) {
   gn_context *c = ctx();
   g_uniform = resolve(g_uniform, "Casuale");
+#ifdef GN_DROPIN_PI  // the same solves with the complex M: pi (and its mass) resident first
+  if (gn_load_pi(c, lat->pi) != GN_OK) fatal("gn_load_pi");
+#endif
   double *target = g_a.data(), *D = g_b.data();
   to_planes(target_inverted->fermion, target, 2);
   double out[11], it = 0.0;
@@ -493,7 +495,6 @@ void ComputeCondensateDirac(const Lattice *lat, double *tr1, double *tr1_abs, do
   double *dst[11] = {tr1, tr1_abs, tr2, tr4, mu2, mu4, chi, chi_abs, chip, c12_nosigma, c12_withsigma};
   for (int k = 0; k < 11; k++) *dst[k] = out[k];
 }
-#endif
 
 void CondensateSigmaPi(const Lattice *lat, const Info *, double *condensate_sigma, double *condensate_sigma_abs,
                        double *mu2, double *mu4, double *chi, double *chip, double *chip_pbc1, double *chip_pbc2) {

@@ -421,6 +421,7 @@ int Engine::condensate(const double *sm, double tol, double *target, double *D, 
                        double out[11], double *iterations, long long *calls, int precision) {
   TraceRange tr("gn condensate");
   const size_t V = size_t(V_);
+  if (u1_ && precision == GN_PREC_FP64_EXACT) throw GnError(GN_ERR_ARG, "the U(1) model has no exact-order mode");
   struct ExactScope {
     bool &flag, saved;
     ExactScope(bool &f, bool on) : flag(f), saved(f) { flag = flag || on; }
@@ -443,7 +444,9 @@ int Engine::condensate(const double *sm, double tol, double *target, double *D, 
   auto solve1 = [&](const double *b) {
     const double *bs[1] = {b};
     double *xs[1] = {target};
-    const int st = solve(sm, bs, xs, 1, 2, tol, 0, 0, 0, precision, info);
+    // U(1) model: the same solves with M = D + sm + i eps pm (the resident pi mass)
+    const int st = u1_ ? solve_cm(sm, pm_, bs, xs, 1, tol, 0, 0, 0, info, precision)
+                       : solve(sm, bs, xs, 1, 2, tol, 0, 0, 0, precision, info);
     if (info[0].status == kCgConverged) {
       *iterations += double(info[0].iters);
       (*calls)++;
@@ -456,13 +459,17 @@ int Engine::condensate(const double *sm, double tol, double *target, double *D, 
     check(cudaMemcpyAsync(signs_, h_signs, V, cudaMemcpyHostToDevice, stream_), "upload signs");
     cond_fill(0, signs_, nullptr, nullptr, vec);
   };
+  auto adj = [&]() {  // D = M^dagger target (AdjDiracFermion)
+    if (u1_) dirac_cm(sm, pm_, target, D, 1, GN_OP_MT);
+    else dirac(sm, target, D, 2, GN_OP_MT);
+  };
   double q[4];
   for (int k = 0; k < 11; k++) out[k] = 0.0;
   double temp[4];
   for (int p = 0; p < 4; p++) {
     z2();
     solve1(vec);
-    dirac(sm, target, D, 2, GN_OP_MT);
+    adj();
     dots(vec, D, q);
     temp[p] = q[0];
   }
@@ -474,7 +481,7 @@ int Engine::condensate(const double *sm, double tol, double *target, double *D, 
   // mu2, chi: the 1/V vector (condensate.c:167-181)
   cond_fill(1, nullptr, nullptr, nullptr, vec);
   solve1(vec);
-  dirac(sm, target, D, 2, GN_OP_MT);
+  adj();
   dots(vec, D, q);
   out[4] = q[1];
   out[5] = out[4] * out[4];
@@ -494,7 +501,7 @@ int Engine::condensate(const double *sm, double tol, double *target, double *D, 
     check(cudaMemcpyAsync(table_, h_tab, sizeof(double) * 2 * L_, cudaMemcpyHostToDevice, stream_), "table");
     cond_fill(2, nullptr, table_, nullptr, vec);
     solve1(vec);
-    dirac(sm, target, D, 2, GN_OP_MT);
+    adj();
     dots(vec, D, q);
     out[8] = q[2] * double(int(V));
   }
@@ -502,9 +509,9 @@ int Engine::condensate(const double *sm, double tol, double *target, double *D, 
   z2();
   check(cudaMemcpyAsync(z, vec, 2 * V * sizeof(double), cudaMemcpyDeviceToDevice, stream_), "copy z");
   solve1(vec);
-  dirac(sm, target, D, 2, GN_OP_MT);
+  adj();
   solve1(D);
-  dirac(sm, target, D, 2, GN_OP_MT);
+  adj();
   dots(z, D, q);
   out[9] = q[3];
   // with sigma-mass insertions (condensate.c:216-230)
@@ -512,10 +519,10 @@ int Engine::condensate(const double *sm, double tol, double *target, double *D, 
   check(cudaMemcpyAsync(z, vec, 2 * V * sizeof(double), cudaMemcpyDeviceToDevice, stream_), "copy z");
   cond_fill(3, nullptr, nullptr, sm, vec);
   solve1(vec);
-  dirac(sm, target, D, 2, GN_OP_MT);
+  adj();
   cond_fill(3, nullptr, nullptr, sm, D);
   solve1(D);
-  dirac(sm, target, D, 2, GN_OP_MT);
+  adj();
   dots(z, D, q);
   out[10] = q[3];
   check(cudaStreamSynchronize(stream_), "condensate");

@@ -2,15 +2,14 @@
  * gn_dropin_pi.h -- the drop-in layer for a program built with PI_INTERACTION
  * (the U(1) Gross-Neveu model): 3d-gross-neveu-model_b200/lib/libgn_dropin_pi.so.
  *
- * It exports every function of gn_dropin.h but ComputeCondensateDirac, with
- * the PI build's meaning: M = D + sigmamass + i epsilon_pi pimass on complex
- * fermion fields (dirac.c:65-69), the CG, the sigma force and the sigma
- * integrators with that M, and CondensateSigmaPi of |(sigma, pi)|
- * (observables.c:345).  It adds the pi functions below.  The reference's own
- * ComputeCondensateDirac, left in place, then runs its solves through this
- * layer.  The struct layouts are those of gn_dropin.h (the reference's
- * headers have no PI_INTERACTION switch) plus Forcepi and Momentapi
- * (moleculardynamics.h:64-67, :94-97).
+ * It exports every function of gn_dropin.h with the PI build's meaning:
+ * M = D + sigmamass + i epsilon_pi pimass on complex fermion fields
+ * (dirac.c:65-69), the CG, the sigma force, the sigma integrators and
+ * ComputeCondensateDirac (condensate.c:114, unchanged by PI_INTERACTION but
+ * for its M) with that M, and CondensateSigmaPi of |(sigma, pi)|
+ * (observables.c:345).  It adds the pi functions below.  The struct layouts
+ * are those of gn_dropin.h (the reference's headers have no PI_INTERACTION
+ * switch) plus Forcepi and Momentapi (moleculardynamics.h:64-67, :94-97).
  *
  * LeapFrog2Pi draws the pi momenta in pairs from the host program's
  * Gauss2MeanVariance (random.c:129), found by name like Gauss1 and Casuale,

@@ -6,7 +6,7 @@ libgn_dropin_pi.so is loaded first with RTLD_GLOBAL, then the reference's code
 compiled with -DPI_INTERACTION (oracle/_ref/libgnref_L{L}_i0_pi.so).  The
 harness then calls the reference's functions by name (DiracFermion, the CG,
 ComputeSigmaForce, ComputePiForce, the energies, CondensateSigmaPi,
-LeapFrog2MinimumNormSigmaVelocityFirst, LeapFrog2Pi) in the order
+LeapFrog2MinimumNormSigmaVelocityFirst, LeapFrog2Pi, ComputeCondensateDirac) in the order
 tests/golden/make_golden_u1.py called them on the reference alone; each binds
 to the drop-in's GPU version.  Random numbers come from the reference's own
 Gauss1, Casuale and Gauss2MeanVariance, found by name.
@@ -86,6 +86,14 @@ def main():
             out.update({f"{name}_ok": bool(ok), f"{name}_dH": dH, f"{name}_accepted": int(accepted),
                         f"{name}_counters": list(ref.counters()), f"{name}_sigma": ref.sigma().tolist(),
                         f"{name}_pi": ref.pi().tolist()})
+    # ComputeCondensateDirac on the state the trajectories left
+    ref.kit_set("Y", 0, g["cond_target0"])
+    ref.lib.gnref_reset_counters()
+    n0 = launches()
+    out["cond_out"] = ref.condensate(1e-9).tolist()
+    counts["condensate"] = launches() - n0
+    out.update(cond_counters=list(ref.counters()), cond_target=cj(ref.kit_get("Y", 0)),
+               cond_D=cj(ref.kit_get("D", 0)))
     out["launches"] = counts
     C.CDLL(None).fflush(None)  # LeapFrog2Pi's printed lines go out before the JSON line
     print(json.dumps(out))

@@ -3,8 +3,8 @@
 The reference compiled with PI_INTERACTION (oracle/build_ref.py with
 extra_defs -DPI_INTERACTION, driven through oracle/ref_harness.c) runs its own
 complex-mass Dirac operator, CG, sigma and pi forces and energies, one
-LeapFrog2MinimumNormSigmaVelocityFirst trajectory and one LeapFrog2Pi
-trajectory on seeded sigma and pi fields; the random streams the trajectories
+LeapFrog2MinimumNormSigmaVelocityFirst trajectory, one LeapFrog2Pi
+trajectory and then ComputeCondensateDirac on seeded sigma and pi fields; the random streams the trajectories
 consumed (Gauss1, the Gauss2MeanVariance pairs of the pi momenta and Casuale,
 all from dSFMT) are recorded so the fixtures replay them without the
 reference's RNG.
@@ -99,6 +99,17 @@ def fixture(L):
                       f"{name}_counters": np.array(ref.counters()), f"{name}_sigma": ref.sigma(),
                       f"{name}_pi": ref.pi()})
     d.update(traj_eps=0.1, traj_steps=3)
+    # ComputeCondensateDirac with the complex M on the state the trajectories
+    # left, from a seeded starting target, with the uniforms its Z2 vectors drew
+    target0 = 0.1 * cplx(rng, V)
+    ref.kit_set("Y", 0, target0)
+    ref.lib.gnref_reset_counters()
+    d.update(cond_sigma=ref.sigma(), cond_pi=ref.pi(), cond_sm=ref.sigmamass(), cond_target0=target0)
+    ref.lib.gnref_rng_save()
+    out = ref.condensate(1e-9)
+    ref.lib.gnref_rng_restore()
+    d.update(cond_uniform=ref.uniform(6 * V), cond_out=out, cond_target=ref.kit_get("Y", 0),
+             cond_D=ref.kit_get("D", 0), cond_counters=np.array(ref.counters()))
     np.savez_compressed(HERE / f"golden_L{L}_u1.npz", **d)
     print(HERE / f"golden_L{L}_u1.npz", "dH", d["traj_dH"], d["trajpi_dH"])
 

@@ -86,7 +86,7 @@ def test_dropin_pi_under_reference_harness(L):
     def rel(a, b):
         return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
     # the replacement took effect: each call site launched the library's kernels
-    assert all(v > 0 for v in out["launches"].values()) and len(out["launches"]) == 5, out["launches"]
+    assert all(v > 0 for v in out["launches"].values()) and len(out["launches"]) == 6, out["launches"]
     assert np.array_equal(np.array(out["pm"]), g["pm"])
     np.testing.assert_allclose(out["sigma_obs"], g["sigma_obs"], rtol=1e-12, atol=1e-16)
     assert np.array_equal(cx(out["M_psi"]), g["M_psi"])
@@ -109,3 +109,9 @@ def test_dropin_pi_under_reference_harness(L):
         assert tuple(out[f"{name}_counters"]) == tuple(g[f"{name}_counters"])
         assert rel(np.array(out[f"{name}_sigma"]), g[f"{name}_sigma"]) < 1e-11
         assert rel(np.array(out[f"{name}_pi"]), g[f"{name}_pi"]) < 1e-11
+    # the condensate with the complex M
+    assert tuple(out["cond_counters"]) == tuple(g["cond_counters"])
+    for k in range(11):
+        assert abs(out["cond_out"][k] - g["cond_out"][k]) <= 1e-11 * max(abs(g["cond_out"][k]), 1e-3), k
+    assert rel(cx(out["cond_target"]), g["cond_target"]) < 1e-11
+    assert rel(cx(out["cond_D"]), g["cond_D"]) < 1e-11

@@ -179,3 +179,25 @@ def test_u1_mixed_precision_trajectories(port):
         assert a[q]["accepted"] == b[q]["accepted"]
         assert b[q]["reliable_updates"] > 0
     assert rel(b[2], a[2]) < 1e-8 and rel(b[3], a[3]) < 1e-8
+
+
+@pytest.mark.parametrize("L", [4, 8])
+def test_u1_condensate(golden, port, L):
+    """ComputeCondensateDirac of the reference's PI build (the same ten solves
+    and M^dagger applies with the complex M), against its fixture: the 11
+    outputs to 1e-11 relative, the reference's CG bookkeeping, and the final
+    target and D to 1e-11."""
+    import gn_b200 as G
+    g = golden(f"golden_L{L}_u1.npz")
+    _, up = port.replay(np.zeros(0), g["cond_uniform"])
+    with G.Lattice(L) as lat:
+        lat.load_sigma(g["cond_sigma"])
+        lat.load_pi(g["cond_pi"])
+        out, target, D, it, calls, st = lat.condensate(g["cond_sm"], 1e-9, g["cond_target0"], up)
+    assert st == G.GN_OK
+    assert port.replay_pos()[1] == 6 * L ** 3
+    assert (it, calls) == tuple(g["cond_counters"])
+    for k in range(11):
+        assert abs(out[k] - g["cond_out"][k]) <= 1e-11 * max(abs(g["cond_out"][k]), 1e-3), (k, out[k])
+    assert rel(target, g["cond_target"]) < 1e-11
+    assert rel(D, g["cond_D"]) < 1e-11
