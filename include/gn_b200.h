@@ -167,7 +167,10 @@ GN_API int gn_evolve_momenta(gn_context *ctx, double *P, const double *F, double
  * tests it, as the reference does); D (2V) receives kit->Ddag_inverted_phi_obs.
  * out[11] = tr1, |tr1|, tr2, tr4, mu2, mu4, chi, |chi|, chi_p, c12 without
  * sigma, c12 with sigma.  cg_iterations / cg_calls (may be NULL) receive the
- * amounts the reference adds to kit->iterations / kit->CG_call. */
+ * amounts the reference adds to kit->iterations / kit->CG_call.  In a context
+ * holding pi (gn_load_pi) M is the U(1) model's complex M with the resident
+ * pimass, as the reference's PI_INTERACTION build runs it; precision
+ * GN_PREC_FP64 or GN_PREC_MIXED there. */
 GN_API int gn_condensate(gn_context *ctx, const double *sigmamass, double tol, double *target, double *D,
                   double (*uniform)(void), double *out, double *cg_iterations, long long *cg_calls, int precision);
 
