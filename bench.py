@@ -473,7 +473,7 @@ def kernel_roofline(lat, stream, a, G):
     inner = max(i["inner_iterations"] for i in infos)
     ru = sum(i["reliable_updates"] for i in infos)
     nbytes = V * ((8 + 44 * 2) * inner + 72 * ru + 12 + 28 * 2)
-    return {"gbs": nbytes / (ms * 1e-3) / 1e9, "kernel": "cg_mixed_kernel<1, 2, 1024, 4> (2 flavours, L=%d)" % lat.L,
+    return {"gbs": nbytes / (ms * 1e-3) / 1e9, "kernel": "cg_mixed_kernel<1, 2, 1024, 4, 0> (2 flavours, L=%d)" % lat.L,
             "ms": ms, "bytes": nbytes, "traffic": CG_MIXED_DRAM_BYTES if lat.L == 64 else None,
             "note": f"{inner} inner iterations, {ru} reliable updates, {ms:.3f} ms per launch; working set "
                     f"{(2 * 5 * 4 + 8 * 3) * V / 1e6:.0f} MB is L2-resident within the solve"}
