@@ -192,3 +192,40 @@ def test_mixed_precision_schemes(lattices, port, L):
         assert np.linalg.norm(r) < 1e-10 * np.linalg.norm(b[k]) * 1.01
         assert im[k]["iterations"] <= 1.1 * i64[k]["iterations"] + 20
         assert rel(xm[k], x64[k]) < 1e-7
+
+
+@pytest.mark.parametrize("L", [6, 10])
+def test_odd_half_rows_force_trajectory_mixed(lattices, port, L):
+    """L/2 odd: every sweep runs one site per item (no 128-bit vectors).  The
+    force and one LFMN2VF trajectory against the CPU restatement on the same
+    random stream, and the mixed solver's true residual."""
+    import gn_b200 as G
+    rng = np.random.default_rng(100 + L)
+    V = L ** 3
+    lat = lattices(L)
+    sigma = rng.normal(0, np.sqrt(2 / (4 * 0.85)), V)
+    sm = lat.sigma_mass(sigma)
+    phi = np.stack([port.dirac(L, sm, rng.normal(size=V), 0) for _ in range(2)])
+    F, X, Y, info, st = lat.sigma_force(0.85, sigma, sm, phi, np.zeros((2, V)), 1e-9)
+    Fr, Xr, Yr, ok, it, calls = port.force(L, 0.85, sigma, sm, phi, np.zeros((2, V)), 1e-9)
+    assert st == 0 and ok and sum(i["iterations"] for i in info) == it
+    assert rel(F, Fr) < RTOL_SOLVE and rel(X, Xr) < RTOL_SOLVE
+    # one trajectory, GPU and port on the same draws
+    gauss = rng.normal(size=3 * V)
+    gp, up = port.replay(gauss, np.array([0.5]))
+    st_port = dict(sigma=sigma.copy(), sm=sm.copy(), P=np.zeros(V), F=np.zeros(V), chi=np.zeros((2, V)),
+                   phi=np.zeros((2, V)), X=np.zeros((2, V)), Y=np.zeros((2, V)))
+    okp, dHp, accp, _, _ = port.trajectory(L, 0.85, 0.1, 3, st_port, gp, up)
+    gp, up = port.replay(gauss, np.array([0.5]))
+    lat.load_sigma(sigma)
+    r = lat.trajectory(0.85, 0.1, 3, gp, up)
+    assert okp and r["ok"] == 1 and r["accepted"] == int(accp)
+    assert abs(r["dH"] - dHp) < 1e-10
+    assert rel(lat.store_sigma()[0], st_port["sigma"]) < 1e-11
+    # mixed precision: FP32 items of one site
+    b = rng.normal(size=(2, V))
+    xm, im, st = lat.cg(sm, b, None, 1e-10, variant=1, relative=True, precision=G.GN_PREC_MIXED)
+    assert st == 0
+    for k in range(2):
+        r2 = b[k] - port.dirac(L, sm, port.dirac(L, sm, xm[k], 1), 0)
+        assert np.linalg.norm(r2) < 1e-10 * np.linalg.norm(b[k]) * 1.01
