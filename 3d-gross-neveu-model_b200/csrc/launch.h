@@ -15,8 +15,9 @@ namespace gn {
 // Threads per block of the solvers: one large block per SM (launch bounds
 // (BS, 1)), because every block arriving at a grid barrier costs about 8 ns
 // (measured).  The hot shapes (one real plane, up to two systems: the two
-// pseudofermion flavours) use 768 threads (80 registers), measured fastest at
-// every L from 8 to 128; the rarely used ones 512 (up to 128 registers).
+// pseudofermion flavours) use 1024 threads (64 registers), so that a sweep of
+// the mixed solver at L = 64 gives every thread one work unit; the rarely
+// used shapes 512 (up to 128 registers).
 constexpr int kWideThreads = 1024;
 constexpr int kSolverThreads = 512;
 

@@ -1,27 +1,31 @@
 // noalloc.cu -- a CG solve on (M M^T) x = b that allocates no memory.
 //
-// Who needs it: callers that must not allocate device memory after start-up --
-// a host code that does all of its memory management itself (for example an
-// HMC driver that sizes every buffer once from the lattice size, as the
-// reference's Allocate* functions do), code that runs between a pool
-// allocator's reservation and its release, or code that is recorded into a
-// CUDA graph, where cudaMalloc / cudaFree are not allowed.  gn_create() needs
-// cudaMalloc for its per-lattice buffers; this entry point does not.
+// Who needs it: callers that must not allocate device memory once they are
+// running.  An HMC driver written like the reference sizes every buffer once,
+// from the lattice size, in its Allocate* functions, and owns all of its
+// device memory from then on; an application that hands this library a fixed
+// budget from its own pool allocator cannot have it call cudaMalloc behind
+// the pool's back, where the allocation would escape the budget, or fail
+// when the pool has taken the rest of the GPU.  gn_create() needs cudaMalloc
+// for its per-lattice buffers; this entry point does not.
 //
 // The solver's scratch (residual, two search directions, M^T p, the per-block
 // partial sums and the grid barrier) lives in the file-scope array below,
 // sized for lattices up to kNoAllocMaxL^3 sites (about 1 MiB).  Every GPU that
-// loads the library holds it until the process exits.  All calls share it, so
-// calls that overlap on the GPU (two streams, two host threads) race: order
-// them, e.g. on one stream.  The array keeps the last call's contents; what
-// must start at zero (barrier counter, error flag) is cleared by every call.
+// loads the library holds it until the process exits.  All calls share it:
+// calls that overlap on the GPU race on it, and so do calls from several host
+// threads even on one stream, because one call's read-back of its outcome can
+// pick up another call's.  Serialise whole calls on the host (one thread at a
+// time, or a lock around the call).  The array keeps the last call's contents;
+// what must start at zero (barrier counter, error flag, outcome) is cleared by
+// every call.
 //
 // Set-up: the host cannot use the array's name as a device address (in host
 // code it is only a stand-in).  The first call on each device, with that
 // device current, asks cudaGetSymbolAddress for the address and the occupancy
-// API for the cooperative grid size and caches both; make that first call
-// before any stream capture.  Later calls only clear the control words, launch
-// the kernel and read the outcome back.
+// API for the cooperative grid size and caches both; that first call should
+// come before any stream capture.  Later calls only clear the control words,
+// launch the kernel and read the outcome back.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -78,6 +82,7 @@ extern "C" GN_API long long gn_cg_noalloc_max_volume(void) { return (long long)k
 
 extern "C" GN_API int gn_cg_noalloc(int L, const double *sigmamass, const double *b, double *x, double tol, int variant,
                                     int relative, long long max_iter, void *stream, gn_cg_info *info) {
+  g_msg[0] = '\0';  // a message describes the failure of the last call only
   if (L < 4 || (L & 1)) return err(GN_ERR_ARG, "gn_cg_noalloc: L must be even and >= 4");
   if (L > kNoAllocMaxL)
     return err(GN_ERR_ARG, "gn_cg_noalloc: L exceeds the static scratch limit of 32 (32768 sites); use gn_cg_device");

@@ -18,8 +18,16 @@ draws them.
   roofline   the dominant kernel: the persistent CG kernel (mixed precision,
              two flavours) of one solve; algorithmic bytes from its iteration
              counts, duration from CUDA events.
-  cpu_baseline / --impl reference: the reference's own C code (compiled from
-             its sources into oracle/_ref/) on the host cores.
+  cpu_baseline one full trajectory of the reference's own C code (compiled
+             from its sources into oracle/_ref/, every CG to 1e-10 |phi|) on
+             one host core, run in a spawned process beside the GPU work.
+  --impl reference: the reference arm, K trajectories of the same code spread
+             over the host cores (one serial process per core); value = K over
+             the wall clock from a common start to the last finish.
+
+The line ends with short summaries of the side measurements (batched chains,
+serving, L = 128, U(1)), the Dirac apply's roofline, the FP64 arm and the
+mixed / FP64 ratio; --detail PATH writes all of them in full.
 
 Multi-GPU: one process per GPU, each an independent chain (the path does not
 shard; replicas only), max over ranks of the timed region.
@@ -66,9 +74,11 @@ def parse():
     ap.add_argument("--eps", type=float, default=0.05)
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--case", choices=["cg64", "dirac128", "dirac256", "traj64", "cgscan", "batched", "serve", "l128",
-                                       "u1"], default=None,
-                    help="run one small case for a profiler instead of the benchmark")
+    ap.add_argument("--no-l128", action="store_true", help="skip the L = 128 mixed-precision case")
+    ap.add_argument("--detail", default=None, help="write every side measurement to this JSON file")
+    ap.add_argument("--case", choices=["cg64", "dirac128", "dirac256", "traj64", "batched", "serve", "l128", "u1",
+                                       "ens", "kernels"],
+                    default=None, help="run one small case for a profiler instead of the benchmark")
     return ap.parse_args()
 
 
@@ -171,37 +181,111 @@ class Clocks:
 
 
 # ---------------------------------------------------------------- reference (CPU)
-def _ref_solve_worker(args):
-    """One reference CG solve (StartX0Imposed..., conjugategradient.c:115) at L
-    from x = 0 on b = M chi, at the absolute tolerance equal to tol * |b|."""
-    L, tol, seed = args
-    sys.path.insert(0, str(ROOT))
-    from oracle.oracle import Ref
-    ref = Ref(L, build=False)
-    ref.init(1231, BETA_S, 0.05, 10)
-    rng = np.random.default_rng(seed)
-    V = L ** 3
-    ref.set_sigma(rng.normal(0.0, np.sqrt(2.0 / (NFLAV * BETA_S)), V))
-    b = ref.dirac(rng.normal(size=V).astype(complex), 0)
-    tol_abs = tol * float(np.linalg.norm(b))
-    t0 = time.perf_counter()
-    _, ok = ref.cg(b, None, tol_abs, 1)
-    dt = time.perf_counter() - t0
-    it, _ = ref.counters()
-    return dt, it
+REF_REL_TAG = "_rel"  # the reference built with GN_REF_RELATIVE_TOL=1e-10 (oracle/build_ref.py REL_TAG)
 
 
-def _port_solve(L, tol, seed):
-    sys.path.insert(0, str(ROOT))
-    from oracle.oracle import Port
-    port = Port()
-    rng = np.random.default_rng(seed)
-    V = L ** 3
-    sm = port.sigma_mass(L, rng.normal(0.0, np.sqrt(2.0 / (NFLAV * BETA_S)), V))
-    b = port.dirac(L, sm, rng.normal(size=V), 0)
-    t0 = time.perf_counter()
-    _, ok, it, _ = port.cg(L, sm, b, None, tol * float(np.linalg.norm(b)), 1)
-    return time.perf_counter() - t0, it
+def ref_rel_path(L):
+    from oracle import build_ref
+    return build_ref.lib_path(L, 0, REF_REL_TAG)
+
+
+def _ref_traj_worker(L, eps, md_steps, seed, ntraj, warm, barrier, q):
+    """`ntraj` trajectories of the reference's own integrator
+    LeapFrog2MinimumNormSigmaVelocityFirst (moleculardynamics.c:1234) at L, in
+    this process, drawing from the reference's dSFMT stream seeded with `seed`.
+    The build (oracle/_ref/libgnref_L{L}_i0_rel.so) stops every CG at
+    |r| < 1e-10 |phi|, the benchmark's rule.  `warm` Dirac applies (dirac.c:46)
+    come first; the clock starts when every worker has reached the barrier.
+    Puts (t_start, t_end, ntraj, cg_iterations, accepted, error)."""
+    try:
+        sys.path.insert(0, str(ROOT))
+        from oracle.oracle import Ref
+        ref = Ref(L, build=False, tag=REF_REL_TAG)
+        ref.init(seed, BETA_S, eps, md_steps)
+        rng = np.random.default_rng(seed)
+        V = L ** 3
+        ref.set_sigma(rng.normal(0.0, np.sqrt(2.0 / (NFLAV * BETA_S)), V))
+        psi = rng.normal(size=V).astype(complex)
+        for _ in range(warm):
+            ref.dirac(psi, 0)
+        acc = 0
+        with tempfile.TemporaryDirectory() as d:
+            barrier.wait()
+            t0 = time.monotonic()
+            for _ in range(ntraj):
+                ok, a, _ = ref.trajectory(os.path.join(d, "acc.txt"))
+                acc += int(a)
+            t1 = time.monotonic()
+        q.put((t0, t1, ntraj, ref.counters()[0], acc, None))
+    except Exception as e:  # reported by the parent
+        barrier.abort()
+        q.put((0.0, 0.0, 0, 0.0, 0, repr(e)))
+
+
+def _port_traj_worker(L, eps, md_steps, seed, ntraj, warm, barrier, q):
+    """The same as _ref_traj_worker with the CPU restatement (oracle/gn_oracle.c)
+    when the reference's build is absent: its own Gaussian draws, every CG to
+    |r| < 1e-10 |b|."""
+    try:
+        sys.path.insert(0, str(ROOT))
+        from oracle.oracle import Port
+        port = Port()
+        V = L ** 3
+        rng = np.random.default_rng(seed)
+        sigma = rng.normal(0.0, np.sqrt(2.0 / (NFLAV * BETA_S)), V)
+        st = dict(sigma=sigma, sm=port.sigma_mass(L, sigma), P=np.zeros(V), F=np.zeros(V), chi=np.zeros((2, V)),
+                  phi=np.zeros((2, V)), X=np.zeros((2, V)), Y=np.zeros((2, V)))
+        gp, up = port.replay(rng.normal(size=3 * V * ntraj), rng.uniform(size=ntraj))
+        for _ in range(warm):
+            port.dirac(L, st["sm"], sigma, 0)
+        acc = 0
+        barrier.wait()
+        t0 = time.monotonic()
+        for _ in range(ntraj):
+            ok, dH, a, _, _ = port.trajectory(L, BETA_S, eps, md_steps, st, gp, up, tol_med=-1e-10, tol_high=-1e-10)
+            acc += int(a)
+        t1 = time.monotonic()
+        q.put((t0, t1, ntraj, st["iterations"], acc, None))
+    except Exception as e:
+        barrier.abort()
+        q.put((0.0, 0.0, 0, 0.0, 0, repr(e)))
+
+
+class CpuTrajectories:
+    """`ntraj` CPU trajectories spread over `procs` spawned processes (the
+    reference is serial: one chain per core, as its own scripts run it).
+    start() returns at once; result() waits and gives trajectories per second
+    from the common start to the last finish."""
+
+    def __init__(self, L, eps, md_steps, ntraj, procs, warm, seed0=1231):
+        import multiprocessing as mp
+        self.kind = "reference" if ref_rel_path(L).exists() else "port"
+        worker = _ref_traj_worker if self.kind == "reference" else _port_traj_worker
+        ctx = mp.get_context("spawn")
+        self.procs = max(1, min(procs, ntraj))
+        self.barrier = ctx.Barrier(self.procs)
+        self.q = ctx.Queue()
+        self.ntraj, self.L = ntraj, L
+        self.ps = [ctx.Process(target=worker, daemon=True,
+                               args=(L, eps, md_steps, seed0 + i, ntraj // self.procs + (i < ntraj % self.procs),
+                                     warm, self.barrier, self.q)) for i in range(self.procs)]
+
+    def start(self):
+        for p in self.ps:
+            p.start()
+        return self
+
+    def result(self, timeout=3600.0):
+        out = [self.q.get(timeout=timeout) for _ in self.ps]
+        for p in self.ps:
+            p.join(timeout=60)
+        errs = [o[5] for o in out if o[5]]
+        if errs:
+            raise RuntimeError(f"CPU trajectories failed: {errs[0]}")
+        wall = max(o[1] for o in out) - min(o[0] for o in out)
+        return {"value": self.ntraj / wall, "wall_s": wall, "kind": self.kind, "cores": self.procs,
+                "cg_iterations_per_traj": sum(o[3] for o in out) / self.ntraj,
+                "acceptance": sum(o[4] for o in out) / self.ntraj}
 
 
 def _u1_ref_solve(L, tol, seed=0):
@@ -224,65 +308,37 @@ def _u1_ref_solve(L, tol, seed=0):
     return dt, ref.counters()[0]
 
 
-def reference_available(L):
-    from oracle import build_ref
-    return build_ref.lib_path(L, 0).exists()
-
-
 def solves_per_trajectory(md_steps):
     # 2 flavours x (1 initial solve + (2 md_steps + 1) forces), minus the first
     # force, whose start vector is already the solution (conjugategradient.c:16-27)
     return 2 * (1 + 2 * md_steps + 1) - 2
 
 
-def cpu_reference_rate(L, tol, md_steps, procs=1, seed=0):
-    """traj/s of the reference from a bounded sample: per process one full CG
-    solve at L, scaled by the solves of one trajectory.  Returns (rate, info)."""
-    nsol = solves_per_trajectory(md_steps)
-    if reference_available(L):
-        kind = "reference"
-        if procs == 1:
-            res = [_ref_solve_worker((L, tol, seed))]
-        else:
-            import multiprocessing as mp
-            ctx = mp.get_context("spawn")
-            with ctx.Pool(procs) as pool:
-                res = pool.map(_ref_solve_worker, [(L, tol, seed + i) for i in range(procs)])
-    else:
-        kind = "port"
-        res = [_port_solve(L, tol, seed)]
-        procs = 1
-    t_solve = statistics.median(r[0] for r in res)
-    its = statistics.median(r[1] for r in res)
-    rate = procs / (nsol * t_solve)
-    info = {"kind": kind, "cores": procs,
-            "sample": (f"{procs} process(es) x one CG solve from x=0 at L={L} to |r| < {tol:g}|b| "
-                       f"({its:.0f} iterations, {t_solve:.2f} s median), scaled by the {nsol} solves of one "
-                       f"trajectory")}
-    return rate, info
+def cpu_line_fields(r, a):
+    sample = (f"{r['cores']} process(es) of the {'reference' if r['kind'] == 'reference' else 'CPU restatement'}'s "
+              f"serial code, {round(r['value'] * r['wall_s'])} full trajectories (LFMN2VF {a.md_steps} x {a.eps}, "
+              f"L={a.L}, every CG to 1e-10 |phi|, {r['cg_iterations_per_traj']:.0f} CG iterations per trajectory), "
+              f"wall clock from a common start to the last finish")
+    return {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"], "sample": sample}
 
 
 def run_reference(a, world, rank):
+    """The reference arm: a.steps trajectories of the reference's own serial
+    code on the host cores, one process per core; a.warmup Dirac applies per
+    process before the clock starts."""
     if rank != 0:
         return
     ncores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
-    procs = max(1, min(ncores, 64))
-    for _ in range(min(a.warmup, 1)):
-        cpu_reference_rate(a.L, a.tol, a.md_steps, 1)
-    rates, infos = [], []
-    for s in range(a.steps):
-        r, info = cpu_reference_rate(a.L, a.tol, a.md_steps, procs, seed=100 * s)
-        rates.append(r)
-        infos.append(info)
-    value = statistics.median(rates)
+    r = CpuTrajectories(a.L, a.eps, a.md_steps, a.steps, min(ncores, 64), a.warmup).start().result()
+    value = r["value"]
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
-            "ms_per_step": 1000.0 / value * infos[0]["cores"], "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"sigma-HMC LFMN2VF L={a.L} beta_s={BETA_S} steps={a.md_steps} eps={a.eps} "
-                                   f"CG rel {a.tol:g}", "l2": "n/a (CPU)"},
+            "ms_per_step": 1000.0 * r["wall_s"] / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded sigma; the reference's own dSFMT draws)",
+            "config": {"workload": f"sigma-HMC LFMN2VF L={a.L} beta_s={BETA_S} steps={a.md_steps} eps={a.eps}, "
+                                   f"every CG to |r| < {a.tol:g}|phi|", "l2": "n/a (CPU)",
+                       "warmup": f"{a.warmup} Dirac applies per process"},
             "impl": "reference",
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": infos[0]["cores"], "kind": infos[0]["kind"],
-                             "sample": infos[0]["sample"]},
+            "cpu_baseline": cpu_line_fields(r, a),
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -297,9 +353,17 @@ def run_ours(a, world, rank, local):
     import torch
 
     import gn_b200 as G
+    L, V = a.L, a.L ** 3
+    # CPU jobs beside the GPU work (spawned processes, started before the first
+    # CUDA call): one reference trajectory on one core (cpu_baseline), and the
+    # CPU restatement's force at L = 128 for the mixed-precision case
+    cpu_job = l128_job = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cpu_job = CpuTrajectories(L, a.eps, a.md_steps, 1, 1, a.warmup).start()
+    if world == 1 and not a.no_l128:
+        l128_job = L128Oracle().start()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    L, V = a.L, a.L ** 3
     lat = G.Lattice(L, local)
     stream = torch.cuda.ExternalStream(lat.stream, device=dev)
     rng = np.random.default_rng(1231 + rank)
@@ -373,59 +437,78 @@ def run_ours(a, world, rank, local):
     # dominant kernel: one two-flavour mixed CG solve, events around the kernel
     roof = kernel_roofline(lat, stream, a, G)
     dirac = dirac_roofline(G, stream, dev)
-    batched = None
+    peaks = load_peaks()
+    detail = {}
     if world == 1:
-        batched = batched_bench(G, dev)
-        lay = (batched["layout"]["group_blocks"], batched["layout"]["big_min_volume"])
-        batched["fp64"] = {k: v for k, v in batched_bench(G, dev, precision=G.GN_PREC_FP64, layout=lay).items()
-                           if k in ("value", "ms_per_ensemble_trajectory", "cg_iterations_per_chain_trajectory",
-                                    "solver_gbs")}
-    l128 = l128_case(G, dev) if world == 1 else None
-    u1 = u1_case(G, dev) if world == 1 else None
-    serving = None
-    if world == 1:
-        serving = serve_bench(G)
-        serving["fp64"] = {k: v for k, v in serve_bench(G, precision=G.GN_PREC_FP64).items()
-                           if k in ("p50_ms", "p99_ms", "throughput_req_per_s")}
-
+        detail["batched"] = batched_bench(G, dev)
+        lay = (detail["batched"]["layout"]["group_blocks"], detail["batched"]["layout"]["big_min_volume"])
+        detail["batched_fp64"] = batched_bench(G, dev, precision=G.GN_PREC_FP64, layout=lay)
+        if l128_job is not None:
+            detail["l128"] = l128_case(G, dev, oracle=l128_job)
+        detail["u1"] = u1_case(G, dev)
+        detail["serving"] = serve_sweep(G)
     cpu = None
-    if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        rate, info = cpu_reference_rate(L, a.tol, a.md_steps, 1)
-        cpu = {"value": rate, "unit": UNIT, **info}
+    if cpu_job is not None:
+        cpu = cpu_line_fields(cpu_job.result(), a)
 
     mixed, fp64 = results["mixed"], results["fp64"]
     value = world * a.steps / (mixed["ms"] / 1000.0)
     fp64_rate = world * a.steps / (fp64["ms"] / 1000.0)
-    peaks = load_peaks()
     iters = [o["inner_iterations"] for o in mixed["out"]]
+    detail["mixed"] = {"inner_iterations_per_traj": statistics.mean(iters),
+                       "reliable_updates_per_traj": statistics.mean(o["reliable_updates"] for o in mixed["out"]),
+                       "acceptance": statistics.mean(o["accepted"] for o in mixed["out"]),
+                       "dH": [round(o["dH"], 6) for o in mixed["out"]]}
+    detail["fp64"] = {"cg_iterations_per_traj": statistics.mean(o["cg_iterations"] for o in fp64["out"]),
+                      "clocks": fp64["clocks"]}
+    detail["roofline"], detail["dirac_roofline"] = roof, dirac
+    # the line: the contract's keys, then short summaries, the claims last
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": mixed["ms"] / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32 inner / f64 reliable updates, f64 dH", "data": "synthetic (seeded N(0,1) momenta and chi)",
-            "config": {"workload": f"sigma-HMC LFMN2VF L={L} (V={V}) beta_s={BETA_S} steps={a.md_steps} "
-                                   f"eps={a.eps}, every CG to |r| < {a.tol:g}|b| (true residual)",
-                       "L": L, "parallelism": f"replicas x{world}",
-                       "l2": "flushed (512 MB write) before every trajectory, inside the timed region"},
-            "fp64": {"value": fp64_rate, "unit": UNIT, "ms_per_step": fp64["ms"] / a.steps,
-                     "cg_iterations_per_traj": statistics.mean(o["cg_iterations"] for o in fp64["out"])},
-            "mixed_over_fp64": value / fp64_rate,
-            "mixed_detail": {"inner_iterations_per_traj": statistics.mean(iters),
-                             "reliable_updates_per_traj": statistics.mean(o["reliable_updates"] for o in mixed["out"]),
-                             "acceptance": statistics.mean(o["accepted"] for o in mixed["out"]),
-                             "dH": [round(o["dH"], 6) for o in mixed["out"]]},
-            "e2e": {"value": world * a.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 3 * V * 8,
-                    "d2h_bytes_per_step": 2 * V * 8},
-            "roofline": roof_json(roof, peaks),
-            "dirac_roofline": roof_json(dirac, peaks),
-            "cpu_baseline": cpu,
+            "dtype": "f32 inner CG, f64 reliable updates and dH", "data": "synthetic (seeded N(0,1) P and chi)",
+            "config": {"workload": f"sigma-HMC LFMN2VF L={L} beta_s={BETA_S} {a.md_steps} x eps {a.eps}, "
+                                   f"every CG to |r| < {a.tol:g}|phi| (true residual)",
+                       "parallelism": f"replicas x{world}", "l2": "flushed (512 MB write) before every trajectory"},
             "clocks": mixed["clocks"],
             "gpu_launches": int(round(mixed["launches"] * a.steps)),
-            "batched": batched,
-            "serving": serving,
-            "mixed_precision_L128": l128,
-            "u1_model_L64": u1}
+            "e2e": {"value": world * a.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 3 * V * 8,
+                    "d2h_bytes_per_step": 2 * V * 8},
+            "cpu_baseline": cpu,
+            "roofline": roof_json(roof, peaks)}
+    line.update(summaries(detail, peaks))
+    line["dirac_roofline"] = {"kernel": "dirac_item_kernel M, L=256", "achieved_gbs": round(dirac["gbs"], 1),
+                              "frac": round(dirac["gbs"] / peaks["hbm_gbs"], 3)}
+    line["fp64"] = {"value": round(fp64_rate, 3), "ms_per_step": round(fp64["ms"] / a.steps, 2)}
+    line["mixed_over_fp64"] = round(value / fp64_rate, 3)
     if rank == 0:
+        if a.detail:
+            Path(a.detail).parent.mkdir(parents=True, exist_ok=True)
+            Path(a.detail).write_text(json.dumps({"line": line, "detail": detail}, indent=1, default=str))
         print(json.dumps(line), flush=True)
     lat.close()
+
+
+def summaries(d, peaks):
+    """Short forms of the side measurements for the bench line."""
+    out = {}
+    if "batched" in d:
+        b, b64 = d["batched"], d["batched_fp64"]
+        out["batched"] = {"mixed_traj_s": round(b["value"], 1), "fp64_traj_s": round(b64["value"], 1),
+                          "solver_frac": round(b["solver_gbs"] / peaks["hbm_gbs"], 3)}
+    if "serving" in d:
+        s = d["serving"]
+        out["serving"] = {"max_sustained_req_s": s["max_sustained_req_s"],
+                          "mixed": [[r["offered_req_per_s"], round(r["throughput_req_per_s"], 1), round(r["p50_ms"]),
+                                     round(r["p99_ms"])] for r in s["mixed"]],
+                          "cols": "offered/s, done/s, p50 ms, p99 ms"}
+    if "l128" in d:
+        out["l128"] = [{k: (round(v, 3) if k in ("beta_s", "solve_speedup", "trajectory_speedup") else
+                            float(f"{v:.2e}")) for k, v in r.items()
+                        if k in ("beta_s", "x_err_vs_oracle", "force_err_vs_oracle", "dH_err_vs_oracle",
+                                 "solve_speedup", "trajectory_speedup") and v is not None} for r in d["l128"]["rows"]]
+    if "u1" in d:
+        out["u1_mixed_speedup"] = [d["u1"]["u1_sigma_mixed_speedup"], d["u1"]["u1_pi_mixed_speedup"]]
+    return out
 
 
 def load_peaks():
@@ -583,6 +666,17 @@ def serve_bench(G, nreq=600, rate=200.0, warm=24, seed=5, precision=None):
     return out
 
 
+def serve_sweep(G, rates=(25.0, 50.0, 100.0, 150.0, 200.0), nreq=300):
+    """serve_bench at a ladder of offered rates in mixed precision, and at 50/s
+    and 200/s in FP64.  max_sustained_req_s: the highest offered rate whose
+    completion rate (requests over first arrival to last completion) stays
+    within 5 % of it, i.e. where the queue does not grow."""
+    mixed = [serve_bench(G, nreq=nreq, rate=r) for r in rates]
+    fp64 = [serve_bench(G, nreq=nreq, rate=r, precision=G.GN_PREC_FP64) for r in (50.0, 200.0)]
+    sus = [r["offered_req_per_s"] for r in mixed if r["throughput_req_per_s"] >= 0.95 * r["offered_req_per_s"]]
+    return {"mixed": mixed, "fp64": fp64, "max_sustained_req_s": max(sus) if sus else None}
+
+
 def u1_case(G, dev, L=64, md_steps=10, eps=0.05, pi_steps=10, tol=1e-10, reps=2):
     """The U(1) model (PI_INTERACTION) at L = 64: ms per sigma trajectory
     (LFMN2VF md_steps x eps with the complex M, every solve to a true relative
@@ -659,28 +753,100 @@ def u1_case(G, dev, L=64, md_steps=10, eps=0.05, pi_steps=10, tol=1e-10, reps=2)
     return out
 
 
-def l128_case(G, dev, betas=(0.7, 0.85, 1.0), L=128, md_steps=10, eps=0.05, tol=1e-10, reliable=50):
+def _l128_fields(beta, L):
+    """sigma, the trajectory's draws and chi_0, chi_1 of the L = 128 case, in
+    the order they are drawn (also the order tests/golden/make_l128_dH.py uses)."""
+    V = L ** 3
+    rng = np.random.default_rng(int(beta * 100))
+    sigma = rng.normal(0.0, np.sqrt(2.0 / (NFLAV * beta)), V)
+    draws = rng.normal(size=3 * V)
+    chi = np.stack([rng.normal(size=V) for _ in range(2)])
+    return sigma, draws, chi
+
+
+def _l128_oracle_worker(beta, L, tol, path, q):
+    """The CPU restatement's sigma force (ComputeSigmaForce, moleculardynamics.c:631)
+    on the L = 128 case's fields: X = (M M^T)^-1 phi from x = 0 and F, at the
+    absolute tolerance tol * min_f |phi_f|, the one the GPU's force is given."""
+    try:
+        sys.path.insert(0, str(ROOT))
+        from oracle.oracle import Port
+        port = Port()
+        sigma, _, chi = _l128_fields(beta, L)
+        sm = port.sigma_mass(L, sigma)
+        phi = np.stack([port.dirac(L, sm, chi[f], 0) for f in range(2)])
+        tol_abs = tol * float(min(np.linalg.norm(phi[0]), np.linalg.norm(phi[1])))
+        t0 = time.monotonic()
+        F, X, Y, ok, it, calls = port.force(L, beta, sigma, sm, phi, np.zeros((2, L ** 3)), tol_abs)
+        np.savez(path, F=F, X=X)
+        q.put((beta, path, ok, it, time.monotonic() - t0, None))
+    except Exception as e:
+        q.put((beta, None, False, 0, 0.0, repr(e)))
+
+
+class L128Oracle:
+    """The oracle side of the L = 128 case: the force and X from the CPU
+    restatement (a spawned process per beta_s, about a minute each), and dH of
+    one trajectory from the fixture tests/golden/oracle_L128_dH.json (about 15
+    CPU minutes per beta_s, made by tests/golden/make_l128_dH.py)."""
+
+    def __init__(self, betas=(0.85,), L=128, tol=1e-10):
+        import multiprocessing as mp
+        ctx = mp.get_context("spawn")
+        self.dir = tempfile.mkdtemp(prefix="gn_l128_")
+        self.q = ctx.Queue()
+        self.ps = [ctx.Process(target=_l128_oracle_worker, daemon=True,
+                               args=(b, L, tol, os.path.join(self.dir, f"b{b}.npz"), self.q)) for b in betas]
+        self.res = None
+        fx = ROOT / "tests" / "golden" / "oracle_L128_dH.json"
+        self.dH = {}
+        if fx.exists():
+            self.dH = {round(r["beta_s"], 6): r["dH"] for r in json.loads(fx.read_text())["rows"] if r["ok"]}
+
+    def start(self):
+        for p in self.ps:
+            p.start()
+        return self
+
+    def force(self, beta):
+        """(X, F, seconds) of the oracle at beta_s, or None if it was not asked for."""
+        if self.res is None:
+            self.res = {}
+            for _ in self.ps:
+                b, path, ok, it, dt, err = self.q.get(timeout=1800)
+                if err is None and ok:
+                    d = np.load(path)
+                    self.res[round(b, 6)] = (d["X"], d["F"], dt)
+                    os.unlink(path)
+            for p in self.ps:
+                p.join(timeout=60)
+        return self.res.get(round(beta, 6))
+
+
+def l128_case(G, dev, betas=(0.7, 0.85, 1.0), L=128, md_steps=10, eps=0.05, tol=1e-10, reliable=50, oracle=None):
     """Mixed precision at L = 128 (V = 2,097,152): FP32 fields and inner CG,
     FP64 reliable updates at least every `reliable` iterations, FP64 dH and
-    Metropolis.  Per beta_s, against the FP64 path on the same fields (sigma
-    ~ N(0, 2/(N_f beta_s)), chi ~ N(0, 1), phi = M chi): the relative error of
-    x = (M M^T)^-1 phi and of the sigma force (both solved to a true relative
-    residual of 1e-10), |dH_mixed - dH_fp64| of one trajectory from the same
-    state and draws (LFMN2VF md_steps x eps), the iteration counts and the
-    solve and trajectory times (CUDA events)."""
+    Metropolis.  Per beta_s (sigma ~ N(0, 2/(N_f beta_s)), chi ~ N(0, 1),
+    phi = M chi), FP64 and mixed on the same fields:
+      - against the FP64 oracle (`oracle`, an L128Oracle): the relative error
+        of X = (M M^T)^-1 phi and of the sigma force, both solved to the same
+        tolerance, and |dH - dH_oracle| of one trajectory from the same state
+        and draws (LFMN2VF md_steps x eps, every solve to 1e-10 |b|);
+      - against the GPU's own FP64 path: the relative error of x, of the force
+        and of dH;
+      - the iteration counts and the solve and trajectory times (CUDA events)."""
     import torch
     rows = []
     V = L ** 3
     for beta in betas:
-        rng = np.random.default_rng(int(beta * 100))
-        sigma = rng.normal(0.0, np.sqrt(2.0 / (NFLAV * beta)), V)
-        draws = torch.tensor(rng.normal(size=3 * V), dtype=torch.float64, device=dev)
+        sigma, draws_h, chi = _l128_fields(beta, L)
+        draws = torch.tensor(draws_h, dtype=torch.float64, device=dev)
         with G.Lattice(L, dev.index) as lat:
             lat.set_reliable_interval(reliable)
             st = torch.cuda.ExternalStream(lat.stream, device=dev)
             lat.load_sigma(sigma)
             sm = lat.store_sigma()[1]
-            phi = np.stack([lat.dirac(sm, rng.normal(size=V), G.GN_OP_M) for _ in range(2)])
+            phi = np.stack([lat.dirac(sm, chi[f], G.GN_OP_M) for f in range(2)])
             row = {"beta_s": beta}
             out = {}
             for prec, name in ((G.GN_PREC_FP64, "fp64"), (G.GN_PREC_MIXED, "mixed")):
@@ -705,17 +871,32 @@ def l128_case(G, dev, betas=(0.7, 0.85, 1.0), L=128, md_steps=10, eps=0.05, tol=
                                           tol_medium=tol, tol_high=tol, relative=True, precision=prec)
                 t1.record(st)
                 t1.synchronize()
-                out[name] = dict(x=x, F=F, dH=r["dH"])
+                out[name] = dict(x=x, X=X, F=F, dH=r["dH"])
                 row[name] = {"iterations": int(max(i["inner_iterations"] for i in infos)),
                              "reliable_updates": int(sum(i["reliable_updates"] for i in infos)),
                              "solve_ms": e0.elapsed_time(e1), "trajectory_ms": t0.elapsed_time(t1),
-                             "trajectory_cg_iterations": r["cg_iterations"]}
-            row["x_rel_err"] = float(np.linalg.norm(out["mixed"]["x"] - out["fp64"]["x"]) /
-                                     np.linalg.norm(out["fp64"]["x"]))
-            row["force_rel_err"] = float(np.linalg.norm(out["mixed"]["F"] - out["fp64"]["F"]) /
-                                         np.linalg.norm(out["fp64"]["F"]))
+                             "trajectory_cg_iterations": r["cg_iterations"], "dH": r["dH"]}
+
+            def rerr(u, v):
+                return float(np.linalg.norm(u - v) / np.linalg.norm(v))
+            row["x_rel_err"] = rerr(out["mixed"]["x"], out["fp64"]["x"])
+            row["force_rel_err"] = rerr(out["mixed"]["F"], out["fp64"]["F"])
             row["dH_abs_diff"] = abs(out["mixed"]["dH"] - out["fp64"]["dH"])
-            row["dH_fp64"] = out["fp64"]["dH"]
+            orc = oracle.force(beta) if oracle is not None else None
+            if orc is not None:
+                Xo, Fo, secs = orc
+                for name in ("fp64", "mixed"):
+                    row[name]["X_err_vs_oracle"] = rerr(out[name]["X"], Xo)
+                    row[name]["force_err_vs_oracle"] = rerr(out[name]["F"], Fo)
+                row["x_err_vs_oracle"] = row["mixed"]["X_err_vs_oracle"]
+                row["force_err_vs_oracle"] = row["mixed"]["force_err_vs_oracle"]
+                row["oracle_force_cpu_s"] = round(secs, 1)
+            dHo = oracle.dH.get(round(beta, 6)) if oracle is not None else None
+            if dHo is not None:
+                row["dH_oracle"] = dHo
+                for name in ("fp64", "mixed"):
+                    row[name]["dH_err_vs_oracle"] = abs(out[name]["dH"] - dHo)
+                row["dH_err_vs_oracle"] = row["mixed"]["dH_err_vs_oracle"]
             row["iteration_overhead"] = row["mixed"]["iterations"] / row["fp64"]["iterations"] - 1.0
             row["solve_speedup"] = row["fp64"]["solve_ms"] / row["mixed"]["solve_ms"]
             row["trajectory_speedup"] = row["fp64"]["trajectory_ms"] / row["mixed"]["trajectory_ms"]
@@ -756,6 +937,58 @@ def dirac_roofline(G, stream, dev, reps=20, L=256):
             "note": f"{ms * 1e3:.1f} us per launch, {reps} back-to-back launches on 384 MB (> L2)"}
 
 
+def ens_case(G, dev, nchains=48, ntraj=2):
+    """A small batched ensemble for a profiler: nchains chains with L drawn
+    from the benchmark's mix {8, 12, 16, 24, 32, 48}, the benchmark's layout
+    (teams of 4 blocks for L >= 16), LFMN2VF 8 x 0.08, mixed precision to
+    1e-10, launched without the graph: per trajectory the refresh launch, one
+    launch per MD step and the final one."""
+    rng = np.random.default_rng(4242)
+    Ls = [int(x) for x in rng.choice([8, 12, 16, 24, 32, 48], size=nchains)]
+    betas = list(np.linspace(0.5, 1.2, nchains))
+    p = G.Ensemble.params(0.08, 8)
+    with G.Ensemble(Ls, betas, seed=1231) as e:
+        for c, (L, b) in enumerate(zip(Ls, betas)):
+            e.load_sigma(c, rng.normal(0.0, np.sqrt(2.0 / (NFLAV * b)), L ** 3))
+        e.set_layout(4, 16 ** 3)
+        e.run(p, ntraj, graph=False)
+        st = e.stats()
+    return {"chains": nchains, "sites": sum(L ** 3 for L in Ls), "trajectories": ntraj,
+            "cg_iterations": sum(s["cg_iterations"] for s in st)}
+
+
+def kernels_case(G, dev, L=160):
+    """One launch of each small kernel of the path at L = 160 (V = 4,096,000;
+    an FP64 plane is 33 MB, so every kernel's inputs exceed the L2): sigma
+    mass, M, M^T, the sigma force's gather (its CG exits at the start: X is
+    given with a tolerance of 1e300), the energy, the condensate's source and
+    dot kernels (solves exit at once the same way), and the U(1) model's
+    complex-mass M, force and energy."""
+    V = L ** 3
+    rng = np.random.default_rng(160)
+    sigma = rng.normal(0.0, np.sqrt(2.0 / (NFLAV * BETA_S)), V)
+    pi = rng.normal(0.0, np.sqrt(2.0 / (NFLAV * BETA_S)), V)
+    with G.Lattice(L, dev.index) as lat:
+        sm = lat.sigma_mass(sigma)
+        psi = rng.normal(size=V)
+        lat.dirac(sm, psi, G.GN_OP_M)
+        lat.dirac(sm, psi, G.GN_OP_MT)
+        phi = rng.normal(size=(2, V))
+        X = rng.normal(size=(2, V))
+        lat.sigma_force(BETA_S, sigma, sm, phi, X, 1e300)
+        lat.energy(BETA_S, sigma, rng.normal(size=V), phi, X)
+        lat.condensate(sm, 1e300, np.zeros(V, complex), lambda: float(rng.uniform()))
+        lat.load_pi(pi)
+        pm = lat.store_pi()[1]
+        z = psi + 1j * rng.normal(size=V)
+        lat.dirac_u1(sm, pm, z, G.GN_OP_M)
+        phic = phi + 1j * rng.normal(size=(2, V))
+        Xc = X + 1j * rng.normal(size=(2, V))
+        lat.sigma_force_u1(BETA_S, sigma, sm, pm, phic, Xc, 1e300)
+        lat.energy_u1(0, BETA_S, sigma, rng.normal(size=V), phic, Xc)
+    return {"L": L, "V": V}
+
+
 def run_case(a):
     """Small cases for ncu: cg64 = one two-flavour CG solve at L=64 in FP64 and in
     mixed precision; dirac128 / dirac256 = 3 Dirac applies at L=128 / 256; traj64 = one
@@ -768,14 +1001,17 @@ def run_case(a):
         r = dirac_roofline(G, None, dev, reps=3, L=128 if a.case == "dirac128" else 256)
         print(json.dumps(r))
         return
-    if a.case == "cgscan":
-        cg_scan(G, dev)
-        return
     if a.case == "l128":
-        print(json.dumps(l128_case(G, dev)))
+        print(json.dumps(l128_case(G, dev, oracle=L128Oracle().start())))
         return
     if a.case == "u1":
         print(json.dumps(u1_case(G, dev)))
+        return
+    if a.case == "ens":
+        print(json.dumps(ens_case(G, dev)))
+        return
+    if a.case == "kernels":
+        print(json.dumps(kernels_case(G, dev)))
         return
     if a.case == "batched":
         r = batched_bench(G, dev)
@@ -784,10 +1020,7 @@ def run_case(a):
         print(json.dumps(batched_bench(G, dev, precision=G.GN_PREC_FP64, layout=lay)), flush=True)
         return
     if a.case == "serve":
-        for prec in (G.GN_PREC_MIXED, G.GN_PREC_FP64):
-            print(json.dumps(serve_bench(G, precision=prec)), flush=True)
-        for prec in (G.GN_PREC_MIXED, G.GN_PREC_FP64):  # a load the GPU sustains
-            print(json.dumps(serve_bench(G, nreq=300, rate=50.0, precision=prec)), flush=True)
+        print(json.dumps(serve_sweep(G)), flush=True)
         return
     L, V = 64, 64 ** 3
     lat = G.Lattice(L, 0)
@@ -807,36 +1040,6 @@ def run_case(a):
                                   a.tol, 1, True, 0, prec)
         print(json.dumps({"precision": prec, "status": st, "info": infos}))
     lat.close()
-
-
-def cg_scan(G, dev, iters=100):
-    """Time per iteration of the persistent solvers against L: two flavours,
-    exactly `iters` iterations (tolerance 0), FP64 and mixed, CUDA events."""
-    import torch
-    for L in (8, 16, 24, 32, 48, 64, 96, 128):
-        V = L ** 3
-        lat = G.Lattice(L, dev.index)
-        rng = np.random.default_rng(L)
-        lat.load_sigma(rng.normal(0.0, np.sqrt(2.0 / (NFLAV * BETA_S)), V))
-        lat.write_state(G.GN_F_PHI, rng.normal(size=2 * V))
-        stream = torch.cuda.ExternalStream(lat.stream, device=dev)
-        row = {"L": L, "V": V}
-        for prec, name in ((G.GN_PREC_FP64, "fp64"), (G.GN_PREC_MIXED, "mixed")):
-            ts = []
-            for rep in range(3):
-                e0, e1 = cuda_events()
-                e0.record(stream)
-                infos, st = lat.cg_device(lat.field_ptr(G.GN_F_SM), lat.field_ptr(G.GN_F_PHI),
-                                          lat.field_ptr(G.GN_F_X), 2, 1, 0.0, 1, False, iters, prec)
-                e1.record(stream)
-                e1.synchronize()
-                ts.append(e0.elapsed_time(e1))
-            ms = min(ts)
-            wbytes = 8 if prec == G.GN_PREC_FP64 else 4
-            row[name + "_us_per_iter"] = round(1000.0 * ms / iters, 2)
-            row[name + "_GBs"] = round(V * (2 * wbytes + 20 * wbytes) * iters / (ms * 1e-3) / 1e9, 1)
-        print(json.dumps(row), flush=True)
-        lat.close()
 
 
 def main():

@@ -368,18 +368,22 @@ GN_API int gn_flush_l2(gn_context *ctx);
 
 /* No counterpart in the reference (it is an addition of this library).
  * CG on (M M^T) x = b for one real right-hand side, like gn_cg_device with
- * precision GN_PREC_FP64, for callers that cannot allocate device memory --
- * host codes that size all of their buffers once up front, code running under
- * an external pool allocator, code recorded into a CUDA graph.  It needs no
- * gn_context and calls no cudaMalloc / cudaFree: the solver's scratch is a
- * static device array of about 1 MiB, sized for L <= 32 (32768 sites), that
- * every GPU loading this library holds until exit.  Larger L returns
- * GN_ERR_ARG.  sigmamass, b (input) and x (in/out) are device pointers of V
- * doubles on the current device; stream is a cudaStream_t (NULL = default).
- * All calls share the static array: calls that overlap on the GPU race, so
- * order them.  The first call on each device sets up the array's address and
- * should come before any stream capture.  Returns like gn_cg;
- * gn_cg_noalloc_error() describes the last failure of the calling thread. */
+ * precision GN_PREC_FP64, for callers that cannot allocate device memory once
+ * they run: an HMC driver that sizes all of its buffers once up front, as the
+ * reference's Allocate* functions do, or an application that gives this
+ * library a fixed budget from its own pool allocator, where a cudaMalloc
+ * would escape the budget or fail.  It needs no gn_context and calls no
+ * cudaMalloc / cudaFree: the solver's scratch is a static device array of
+ * about 1 MiB, sized for L <= 32 (32768 sites), that every GPU loading this
+ * library holds until exit.  Larger L returns GN_ERR_ARG.  sigmamass, b
+ * (input) and x (in/out) are device pointers of V doubles on the current
+ * device; stream is a cudaStream_t (NULL = default).  All calls share the
+ * static array: calls that overlap on the GPU race, and so do calls from
+ * several host threads on one stream, so serialise whole calls on the host.
+ * The first call on each device sets up the array's address and should come
+ * before any stream capture.  Returns like gn_cg; gn_cg_noalloc_error()
+ * describes the failure of the calling thread's last call ("" after a call
+ * that did not fail). */
 GN_API int gn_cg_noalloc(int L, const double *sigmamass, const double *b, double *x, double tol, int variant,
                          int relative, long long max_iter, void *stream, gn_cg_info *info);
 GN_API const char *gn_cg_noalloc_error(void);

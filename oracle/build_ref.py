@@ -12,8 +12,13 @@ Flags follow the reference README's build line (``gcc -O3 *.c -lm``), plus
 files include) and ``-fPIC -shared`` so ctypes can load the result.  test.c
 (the reference ``main``) is left out; the harness replaces it.
 
-Usage:  python oracle/build_ref.py [--L 4 8 16 ...] [--integrator 0 1 2]
-Outputs: oracle/_ref/libgnref_L{L}_i{I}.so
+The reference tree is taken from --reference DIR, else from the environment
+variable GN_REFERENCE_DIR, else from a directory named "reference" beside the
+repository's own directory.  Without it nothing is built, and the objects
+already under oracle/_ref/ are used as they are.
+
+Usage:  python oracle/build_ref.py [--reference DIR] [--L 4 8 16 ...] [--integrator 0 1 2]
+Outputs: oracle/_ref/libgnref_L{L}_i{I}{tag}.so
 """
 from __future__ import annotations
 
@@ -26,10 +31,12 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
-REF_DIR = Path(os.environ.get("GN_REFERENCE_DIR", "/root/reference"))
+REF_DIR = Path(os.environ.get("GN_REFERENCE_DIR") or HERE.parent.parent / "reference")
 
 DEFAULT_L = (4, 6, 8, 12, 16, 24, 32, 48, 64)
 PI_DEFS, PI_TAG = ("-DPI_INTERACTION",), "_pi"  # the U(1) model's build
+# every CG stopped at 1e-10 |phi| (ref_config.h): the benchmark's CPU arm
+REL_DEFS, REL_TAG = ("-DGN_REF_RELATIVE_TOL=1e-10",), "_rel"
 CFLAGS = ["-O3", "-fcommon", "-fPIC", "-w"]
 
 
@@ -85,15 +92,21 @@ def build_all(Ls=DEFAULT_L, integrators=(0,)) -> list[Path]:
     # the U(1) model (PI_INTERACTION): the test sizes and the benchmark's L = 64
     for L in (4, 8, 64):
         built.append(build(L, 0, PI_DEFS, PI_TAG))
+    # the benchmark's workload (L = 64, every solve to 1e-10 |phi|) for the CPU baseline
+    built.append(build(64, 0, REL_DEFS, REL_TAG))
     return built
 
 
 def main() -> int:
+    global REF_DIR
     ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default=None, help="the reference's source tree")
     ap.add_argument("--L", type=int, nargs="*", default=list(DEFAULT_L))
     ap.add_argument("--integrator", type=int, nargs="*", default=[0])
     ap.add_argument("--force", action="store_true")
     a = ap.parse_args()
+    if a.reference:
+        REF_DIR = Path(a.reference)
     if not available():
         print(f"reference not present at {REF_DIR}; nothing to build", file=sys.stderr)
         return 0

@@ -179,6 +179,8 @@ static double norm_fermion(const double *v, long V, int ncomp)
  *            START_X0_NULL: early exit when the incoming x already satisfies tol);
  * variant 1: StartX0ImposedConjugateGradient... (conjugategradient.c:115-182).
  * Solves (M M^T) x = b, absolute stop ||r|| < tol, at most max_iter iterations.
+ * A negative tol asks for the relative stop ||r|| < |tol| ||b|| instead (the
+ * benchmark's rule; the reference's own callers always pass tol > 0).
  * Returns 1 on convergence.  *iters = iteration+1 and *counted = 1 when the
  * reference would add to kit->iterations / kit->CG_call; 0 on an early exit. */
 int gno_cg(int L, const double *sm, const double *b, double *x, int ncomp, double tol, int variant, long max_iter,
@@ -191,6 +193,7 @@ int gno_cg(int L, const double *sm, const double *b, double *x, int ncomp, doubl
     int ok = 0;
     *iters = 0;
     *counted = 0;
+    if (tol < 0.0) tol = -tol * norm_fermion(b, V, ncomp);
     if (variant == 0) {
         memcpy(r, b, sizeof(double) * n);
         gno_dirac(L, sm, x, t1, ncomp, 1);

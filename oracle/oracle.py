@@ -269,6 +269,13 @@ class Ref:
     def uniform(self, n):
         return np.array([self.lib.gnref_casuale() for _ in range(n)])
 
+    def rng_save(self):
+        """Keep a copy of the global dSFMT state (random.c:9), to replay the same draws."""
+        self.lib.gnref_rng_save()
+
+    def rng_restore(self):
+        self.lib.gnref_rng_restore()
+
     def fn_ptrs(self):
         return (C.cast(self.lib.gnref_gauss1, C.c_void_p).value, C.cast(self.lib.gnref_casuale, C.c_void_p).value)
 

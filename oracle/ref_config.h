@@ -15,7 +15,13 @@
  *      2 = LFMN2SIGMA), so that the alternative integrators of
  *      moleculardynamics.c:859 and :1018 can be pinned as well;
  *   - the CG tolerances can be overridden with -DGN_REF_MEDIUM_TOL /
- *     -DGN_REF_HIGH_TOL (macro.h:135-136), used only by the CPU baseline.
+ *     -DGN_REF_HIGH_TOL (macro.h:135-136), used only by the CPU baseline;
+ *   - with -DGN_REF_RELATIVE_TOL=t both tolerances become t |phi|, evaluated
+ *     at each solve by gnref_relative_tolerance() (ref_harness.c), so that the
+ *     reference's absolute stopping test |r| < tol (conjugategradient.c:94)
+ *     is the relative test of the benchmark workload.  The macro is read where
+ *     the integrators pass it (moleculardynamics.c:1263, :1279, ...), so the
+ *     reference's code is unchanged.
  */
 #ifndef MACRO_H
 #define MACRO_H
@@ -88,6 +94,11 @@
 /* conjugate gradient (macro.h:129-136) */
 #define START_X0_NULL
 #define MAX_CONJUGATE_GRADIENT_ITERATION (VOLUME + 1)
+#ifdef GN_REF_RELATIVE_TOL
+double gnref_relative_tolerance(void);
+#define MEDIUM_PRECISION_INVERSION (gnref_relative_tolerance())
+#define HIGH_PRECISION_INVERSION (gnref_relative_tolerance())
+#else
 #ifdef GN_REF_MEDIUM_TOL
 #define MEDIUM_PRECISION_INVERSION (GN_REF_MEDIUM_TOL)
 #else
@@ -97,6 +108,7 @@
 #define HIGH_PRECISION_INVERSION (GN_REF_HIGH_TOL)
 #else
 #define HIGH_PRECISION_INVERSION (1e-9)
+#endif
 #endif
 
 /* condensate noise (macro.h:146) */

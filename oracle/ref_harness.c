@@ -211,6 +211,26 @@ void gnref_kit_get(int which, int f, double complex *v) { memcpy(v, kit_vec(whic
 void gnref_counters(double *iterations, int *calls) { *iterations = g_kit.iterations; *calls = g_kit.CG_call; }
 void gnref_reset_counters(void) { g_kit.iterations = 0.0; g_kit.CG_call = 0; }
 
+#ifdef GN_REF_RELATIVE_TOL
+/* The CG tolerance of a build with -DGN_REF_RELATIVE_TOL=t (ref_config.h):
+ * t times the smaller of the flavours' |phi_f| at the time of the call.  Every
+ * solve of a trajectory has b = phi_f (moleculardynamics.c:1263, :596), so the
+ * reference's absolute test |r| < tol becomes |r| < t |phi|, the benchmark's
+ * relative stopping rule.  The flavours' norms differ by ~1/sqrt(V); taking
+ * the smaller makes the larger flavour's test slightly stricter, never looser. */
+double gnref_relative_tolerance(void)
+{
+    double m = -1.0;
+    for (int f = 0; f < HALFNFLAV; f++) {
+        const double complex *v = g_kit.phi.flav[f].fermion;
+        double s = 0.0;
+        for (int x = 0; x < VOLUME; x++) s += creal(v[x]) * creal(v[x]) + cimag(v[x]) * cimag(v[x]);
+        if (m < 0.0 || s < m) m = s;
+    }
+    return (GN_REF_RELATIVE_TOL) * sqrt(m);
+}
+#endif
+
 /* ---------------- Dirac (dirac.c) ---------------- */
 /* which: 0 = DiracFermion (dirac.c:46), 1 = AdjDiracFermion (dirac.c:88),
  *        2 = SubtractDiracFermion (dirac.c:213; out is read and updated) */

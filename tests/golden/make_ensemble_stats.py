@@ -1,9 +1,10 @@
 """Equilibrium statistics of the reference's own sigma-HMC chains, the
 yardstick of the batched GPU chains (tests/test_gpu_ensemble.py).
 
-For L = 8 and beta_s in BETAS the reference (compiled in place by
-oracle/build_ref.py, CG tolerances tightened to 1e-9 absolute, i.e. about
-5e-11 relative at this size) runs LFMN2VF trajectories with eps = 0.08, 8 MD
+For L (8 by default; 12 and 16 too) and beta_s in BETAS the reference
+(compiled in place by oracle/build_ref.py, CG tolerances tightened to 1e-9
+absolute, about 5e-11 relative at L = 8 and 1e-11 at L = 16) runs LFMN2VF
+trajectories with eps = 0.08, 8 MD
 steps, from sigma ~ N(0, 2/(N_f beta_s)), seed 1231: THERM trajectories of
 thermalisation, then NMEAS measured ones.  Recorded per beta_s, each with an
 error from binning:
@@ -13,13 +14,15 @@ error from binning:
   of sigma_bar: the model's Z2 symmetry maps sigma -> -sigma and tr1 -> -tr1,
   and a chain in the broken phase stays in one of the two vacua, so only the
   oriented value is comparable between chains.
-Output: tests/golden/ensemble_reference_L8.json.
+The three beta_s run in parallel processes.
+Output: tests/golden/ensemble_reference_L{L}.json.
 
-Usage: python tests/golden/make_ensemble_stats.py
+Usage: python tests/golden/make_ensemble_stats.py [L]
 """
 from __future__ import annotations
 
 import json
+import multiprocessing as mp
 import sys
 import tempfile
 from pathlib import Path
@@ -31,7 +34,7 @@ sys.path.insert(0, str(HERE.parent.parent))
 
 from oracle.oracle import Ref  # noqa: E402
 
-L = 8
+L = int(sys.argv[1]) if len(sys.argv) > 1 and __name__ == "__main__" else 8
 BETAS = (0.6, 0.85, 1.1)
 EPS, STEPS = 0.08, 8
 THERM, NMEAS, NBIN, COND_EVERY = 200, 2000, 20, 20
@@ -44,7 +47,8 @@ def binned(x, nbin=NBIN):
     return float(x.mean()), float(b.std(ddof=1) / np.sqrt(nbin))
 
 
-def run(beta):
+def run(args):
+    L, beta = args
     ref = Ref(L, 0, extra_defs=TIGHT, tag="_tight")
     ref.init(1231, beta, EPS, STEPS)
     rng = np.random.default_rng(int(beta * 1000))
@@ -74,10 +78,12 @@ def run(beta):
 
 def main():
     res = {"L": L, "eps": EPS, "steps": STEPS, "integrator": 0, "therm": THERM, "betas": {}}
-    for b in BETAS:
-        res["betas"][str(b)] = run(b)
-        print(b, res["betas"][str(b)], flush=True)
-    (HERE / "ensemble_reference_L8.json").write_text(json.dumps(res, indent=1) + "\n")
+    Ref(L, 0, extra_defs=TIGHT, tag="_tight")  # build once, before the workers load it
+    with mp.get_context("spawn").Pool(len(BETAS)) as pool:
+        for b, r in zip(BETAS, pool.map(run, [(L, b) for b in BETAS])):
+            res["betas"][str(b)] = r
+            print(b, r, flush=True)
+    (HERE / f"ensemble_reference_L{L}.json").write_text(json.dumps(res, indent=1) + "\n")
 
 
 if __name__ == "__main__":

@@ -3,7 +3,7 @@ lattice sizes in persistent kernels per MD step, replayed as a CUDA graph,
 with device Philox random numbers.
 
 - Statistics agree with the reference's own chains within statistical errors
-  (tests/golden/ensemble_reference_L8.json, made by
+  (tests/golden/ensemble_reference_L{8,12,16}.json, made by
   tests/golden/make_ensemble_stats.py) for three beta_s: acceptance,
   <sigma^2>, <|sigma_bar|> and the condensate oriented by the sign of
   sigma_bar (the Z2 symmetry sigma -> -sigma flips tr1 with it; a chain in the
@@ -56,9 +56,10 @@ def test_chain_alone_equals_chain_in_mix():
         assert st["accepted"] == st_alone["accepted"] and st["sum_dH"] == st_alone["sum_dH"]
 
 
-def test_ensemble_statistics_vs_reference():
+@pytest.mark.parametrize("L0", [8, 12, 16])
+def test_ensemble_statistics_vs_reference(L0):
     import gn_b200 as G
-    ref = json.loads((GOLD / "ensemble_reference_L8.json").read_text())
+    ref = json.loads((GOLD / f"ensemble_reference_L{L0}.json").read_text())
     L, nper = ref["L"], 32
     betas = [float(b) for b in ref["betas"]]
     Ls = [L] * (nper * len(betas))
@@ -72,7 +73,7 @@ def test_ensemble_statistics_vs_reference():
     with G.Ensemble(Ls, bet, seed=2024) as e:
         for c, b in enumerate(bet):
             e.load_sigma(c, _sigma0(L, b, 1000 + c))
-        e.run(p, 100)  # thermalisation
+        e.run(p, 100 if L <= 8 else 200)  # thermalisation
         e.stats(reset=True)
         for k in range(nchunk):
             e.run(p, per)
