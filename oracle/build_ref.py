@@ -92,8 +92,10 @@ def build_all(Ls=DEFAULT_L, integrators=(0,)) -> list[Path]:
     # the U(1) model (PI_INTERACTION): the test sizes and the benchmark's L = 64
     for L in (4, 8, 64):
         built.append(build(L, 0, PI_DEFS, PI_TAG))
-    # the benchmark's workload (L = 64, every solve to 1e-10 |phi|) for the CPU baseline
-    built.append(build(64, 0, REL_DEFS, REL_TAG))
+    # every solve to 1e-10 |phi|: the benchmark's workload (L = 64) for the CPU
+    # baseline, and L = 8 for the test of the reference arm
+    for L in (8, 64):
+        built.append(build(L, 0, REL_DEFS, REL_TAG))
     return built
 
 
