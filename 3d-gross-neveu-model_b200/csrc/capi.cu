@@ -609,6 +609,11 @@ int gn_md_evolve(gn_context *ctx, const gn_hmc_params *params, gn_traj_result *r
   });
 }
 
+int gn_evolve_sigma_in_time(gn_context *ctx, const gn_hmc_params *params, gn_traj_result *res) {
+  if (!params || !res) return fail(GN_ERR_ARG, "null pointer");
+  return guarded(ctx, [&](gn::Engine &E) { return E.evolve_in_time(*params, res); });
+}
+
 long long gn_launch_count(gn_context *ctx) { return (ctx && ctx->eng) ? ctx->eng->launches : 0; }
 
 int gn_flush_l2(gn_context *ctx) {

@@ -297,6 +297,42 @@ bool trajectory(Lattice *lattice, Info *info, Forcesigma *force, Momentasigma *m
   return true;
 }
 
+#ifndef GN_DROPIN_PI
+// The reference's EvolveSigmaInTime* helpers (moleculardynamics.c:1460-1625)
+// on the GPU: the fields they read go up, gn_evolve_sigma_in_time runs the
+// helper's steps, and the fields they write come back.
+void evolve_in_time(Lattice *lattice, Info *info, Forcesigma *force, Momentasigma *momenta, Fermionkit *kit,
+                    double epsilon, int step, int integrator) {
+  gn_context *c = ctx();
+  if (gn_load_sigma(c, lattice->sigma) != GN_OK) fatal("gn_load_sigma");
+  pair_to_real(kit->phi, g_a.data());
+  pair_to_real(kit->inverted_phi, g_b.data());
+  if (gn_write_state(c, GN_F_P, momenta->momenta) != GN_OK || gn_write_state(c, GN_F_PHI, g_a.data()) != GN_OK ||
+      gn_write_state(c, GN_F_X, g_b.data()) != GN_OK)
+    fatal("gn_write_state");
+  gn_hmc_params hp;
+  hp.beta_s = info->beta_scalar;
+  hp.eps = epsilon;
+  hp.steps = step;
+  hp.integrator = integrator;
+  hp.tol_medium = g_tol_medium;
+  hp.tol_high = g_tol_high;
+  hp.relative = 0;
+  hp.precision = g_precision;
+  gn_traj_result r;
+  if (gn_evolve_sigma_in_time(c, &hp, &r) < 0) fatal("gn_evolve_sigma_in_time");
+  if (gn_store_sigma(c, lattice->sigma, lattice->sigmamass) != GN_OK) fatal("gn_store_sigma");
+  if (gn_read_state(c, GN_F_P, momenta->momenta) != GN_OK || gn_read_state(c, GN_F_F, force->force) != GN_OK ||
+      gn_read_state(c, GN_F_X, g_a.data()) != GN_OK || gn_read_state(c, GN_F_Y, g_b.data()) != GN_OK)
+    fatal("gn_read_state");
+  real_to_pair(g_a.data(), kit->inverted_phi);
+  real_to_pair(g_b.data(), kit->inverted_phi_obs);
+  kit->iterations += r.cg_iterations;
+  kit->CG_call += int(r.cg_calls);
+  lattice->distance_sigma += r.distance;
+}
+#endif
+
 #ifdef GN_DROPIN_PI
 void draw_pair(double *a, double *b) { g_gauss2(a, b, 0.0, 1.0); }  // DrawPiMomentaFromGaussianDistribution
 
@@ -471,6 +507,21 @@ bool LeapFrog2MinimumNormSigmaVelocityFirst(Lattice *lattice, Info *info, Forces
                                             const char *acceptance_file) {
   return trajectory(lattice, info, force, momenta, kit, epsilon, step, acceptance_file, GN_LFMN2VF);
 }
+#ifndef GN_DROPIN_PI
+void EvolveSigmaInTimeLF2(Lattice *lattice, Info *info, Forcesigma *force, Momentasigma *momenta, const Fermioncoor *,
+                          Fermionkit *kit, double epsilon, const int step) {
+  evolve_in_time(lattice, info, force, momenta, kit, epsilon, step, GN_LF2);
+}
+void EvolveSigmaInTimeMinimumNormLF2(Lattice *lattice, Info *info, Forcesigma *force, Momentasigma *momenta,
+                                     const Fermioncoor *, Fermionkit *kit, double epsilon, const int step) {
+  evolve_in_time(lattice, info, force, momenta, kit, epsilon, step, GN_LFMN2);
+}
+void EvolveSigmaInTimeMinimumNormSigmaVelocityFirst(Lattice *lattice, Info *info, Forcesigma *force,
+                                                    Momentasigma *momenta, const Fermioncoor *, Fermionkit *kit,
+                                                    double epsilon, const int step) {
+  evolve_in_time(lattice, info, force, momenta, kit, epsilon, step, GN_LFMN2VF);
+}
+#endif
 
 void ComputeCondensateDirac(const Lattice *lat, double *tr1, double *tr1_abs, double *tr2, double *tr4, double *mu2,
                             double *mu4, double *chi, double *chi_abs, double *chip, double *c12_nosigma,

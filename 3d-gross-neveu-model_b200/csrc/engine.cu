@@ -416,6 +416,71 @@ int Engine::trajectory(const gn_hmc_params &hp, double (*gauss)(void), double (*
   return GN_OK;
 }
 
+// The reference's MD helpers (moleculardynamics.c:1460-1625) as they behave:
+// every solve's bool is ignored; a force whose solve fails is left at zero
+// (ComputeSigmaForce zeroes it first, :634) and its flavour loop stops at the
+// failure; sigma is never restored.
+int Engine::evolve_in_time(const gn_hmc_params &hp, gn_traj_result *res) {
+  TraceRange tr("gn evolve in time");
+  if (hp.steps < 1) throw GnError(GN_ERR_ARG, "steps must be >= 1");
+  if (hp.integrator < 0 || hp.integrator > 2) throw GnError(GN_ERR_ARG, "unknown integrator");
+  if (u1_) throw GnError(GN_ERR_ARG, "the MD helpers are built for the Z2 model only");
+  const size_t V = size_t(V_);
+  memset(res, 0, sizeof *res);
+  struct ExactScope {
+    bool &flag, saved;
+    ExactScope(bool &f, bool on) : flag(f), saved(f) { flag = flag || on; }
+    ~ExactScope() { flag = saved; }
+  } exact_scope(exact, hp.precision == GN_PREC_FP64_EXACT);
+  const double *phis[2] = {phi_, phi_ + V};
+  double *Xs[2] = {X_, X_ + V};
+  SolveInfo info[2];
+  double iters = 0.0;
+  long long calls = 0, inner = 0, rel = 0;
+  int all_ok = 1;
+  const std::vector<Op> ops = evolve_schedule(hp.integrator, hp.eps, hp.steps);
+  for (size_t k = 0; k < ops.size(); k++) {
+    const Op &o = ops[k];
+    if (o.op == OP_F_MED || o.op == OP_F_HIGH) {
+      const double tol = o.op == OP_F_MED ? hp.tol_medium : hp.tol_high;
+      const int st = solve(sm_, phis, Xs, 2, 1, tol, 0, hp.relative, 0, hp.precision, info);
+      count_flavours(info, 2, iters, calls, inner, rel);
+      if (st != GN_OK) {
+        all_ok = 0;
+        check(cudaMemsetAsync(F_, 0, V * sizeof(double), stream_), "zero force");
+        continue;
+      }
+      dirac(sm_, X_, Y_, 2, GN_OP_MT);
+      if (k + 1 < ops.size() && ops[k + 1].op == OP_P) {
+        force(X_, Y_, sigma(), hp.beta_s, F_, P_, ops[k + 1].c);
+        k++;
+      } else {
+        force(X_, Y_, sigma(), hp.beta_s, F_, nullptr, 0.0);
+      }
+    } else if (o.op == OP_P) {
+      momenta(P_, F_, o.c);
+    } else if (o.op == OP_Q) {
+      sigma_mass(sigma(), P_, o.c, sigma_alt(), sm_);
+      swap_sigma();
+      distance += o.c;
+      res->distance += o.c;
+    } else {  // OP_S_HIGH / OP_C_HIGH: both flavours, results not checked
+      const int st = solve(sm_, phis, Xs, 2, 1, hp.tol_high, o.op == OP_S_HIGH ? 1 : 0, hp.relative, 0,
+                           hp.precision, info);
+      count_flavours(info, 2, iters, calls, inner, rel);
+      if (st != GN_OK) all_ok = 0;
+    }
+  }
+  check(cudaStreamSynchronize(stream_), "evolve in time");
+  res->ok = all_ok;
+  res->accepted = 1;
+  res->cg_iterations = iters;
+  res->cg_calls = calls;
+  res->inner_iterations = inner;
+  res->reliable_updates = rel;
+  return all_ok ? GN_OK : GN_NOT_CONVERGED;
+}
+
 // ------------------------------------------------------------------ condensate
 int Engine::condensate(const double *sm, double tol, double *target, double *D, double (*uniform)(void),
                        double out[11], double *iterations, long long *calls, int precision) {

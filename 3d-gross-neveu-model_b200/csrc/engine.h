@@ -91,6 +91,9 @@ class Engine {
   // One trajectory on the resident state; see gn_trajectory in gn_b200.h.
   int trajectory(const gn_hmc_params &hp, double (*gauss)(void), double (*uniform)(void), const double *pre_P,
                  const double *pre_chi, gn_traj_result *res);
+  // The reference's EvolveSigmaInTime* helpers on the resident sigma, P, phi
+  // and X (evolve_schedule); see gn_evolve_sigma_in_time in gn_b200.h.
+  int evolve_in_time(const gn_hmc_params &hp, gn_traj_result *res);
 
   // Full condensate measurement (condensate.c:114-244) on device pointers.
   int condensate(const double *sm, double tol, double *target, double *D, double (*uniform)(void), double out[11],
@@ -173,6 +176,11 @@ class Engine {
   float *mx_work_ = nullptr;   // mixed precision: kMaxRhs * 5 vectors * 2 planes * V
   float *sm32_ = nullptr;
   float *pm32_ = nullptr;  // the U(1) model: FP32 copy of the pi mass
+  // the second system of a two-team mixed solve (cg_mixed_duo_kernel): its
+  // arrival counter and its FP32 copy of sm (each team writes its own)
+  PhaseBar *bar2_ = nullptr;
+  float *sm32b_ = nullptr;
+  bool mixed_duo_ = true;
   double *partials_ = nullptr;
   double *h_partials_ = nullptr;
   PhaseBar *bar_ = nullptr;

@@ -183,7 +183,8 @@ Ensemble::Ensemble(int n, const int *L, const double *beta_s, const unsigned lon
   check(cudaMalloc(&d_order_, n * sizeof(int)), "cudaMalloc order");
   check(cudaMalloc(&d_queue_, kMaxNodes * kMaxTiers * sizeof(int)), "cudaMalloc queue");
   check(cudaMalloc(&d_bars_, size_t(kMaxNodes) * kMaxTiers * capacity_ * sizeof(PhaseBar)), "cudaMalloc bars");
-  check(cudaMalloc(&d_partials_, size_t(kMaxTiers) * capacity_ * 2 * (kSyncQ + 1) * sizeof(double)),
+  // two regions: the teams' partial sums, and those of the second flavour of two-team solves
+  check(cudaMalloc(&d_partials_, size_t(2) * kMaxTiers * capacity_ * 2 * (kSyncQ + 1) * sizeof(double)),
         "cudaMalloc partials");
   check(cudaMalloc(&d_cg_state_, size_t(capacity_) * kMaxRhs * sizeof(CgState)), "cudaMalloc cg state");
   check(cudaMalloc(&d_err_, sizeof(int)), "cudaMalloc err");
@@ -346,6 +347,8 @@ void Ensemble::launch_node(const Plan &pl, int k, double tol) {
   a.queue = d_queue_ + kMaxTiers * k;
   a.bars = d_bars_ + size_t(k) * kMaxTiers * capacity_;
   a.partials = d_partials_;
+  a.partials2 = d_partials_ + size_t(kMaxTiers) * capacity_ * 2 * (kSyncQ + 1);
+  a.duo = ens_duo_enabled();
   a.cg_state = d_cg_state_;
   a.err = d_err_;
   a.seed = seed_;

@@ -15,6 +15,7 @@
 // number as the counter, so a chain's results do not depend on the chains
 // beside it or on which team ran it (for a fixed team size).
 #pragma once
+#include <cstdlib>
 #include "../../include/gn_b200.h"
 #include "mixed_kernel.cuh"
 #include "ops_kernels.cuh"
@@ -99,6 +100,8 @@ struct EnsLaunch {
   int *queue;         // [kMaxTiers] next task of each tier; zero before the launch
   PhaseBar *bars;     // [kMaxTiers][gridDim.x] team barrier counters; zero before the launch
   double *partials;   // [kMaxTiers][gridDim.x][2][kSyncQ + 1]
+  double *partials2;  // the same again, for the second flavour of a two-team solve
+  int duo;            // solve the two flavours as two teams of half blocks
   CgState *cg_state;  // [gridDim.x][kMaxRhs] solver status scratch
   int *err;
   unsigned long long seed;
@@ -135,6 +138,78 @@ template <int W>
 __device__ __noinline__ void ens_solve64(const CgArgs<double> &a, Team &t, SyncShared &sh, CgShared &cs) {
   cg_solve<double, 1, 2, W>(a, t, sh, cs);
 }
+template <int W>
+__device__ __noinline__ void ens_solve_half(const MixedArgs &a, Team &t, SyncShared &sh, MixedShared &ms) {
+  mixed_solve<1, 1, W>(a, t, sh, ms);
+}
+
+// The second flavour's team state of a two-team solve: its own arrival
+// counter and partial sums (the first flavour uses the team's), and its phase
+// count, kept from one solve of the launch to the next.
+struct DuoSync {
+  PhaseBar *bar;
+  double *partials;
+  unsigned long long nph;
+};
+
+// Shared memory of the two half teams.
+struct DuoShared {
+  SyncShared sh[2];
+  MixedShared ms[2];
+  unsigned long long nph[2];
+};
+
+// Both flavours of a mixed-precision solve as two teams of half blocks, as in
+// cg_mixed_duo_kernel: flavour h runs on the threads [h B/2, (h+1) B/2) of
+// every block of the team, with named barrier 1 + h, so one flavour's phase
+// ends overlap the other's sweeps; on a team of several blocks flavour 1
+// starts half an iteration behind.  a holds both systems (nrhs = 2, sm32
+// already formed by the whole team).  On return every thread of the team holds
+// both phase counts.  Measured on the 256-chain benchmark mix: 372 chain
+// trajectories/s against 336 in lock step (without the offset).
+__device__ __forceinline__ void ens_duo_solve(const MixedArgs &a, int w, Team &t, DuoSync &d, DuoShared &ds) {
+  const uint32_t half = blockDim.x / 2;
+  const int h = threadIdx.x >= half ? 1 : 0;
+  Team ht = t;
+  ht.tid = uint32_t(t.brank) * half + (threadIdx.x - h * half);
+  ht.nthreads = uint32_t(t.nblocks) * half;
+  set_block_share(ht, threadIdx.x - h * half, half, 1 + h);
+  if (h) {
+    ht.bar = d.bar;
+    ht.partials = d.partials;
+    ht.nph = d.nph;
+  }
+  MixedArgs ah = a;
+  ah.nrhs = 1;
+  ah.b[0] = a.b[h];
+  ah.x[0] = a.x[h];
+  ah.t64[0] = a.t64[h];
+  ah.rh[0] = a.rh[h];
+  ah.ph[0] = a.ph[h];
+  ah.uh[0] = a.uh[h];
+  ah.ah[0] = a.ah[h];
+  ah.xh[0] = a.xh[h];
+  ah.state = a.state + h;
+  ah.lead = nullptr;
+  if (h == 1 && t.nblocks > 1) {
+    // start half an iteration behind flavour 0: after its first phase end on
+    // the team's counter (a bounded wait; only a matter of timing)
+    if (ht.btid == 0) {
+      const unsigned long long target = (t.nph + 1ull) * t.nblocks;
+      unsigned spins = 0;
+      while (ld_relaxed64(&t.bar->arrived) < target && ++spins < (1u << 20)) {
+      }
+    }
+    team_sync(ht);
+  }
+  if (w == 4) ens_solve_half<4>(ah, ht, ds.sh[h], ds.ms[h]);
+  else if (w == 2) ens_solve_half<2>(ah, ht, ds.sh[h], ds.ms[h]);
+  else ens_solve_half<1>(ah, ht, ds.sh[h], ds.ms[h]);
+  if (ht.btid == 0) ds.nph[h] = ht.nph;
+  __syncthreads();  // the whole block again
+  t.nph = ds.nph[0];
+  d.nph = ds.nph[1];
+}
 
 // Box-Muller on two uniforms: two N(0, 1) values.
 __device__ __forceinline__ void box_muller(uint64_t a, uint64_t b, double &z0, double &z1) {
@@ -150,7 +225,7 @@ __device__ __forceinline__ double eps_scale(const EnsState *st) { return st->eps
 
 // The chain's ops [op_begin, op_end) by team t.  Returns false on a barrier timeout.
 static __device__ __noinline__ bool ens_run_chain(const EnsLaunch &L, int c, Team &t, SyncShared &sh, MixedShared &ms,
-                                                  CgShared &cs) {
+                                                  CgShared &cs, DuoSync &duo, DuoShared &ds) {
   const EnsChain &ch = L.chains[c];
   EnsState *st = ch.state;
   const int op_begin = L.op_begin >= 0 ? L.op_begin : ch.op_begin;
@@ -241,6 +316,7 @@ static __device__ __noinline__ bool ens_run_chain(const EnsLaunch &L, int c, Tea
         a.variant = 1;
         a.rel = 1;
         a.scheme = mixed_scheme(g.V, nrhs, 1);
+        a.sm32_ready = 0;
         a.tol = L.tol;
         a.max_iter = (long long)V + 1;
         a.delta = L.delta;
@@ -250,21 +326,30 @@ static __device__ __noinline__ bool ens_run_chain(const EnsLaunch &L, int c, Tea
         a.err = t.err;
         a.abort_flag = nullptr;
         a.state = L.cg_state + size_t(blockIdx.x) * kMaxRhs;
-        if (ch.w == 4) ens_solve<4>(a, t, sh, ms);
-        else if (ch.w == 2) ens_solve<2>(a, t, sh, ms);
-        else ens_solve<1>(a, t, sh, ms);
+        if (L.duo && nrhs == 2) {
+          // sm32 by the whole team, then one flavour per half of every block
+          for (uint32_t i = t.tid; i < V; i += t.nthreads) ch.sm32[i] = float(ch.sm[i]);
+          ok = end_phase<0>(acc, sh, t);
+          a.sm32_ready = 1;
+          if (ok) ens_duo_solve(a, ch.w, t, duo, ds);
+        } else {
+          if (ch.w == 4) ens_solve<4>(a, t, sh, ms);
+          else if (ch.w == 2) ens_solve<2>(a, t, sh, ms);
+          else ens_solve<1>(a, t, sh, ms);
+        }
         status = ms.status;
         iters = ms.iters;
       }
       if (leader) {
+        const bool two = ch.precision != GN_PREC_FP64 && L.duo && nrhs == 2;
         for (int k = 0; k < nrhs; k++) {
-          const int s = status[k];
+          const int s = two ? ds.ms[k].status[0] : status[k];
           if (s != kCgConverged && s != kCgConvergedStart) st->failed = 1;
-          st->iters += (s == kCgConverged) ? iters[k] : 0;
-          if (ch.precision != GN_PREC_FP64) st->reliable += ms.nru[k];
+          st->iters += (s == kCgConverged) ? (two ? ds.ms[k].iters[0] : iters[k]) : 0;
+          if (ch.precision != GN_PREC_FP64) st->reliable += two ? ds.ms[k].nru[0] : ms.nru[k];
         }
       }
-      ok = ld_relaxed_int(t.err) == 0;
+      ok = ok && ld_relaxed_int(t.err) == 0;
     } else if (op.code == E_FORCE) {
       if (ch.w >= 2) team_dirac2<2, 1>(g, t, ch.sm, ch.X, ch.Y);
       else team_dirac2<1, 1>(g, t, ch.sm, ch.X, ch.Y);
@@ -397,6 +482,13 @@ static __device__ __noinline__ bool ens_run_chain(const EnsLaunch &L, int c, Tea
   return true;
 }
 
+// Whether the batched kernel solves the two flavours as two teams of half
+// blocks (default), or in lock step on the whole team (GN_ENS_DUO=0).
+inline int ens_duo_enabled() {
+  const char *e = getenv("GN_ENS_DUO");
+  return (e != nullptr && e[0] == '0') ? 0 : 1;
+}
+
 // Defined in one translation unit (ensemble.cu, which sets
 // GN_DEFINE_ENSEMBLE_KERNEL); the others launch it through this declaration.
 __global__ void __launch_bounds__(kEnsThreads, 1) ens_node_kernel(EnsLaunch L);
@@ -406,6 +498,7 @@ __global__ void __launch_bounds__(kEnsThreads, 1) ens_node_kernel(EnsLaunch L) {
   __shared__ SyncShared sh;
   __shared__ MixedShared ms;
   __shared__ CgShared cs;
+  __shared__ DuoShared ds;
   __shared__ int s_task;
   int tb = 0;  // first order index of the tier
   for (int tier = 0; tier < L.ntier; tier++) {
@@ -423,6 +516,10 @@ __global__ void __launch_bounds__(kEnsThreads, 1) ens_node_kernel(EnsLaunch L) {
         gt.partials = L.partials + (size_t(tier) * gridDim.x + size_t(group) * gs) * 2 * (kSyncQ + 1);
         gt.err = L.err;
         gt.nph = 0;
+        whole_block(gt);
+        // the second flavour's counter: past the tier's gridDim.x / gs team counters
+        DuoSync duo{L.bars + size_t(tier) * gridDim.x + gridDim.x / gs + group,
+                    L.partials2 + (size_t(tier) * gridDim.x + size_t(group) * gs) * 2 * (kSyncQ + 1), 0ull};
         for (;;) {
           int task = 0;
           if (grank == 0 && threadIdx.x == 0) task = tb + atomicAdd(&L.queue[tier], 1);
@@ -432,7 +529,7 @@ __global__ void __launch_bounds__(kEnsThreads, 1) ens_node_kernel(EnsLaunch L) {
           if (!end_phase<0>(acc, sh, gt, task)) return;  // the team leader's task, to every block
           task = sh.flag;
           if (task >= te) break;
-          if (!ens_run_chain(L, L.order[task], gt, sh, ms, cs)) return;
+          if (!ens_run_chain(L, L.order[task], gt, sh, ms, cs, duo, ds)) return;
         }
       }
     } else {
@@ -445,13 +542,15 @@ __global__ void __launch_bounds__(kEnsThreads, 1) ens_node_kernel(EnsLaunch L) {
       bt.partials = nullptr;
       bt.err = L.err;
       bt.nph = 0;
+      whole_block(bt);
+      DuoSync duo{nullptr, nullptr, 0ull};  // one-block teams need no counters
       for (;;) {
         if (threadIdx.x == 0) s_task = tb + atomicAdd(&L.queue[tier], 1);
         __syncthreads();
         const int task = s_task;
         __syncthreads();
         if (task >= te) break;
-        if (!ens_run_chain(L, L.order[task], bt, sh, ms, cs)) return;
+        if (!ens_run_chain(L, L.order[task], bt, sh, ms, cs, duo, ds)) return;
       }
     }
     tb = te;

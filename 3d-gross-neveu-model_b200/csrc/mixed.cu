@@ -1,6 +1,7 @@
 // mixed.cu -- host side of the mixed-precision solver (FP32 inner iterations,
 // FP64 reliable updates).  Built with FMA contraction on: nothing in this
 // translation unit reproduces a reference result bit for bit.
+#include <cstdlib>
 #include <cstring>
 
 #include "engine.h"
@@ -18,6 +19,19 @@ void Engine::mixed_init() {
   mx_work_ = (float *)alloc(size_t(kMaxRhs) * kMixedVecs * 2 * V * sizeof(float));
   sm32_ = (float *)alloc(V * sizeof(float));
   pm32_ = (float *)alloc(V * sizeof(float));
+  sm32b_ = (float *)alloc(V * sizeof(float));
+  bar2_ = (PhaseBar *)alloc(sizeof(PhaseBar));
+  const char *duo = getenv("GN_MIXED_DUO");
+  mixed_duo_ = !(duo != nullptr && duo[0] == '0');
+}
+
+// Two real systems as two teams of half blocks (cg_mixed_duo_kernel).
+template <int W>
+static const void *mixed_duo_kernel() {
+  return (const void *)cg_mixed_duo_kernel<1, kWideThreads, W>;
+}
+static const void *mixed_duo_kernel_ptr(int w) {
+  return w == 4 ? mixed_duo_kernel<4>() : w == 2 ? mixed_duo_kernel<2>() : mixed_duo_kernel<1>();
 }
 
 template <int W>
@@ -94,6 +108,42 @@ int Engine::solve_mixed(const double *sm, const double *const *b, double *const 
   }
   const int w = fp64_width(L_, ptrs, 2 + 2 * nrhs) == 2 ? row_width(L_, 4) : 1;
   const int nb = cg_blocks(ncomp, nrhs, true, w);
+  if (mixed_duo_ && pm == nullptr && ncomp == 1 && nrhs == 2) {
+    // the two systems as two teams of half blocks: the same units per thread,
+    // each team with its own counter, partials (after the first team's
+    // 2 (kSyncQ + 1) nb slots), sm32 copy and state slot
+    const void *fn = mixed_duo_kernel_ptr(w);
+    const int cap = coop_capacity(fn, kWideThreads);
+    if (cap < 1) throw GnError(GN_ERR_CUDA, "CG kernel cannot be resident as a cooperative grid");
+    const int nbd = nb < cap ? nb : cap;
+    MixedArgs a1 = a;
+    a.nrhs = a1.nrhs = 1;
+    a1.b[0] = a.b[1];
+    a1.x[0] = a.x[1];
+    a1.t64[0] = a.t64[1];
+    a1.rh[0] = a.rh[1];
+    a1.ph[0] = a.ph[1];
+    a1.uh[0] = a.uh[1];
+    a1.ah[0] = a.ah[1];
+    a1.xh[0] = a.xh[1];
+    for (int k = 1; k < kMaxRhs; k++) {
+      a.b[k] = a1.b[k] = nullptr;
+      a.x[k] = a1.x[k] = nullptr;
+    }
+    a1.sm32 = sm32b_;
+    a1.bar = bar2_;
+    a1.partials = partials_ + size_t(2) * (kSyncQ + 1) * nbd;
+    a1.state = state_ + 1;
+    a.lead = nullptr;
+    a1.lead = &bar_->arrived;  // team 1 starts after team 0's first phase
+    a1.lead_count = (unsigned long long)nbd;
+    check(cudaMemsetAsync(bar2_, 0, sizeof(PhaseBar), stream_), "memset");
+    void *args[] = {(void *)&a, (void *)&a1};
+    check(cudaLaunchCooperativeKernel(fn, dim3(nbd), dim3(kWideThreads), args, 0, stream_),
+          "cg_mixed_duo_kernel launch");
+    launches++;
+    return finish_solve(nrhs, info);
+  }
   const void *fn;
   if (pm != nullptr) {
     const int nr = rhs_slots(nrhs);

@@ -52,6 +52,11 @@ struct SyncShared {
 // A team: the blocks that sweep one lattice together and synchronise among
 // themselves -- the whole grid of a single-lattice solve, or a group of
 // blocks of the batched kernel.  A one-block team needs no global memory.
+//
+// A block normally gives all its threads to one team.  It can also hold two
+// teams side by side (cg_mixed_duo_kernel): each then owns a contiguous,
+// warp-aligned share of the block's threads and synchronises that share with
+// a named barrier of its own, so the two teams never wait for each other.
 struct Team {
   uint32_t tid;       // thread index within the team
   uint32_t nthreads;  // threads in the team
@@ -61,7 +66,25 @@ struct Team {
   double *partials;   // [2][kSyncQ + 1][nblocks] partial sums (nblocks > 1)
   int *err;           // set to 1 by a wait that timed out
   unsigned long long nph;  // phases ended so far (the same count in every block of the team)
+  uint32_t btid;      // thread index within this block's share of the team
+  uint32_t bsize;     // threads of this block in the team (a multiple of 32)
+  int bid;            // named barrier of that share: 0 = the whole block (__syncthreads)
 };
+
+// The team's threads in this block: the whole block, or a share of it given
+// by (btid, bsize, bid).
+__device__ __forceinline__ void set_block_share(Team &t, uint32_t btid, uint32_t bsize, int bid) {
+  t.btid = btid;
+  t.bsize = bsize;
+  t.bid = bid;
+}
+__device__ __forceinline__ void whole_block(Team &t) { set_block_share(t, threadIdx.x, blockDim.x, 0); }
+
+// Barrier of the team's threads in this block.
+__device__ __forceinline__ void team_sync(const Team &t) {
+  if (t.bid == 0) __syncthreads();
+  else asm volatile("bar.sync %0, %1;" ::"r"(t.bid), "r"(t.bsize) : "memory");
+}
 
 // The whole grid as one team.
 __device__ __forceinline__ Team grid_team(PhaseBar *bar, double *partials, int *err) {
@@ -74,6 +97,7 @@ __device__ __forceinline__ Team grid_team(PhaseBar *bar, double *partials, int *
   t.partials = partials;
   t.err = err;
   t.nph = 0;
+  whole_block(t);
   return t;
 }
 
@@ -86,13 +110,13 @@ __device__ __forceinline__ Team grid_team(PhaseBar *bar, double *partials, int *
 template <int NQ>
 __device__ __forceinline__ bool phase_arrive_wait(double (&acc)[kSyncQ], SyncShared &sh, const Team &t,
                                                   int flag = 0) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int lane = t.btid & 31, w = t.btid >> 5, nw = t.bsize >> 5;
 #pragma unroll
   for (int q = 0; q < NQ; q++) {
     const double v = warp_sum(acc[q]);
     if (lane == 0) sh.red[q * 32 + w] = v;
   }
-  __syncthreads();
+  team_sync(t);
   if (w == 0) {
     double tot[NQ > 0 ? NQ : 1];
 #pragma unroll
@@ -127,7 +151,7 @@ __device__ __forceinline__ bool phase_arrive_wait(double (&acc)[kSyncQ], SyncSha
       }
     }
   }
-  __syncthreads();
+  team_sync(t);
   return sh.ok != 0;
 }
 
@@ -138,17 +162,17 @@ template <int NQ>
 __device__ __forceinline__ void phase_totals(SyncShared &sh, Team &t) {
   if (t.nblocks > 1) {
     const double *slot = t.partials + (t.nph & 1ull) * size_t(kSyncQ + 1) * t.nblocks;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int lane = t.btid & 31, w = t.btid >> 5;
     if (w < NQ) {
       const double *p = slot + size_t(w) * t.nblocks;
       double s = 0.0;
       for (int b = lane; b < t.nblocks; b += 32) s += p[b];
       s = warp_sum(s);
       if (lane == 0) sh.val[w] = s;
-    } else if (threadIdx.x == blockDim.x - 1) {
+    } else if (t.btid == t.bsize - 1) {
       sh.flag = reinterpret_cast<const int *>(slot + size_t(NQ) * t.nblocks)[0];
     }
-    __syncthreads();
+    team_sync(t);
   }
   t.nph++;
 }
@@ -162,15 +186,14 @@ __device__ __forceinline__ bool end_phase(double (&acc)[kSyncQ], SyncShared &sh,
   return ok;
 }
 
-
 // A team barrier without sums: on return the team's writes before the call
 // are visible to this block.  About 1.5 us on B200 for a grid of 64 - 148
 // blocks of 1024 threads, against 3.2 - 3.7 us for an end_phase with sums
 // (the block and team reductions and the read of the partials are what it
 // saves); 0.28 us for a one-block team.  Counts as one phase of the team.
 __device__ __forceinline__ bool team_barrier(SyncShared &sh, Team &t) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
+  team_sync(t);
+  if (t.btid == 0) {
     int ok = 1;
     if (t.nblocks > 1) {
       red_release_add64(&t.bar->arrived, 1ull);
@@ -188,7 +211,7 @@ __device__ __forceinline__ bool team_barrier(SyncShared &sh, Team &t) {
     sh.ok = ok;
   }
   t.nph++;
-  __syncthreads();
+  team_sync(t);
   return sh.ok != 0;
 }
 

@@ -25,6 +25,7 @@ __global__ void selftest_timeout_kernel(PhaseBar *bar, int *err) {
   t.partials = nullptr;
   t.err = err;
   t.nph = 0;
+  whole_block(t);
   team_barrier(sh, t);
 }
 

@@ -161,6 +161,7 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
         "gn_trajectory_device": ([v, C.POINTER(HmcParams), C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.POINTER(TrajResult)], C.c_int),
         "gn_md_evolve": ([v, C.POINTER(HmcParams), C.POINTER(TrajResult)], C.c_int),
+        "gn_evolve_sigma_in_time": ([v, C.POINTER(HmcParams), C.POINTER(TrajResult)], C.c_int),
         "gn_launch_count": ([v], C.c_longlong),
         "gn_flush_l2": ([v], C.c_int),
         "gn_set_parity_mode": ([v, C.c_int], C.c_int),
@@ -469,6 +470,16 @@ class Lattice:
         hp = HmcParams(beta_s, eps, steps, integrator, tol_medium, tol_high, int(relative), precision)
         res = TrajResult()
         self._check(self.lib.gn_md_evolve(self.ctx, C.byref(hp), C.byref(res)), allow=(GN_OK, GN_NOT_CONVERGED))
+        return res.as_dict()
+
+    def evolve_in_time(self, beta_s, eps, steps, integrator=GN_LFMN2VF, tol_medium=1e-3, tol_high=1e-9,
+                       relative=False, precision=GN_PREC_FP64):
+        """The reference's EvolveSigmaInTime* helper of `integrator` on the
+        resident sigma, P, phi and X (gn_evolve_sigma_in_time)."""
+        hp = HmcParams(beta_s, eps, steps, integrator, tol_medium, tol_high, int(relative), precision)
+        res = TrajResult()
+        self._check(self.lib.gn_evolve_sigma_in_time(self.ctx, C.byref(hp), C.byref(res)),
+                    allow=(GN_OK, GN_NOT_CONVERGED))
         return res.as_dict()
 
     def set_parity_mode(self, on=True):

@@ -75,6 +75,7 @@ def parse():
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-l128", action="store_true", help="skip the L = 128 mixed-precision case")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving sweep")
     ap.add_argument("--detail", default=None, help="write every side measurement to this JSON file")
     ap.add_argument("--case", choices=["cg64", "dirac128", "dirac256", "traj64", "batched", "serve", "l128", "u1",
                                        "ens", "kernels"],
@@ -446,7 +447,8 @@ def run_ours(a, world, rank, local):
         if l128_job is not None:
             detail["l128"] = l128_case(G, dev, oracle=l128_job)
         detail["u1"] = u1_case(G, dev)
-        detail["serving"] = serve_sweep(G)
+        if not a.no_serve:
+            detail["serving"] = serve_sweep(G)
     cpu = None
     if cpu_job is not None:
         cpu = cpu_line_fields(cpu_job.result(), a)
@@ -957,9 +959,10 @@ def ens_case(G, dev, nchains=48, ntraj=2):
             "cg_iterations": sum(s["cg_iterations"] for s in st)}
 
 
-def kernels_case(G, dev, L=160):
-    """One launch of each small kernel of the path at L = 160 (V = 4,096,000;
-    an FP64 plane is 33 MB, so every kernel's inputs exceed the L2): sigma
+def kernels_case(G, dev, L=128):
+    """One launch of each small kernel of the path at L = 128 (V = 2,097,152;
+    an FP64 plane is 16.8 MB; a profiler run with its cache flush between
+    passes sees every kernel start cold): sigma
     mass, M, M^T, the sigma force's gather (its CG exits at the start: X is
     given with a tolerance of 1e300), the energy, the condensate's source and
     dot kernels (solves exit at once the same way), and the U(1) model's

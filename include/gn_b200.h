@@ -317,16 +317,32 @@ GN_API int gn_trajectory(gn_context *ctx, const gn_hmc_params *params, double (*
                   gn_traj_result *res);
 
 /* The molecular dynamics of one trajectory without draws and without the
- * Metropolis test, as the reference's EvolveSigmaInTimeLF2 /
- * ...MinimumNormLF2 / ...MinimumNormSigmaVelocityFirst helpers
- * (moleculardynamics.c:1460-1625, used by its DEBUG_LF2_SIGMA reversibility
- * check): from the resident sigma, P (GN_F_P) and phi (GN_F_PHI; in the U(1)
- * model GN_F_PHI_C), with params->integrator's schedule as gn_trajectory runs
- * it.  phi is not formed from chi.  res->H0, H1, dH are the energies before
- * and after; sigma and P are left evolved (res->accepted = 1), or restored
- * when a solve fails (GN_NOT_CONVERGED).  Flipping P and evolving again
- * retraces the trajectory. */
+ * Metropolis test (a reversibility check in the manner of the reference's
+ * DEBUG_LF2_SIGMA): from the resident sigma, P (GN_F_P) and phi (GN_F_PHI;
+ * in the U(1) model GN_F_PHI_C), exactly the initial solve, energies and MD
+ * schedule gn_trajectory runs for params->integrator.  phi is not formed from
+ * chi.  res->H0, H1, dH are the energies before and after; sigma and P are
+ * left evolved (res->accepted = 1), or restored when a solve fails
+ * (GN_NOT_CONVERGED).  Flipping P and evolving again retraces the trajectory.
+ * For the reference's own helpers, with their tolerance pattern, see
+ * gn_evolve_sigma_in_time. */
 GN_API int gn_md_evolve(gn_context *ctx, const gn_hmc_params *params, gn_traj_result *res);
+
+/* The reference's MD helpers, replaced one for one:
+ * EvolveSigmaInTimeLF2 (moleculardynamics.c:1460, params->integrator GN_LF2),
+ * EvolveSigmaInTimeMinimumNormLF2 (:1489, GN_LFMN2) and
+ * EvolveSigmaInTimeMinimumNormSigmaVelocityFirst (:1551, GN_LFMN2VF), on the
+ * resident sigma, P (GN_F_P), phi (GN_F_PHI) and X (GN_F_X, the start of
+ * every early-exit solve); Z2 model only (GN_ERR_ARG in a U(1) context).
+ * Their step sequences and tolerances are the helpers' own: the LF2 and
+ * LFMN2 helpers take their first force at tol_high, the velocity-first one
+ * runs an X0-imposed solve before and an early-exit solve after the
+ * integrator's MD.  No draws, no energies, no Metropolis test, sigma never
+ * restored; as in the reference a force whose solve fails is left at zero and
+ * the MD goes on.  Leaves sigma, sigmamass, P, F, X and Y (= M^T X) evolved;
+ * res->cg_iterations / cg_calls add up the counted solves, res->distance the
+ * sigma steps, res->ok = 0 (and GN_NOT_CONVERGED) if any solve failed. */
+GN_API int gn_evolve_sigma_in_time(gn_context *ctx, const gn_hmc_params *params, gn_traj_result *res);
 
 /* ---- device-resident entry points ------------------------------------- */
 

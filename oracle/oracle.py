@@ -242,6 +242,7 @@ class Ref:
         lib.gnref_evolve_sigma.argtypes = [C.c_double]
         lib.gnref_evolve_momenta.argtypes = [C.c_double]
         lib.gnref_trajectory.argtypes = [C.c_char_p, _ip]
+        lib.gnref_evolve_in_time.argtypes = [C.c_int, C.c_double, C.c_int]
         lib.gnref_info.argtypes = [_ip, _ip, _dp]
         lib.gnref_condensate.argtypes = [C.c_double, _dp]
         lib.gnref_seed.argtypes = [C.c_uint]
@@ -359,6 +360,11 @@ class Ref:
                 last = fh.read().strip().splitlines()[-1]
             dH = float(last.split("\t")[11])
         return bool(ok), bool(acc.value), dH
+
+    def evolve_in_time(self, which, eps, steps):
+        """EvolveSigmaInTime* (which: 0 LFMN2VF, 1 LF2, 2 LFMN2) on the current
+        sigma, momenta and the kit's phi / inverted_phi."""
+        self.lib.gnref_evolve_in_time(int(which), float(eps), int(steps))
 
     def condensate(self, tol=1e-9):
         out = np.zeros(11)

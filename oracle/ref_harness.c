@@ -291,6 +291,18 @@ int gnref_trajectory(const char *accfile, int *accepted)
     *accepted = g_info.hybrid_accepted_sigma - before;
     return ok ? 1 : 0;
 }
+/* The MD helpers of the reference's reversibility check, on the current sigma,
+ * momenta and the kit's phi / inverted_phi: which = 0 EvolveSigmaInTimeMinimumNormSigmaVelocityFirst
+ * (moleculardynamics.c:1551), 1 EvolveSigmaInTimeLF2 (:1460), 2 EvolveSigmaInTimeMinimumNormLF2 (:1489). */
+void gnref_evolve_in_time(int which, double eps, int step)
+{
+    if (which == 0)
+        EvolveSigmaInTimeMinimumNormSigmaVelocityFirst(&g_lat, &g_info, &g_force, &g_mom, &g_fcor, &g_kit, eps, step);
+    else if (which == 1)
+        EvolveSigmaInTimeLF2(&g_lat, &g_info, &g_force, &g_mom, &g_fcor, &g_kit, eps, step);
+    else
+        EvolveSigmaInTimeMinimumNormLF2(&g_lat, &g_info, &g_force, &g_mom, &g_fcor, &g_kit, eps, step);
+}
 void gnref_info(int *accepted, int *done, double *acceptance)
 {
     *accepted = g_info.hybrid_accepted_sigma;

@@ -25,6 +25,13 @@ ROOT = Path(__file__).resolve().parent.parent
 sys.path.insert(0, str(ROOT))
 
 
+def evolve_inputs(L):
+    """sigma, P and chi of the MD-helper check (seeded)."""
+    rng = np.random.default_rng(11)
+    V = L ** 3
+    return rng.normal(0.0, np.sqrt(2.0 / (4 * 0.85)), V), rng.normal(size=V), rng.normal(size=(2, V))
+
+
 def main():
     hmc = dict(np.load(sys.argv[1]))
     cond = dict(np.load(sys.argv[2]))
@@ -76,6 +83,22 @@ def main():
     out["launches"]["dirac"] = launches() - n0
     out["psi"] = psi.tolist()
     out["sm"] = ref.sigmamass().tolist()
+    # the MD helper of the reference's reversibility check (EvolveSigmaInTime*)
+    # through its call site, on the inputs of evolve_inputs()
+    sig0, P0, chi = evolve_inputs(L)
+    ref.init(1231, float(hmc["beta_s"]), 0.1, 4)
+    ref.set_sigma(sig0)
+    ref.set_momenta(P0)
+    for f in range(2):
+        ref.kit_set("phi", f, ref.dirac(chi[f].astype(complex), 0))
+        ref.kit_set("X", f, np.zeros(L ** 3, complex))
+    ref.lib.gnref_reset_counters()
+    n0 = launches()
+    ref.evolve_in_time(int(hmc["integrator"]), 0.1, 4)
+    out["launches"]["evolve"] = launches() - n0
+    out["evolve_sigma"] = ref.sigma().tolist()
+    out["evolve_P"] = ref.momenta().tolist()
+    out["evolve_counters"] = list(ref.counters())
     print(json.dumps(out))
     _ = lib
 

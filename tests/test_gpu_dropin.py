@@ -22,6 +22,26 @@ ROOT = Path(__file__).resolve().parent.parent
 GOLD = ROOT / "tests" / "golden"
 
 
+def evolve_reference(L, beta_s, integrator):
+    """The reference's own EvolveSigmaInTime* (no drop-in in this process) on the
+    driver's inputs: (sigma, P, counters)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from dropin_driver import evolve_inputs
+
+    from oracle.oracle import Ref
+    ref = Ref(L, build=False)
+    sig0, P0, chi = evolve_inputs(L)
+    ref.init(1231, beta_s, 0.1, 4)
+    ref.set_sigma(sig0)
+    ref.set_momenta(P0)
+    for f in range(2):
+        ref.kit_set("phi", f, ref.dirac(chi[f].astype(complex), 0))
+        ref.kit_set("X", f, np.zeros(L ** 3, complex))
+    ref.lib.gnref_reset_counters()
+    ref.evolve_in_time(integrator, 0.1, 4)
+    return ref.sigma(), ref.momenta(), list(ref.counters())
+
+
 def test_dropin_under_reference_driver(port):
     from oracle import build_ref
     if not build_ref.lib_path(8, 0).exists():
@@ -40,11 +60,16 @@ def test_dropin_under_reference_driver(port):
         assert abs(out["condensate"][k] - c["out"][k]) <= 1e-11 * max(abs(c["out"][k]), 1e-3)
     assert tuple(out["condensate_counters"]) == tuple(c["counters"])
     # the replacement took effect: each phase launched the library's kernels
-    assert all(out["launches"][k] > 0 for k in ("trajectories", "condensate", "dirac")), out["launches"]
+    assert all(out["launches"][k] > 0 for k in ("trajectories", "condensate", "dirac", "evolve")), out["launches"]
     assert out["launches"]["trajectories"] >= 20 * 5  # 20 trajectories, each with solves, forces and steps
     # DiracFermion called by the reference's harness equals the reference's own M, bit for bit
     L = 8
     assert np.array_equal(np.array(out["M_psi"]), port.dirac(L, np.array(out["sm"]), np.array(out["psi"]), 0))
+    # EvolveSigmaInTimeMinimumNormSigmaVelocityFirst called by the reference's harness
+    s_ref, P_ref, cnt_ref = evolve_reference(L, float(g["beta_s"]), int(g["integrator"]))
+    assert out["evolve_counters"] == cnt_ref
+    assert np.max(np.abs(np.array(out["evolve_sigma"]) - s_ref)) < 1e-12 * np.max(np.abs(s_ref))
+    assert np.max(np.abs(np.array(out["evolve_P"]) - P_ref)) < 1e-11 * np.max(np.abs(P_ref))
 
 
 def test_dropin_exact_mode_is_bit_identical():
@@ -63,6 +88,9 @@ def test_dropin_exact_mode_is_bit_identical():
     assert [tuple(c) for c in out["counters"]] == [tuple(c) for c in g["counters"]]
     c = dict(np.load(GOLD / "golden_L8_cond.npz"))
     assert out["condensate"] == [float(v) for v in c["out"]]
+    s_ref, P_ref, cnt_ref = evolve_reference(8, float(g["beta_s"]), int(g["integrator"]))
+    assert out["evolve_counters"] == cnt_ref
+    assert out["evolve_sigma"] == s_ref.tolist() and out["evolve_P"] == P_ref.tolist()
 
 
 @pytest.mark.parametrize("L", [4, 8])
