@@ -89,8 +89,12 @@ __device__ __forceinline__ void sys_list_from(SysList &sl, const int *flag, int 
 // numbering, so a warp reads contiguous vectors of one system.
 template <typename F>
 __device__ __forceinline__ void for_units(uint32_t NI, const SysList &sl, const Team &t, F f) {
+  // the team's indices in registers: when the team is held in memory (a solver
+  // called with a reference to its caller's), the stores of f() could alias it
+  // and would make every step of the loop reload them
+  const uint32_t tid = t.tid, nthreads = t.nthreads;
   const uint32_t total = uint32_t(sl.n) * NI;
-  for (uint32_t u = t.tid; u < total; u += t.nthreads) {
+  for (uint32_t u = tid; u < total; u += nthreads) {
     uint32_t j = u;
     int ka = 0;
     while (j >= NI) {

@@ -129,7 +129,11 @@ __device__ __forceinline__ void team_dirac2(const Geom &g, const Team &t, const 
 }
 
 // The solvers of one chain, one function per item width (each gets its own
-// register allocation instead of sharing the caller's).
+// register allocation instead of sharing the caller's).  The argument structs
+// live in shared memory, written by one thread of the block: read through a
+// reference to the caller's stack, every access of the sweeps was a
+// local-memory load (ncu: more local than global load requests in this
+// kernel).
 template <int W>
 __device__ __noinline__ void ens_solve(const MixedArgs &a, Team &t, SyncShared &sh, MixedShared &ms) {
   mixed_solve<1, 2, W>(a, t, sh, ms);
@@ -152,22 +156,25 @@ struct DuoSync {
   unsigned long long nph;
 };
 
-// Shared memory of the two half teams.
+// Shared memory of a chain's solves: the argument structs and the two half
+// teams' state.
 struct DuoShared {
   SyncShared sh[2];
   MixedShared ms[2];
   unsigned long long nph[2];
+  MixedArgs args[2];  // the solve (args[0]), or one flavour per half team
+  CgArgs<double> args64;
 };
 
 // Both flavours of a mixed-precision solve as two teams of half blocks, as in
 // cg_mixed_duo_kernel: flavour h runs on the threads [h B/2, (h+1) B/2) of
 // every block of the team, with named barrier 1 + h, so one flavour's phase
 // ends overlap the other's sweeps; on a team of several blocks flavour 1
-// starts half an iteration behind.  a holds both systems (nrhs = 2, sm32
-// already formed by the whole team).  On return every thread of the team holds
-// both phase counts.  Measured on the 256-chain benchmark mix: 372 chain
-// trajectories/s against 336 in lock step (without the offset).
-__device__ __forceinline__ void ens_duo_solve(const MixedArgs &a, int w, Team &t, DuoSync &d, DuoShared &ds) {
+// starts half an iteration behind.  ds.args[h] holds flavour h's solve
+// (nrhs = 1, sm32 already formed by the whole team).  On return every thread
+// of the team holds both phase counts.  Measured on the 256-chain benchmark
+// mix: 372 chain trajectories/s against 336 in lock step (without the offset).
+__device__ __forceinline__ void ens_duo_solve(int w, Team &t, DuoSync &d, DuoShared &ds) {
   const uint32_t half = blockDim.x / 2;
   const int h = threadIdx.x >= half ? 1 : 0;
   Team ht = t;
@@ -179,18 +186,6 @@ __device__ __forceinline__ void ens_duo_solve(const MixedArgs &a, int w, Team &t
     ht.partials = d.partials;
     ht.nph = d.nph;
   }
-  MixedArgs ah = a;
-  ah.nrhs = 1;
-  ah.b[0] = a.b[h];
-  ah.x[0] = a.x[h];
-  ah.t64[0] = a.t64[h];
-  ah.rh[0] = a.rh[h];
-  ah.ph[0] = a.ph[h];
-  ah.uh[0] = a.uh[h];
-  ah.ah[0] = a.ah[h];
-  ah.xh[0] = a.xh[h];
-  ah.state = a.state + h;
-  ah.lead = nullptr;
   if (h == 1 && t.nblocks > 1) {
     // start half an iteration behind flavour 0: after its first phase end on
     // the team's counter (a bounded wait; only a matter of timing)
@@ -202,9 +197,9 @@ __device__ __forceinline__ void ens_duo_solve(const MixedArgs &a, int w, Team &t
     }
     team_sync(ht);
   }
-  if (w == 4) ens_solve_half<4>(ah, ht, ds.sh[h], ds.ms[h]);
-  else if (w == 2) ens_solve_half<2>(ah, ht, ds.sh[h], ds.ms[h]);
-  else ens_solve_half<1>(ah, ht, ds.sh[h], ds.ms[h]);
+  if (w == 4) ens_solve_half<4>(ds.args[h], ht, ds.sh[h], ds.ms[h]);
+  else if (w == 2) ens_solve_half<2>(ds.args[h], ht, ds.sh[h], ds.ms[h]);
+  else ens_solve_half<1>(ds.args[h], ht, ds.sh[h], ds.ms[h]);
   if (ht.btid == 0) ds.nph[h] = ht.nph;
   __syncthreads();  // the whole block again
   t.nph = ds.nph[0];
@@ -269,79 +264,103 @@ static __device__ __noinline__ bool ens_run_chain(const EnsLaunch &L, int c, Tea
       const int nrhs = op.c > 0.0 ? int(op.c) : 2;
       const int *status;
       const long long *iters;
+      const bool two = ch.precision != GN_PREC_FP64 && L.duo && nrhs == 2;
       if (ch.precision == GN_PREC_FP64) {
-        CgArgs<double> a;
-        a.g = g;
-        a.sm = ch.sm;
-        for (int k = 0; k < kMaxRhs; k++) {
-          const size_t off = size_t(k < 2 ? k : 1) * V;
-          a.b[k] = ch.phi + off;
-          a.x[k] = ch.X + off;
-          a.r[k] = ch.r64 + off;
-          a.p0[k] = ch.pa64 + off;
-          a.p1[k] = ch.pb64 + off;
-          a.t[k] = ch.t64 + off;
+        CgArgs<double> &a = ds.args64;
+        if (threadIdx.x == 0) {
+          a.g = g;
+          a.sm = ch.sm;
+          for (int k = 0; k < kMaxRhs; k++) {
+            const size_t off = size_t(k < 2 ? k : 1) * V;
+            a.b[k] = ch.phi + off;
+            a.x[k] = ch.X + off;
+            a.r[k] = ch.r64 + off;
+            a.p0[k] = ch.pa64 + off;
+            a.p1[k] = ch.pb64 + off;
+            a.t[k] = ch.t64 + off;
+          }
+          a.nrhs = nrhs;
+          a.variant = 1;
+          a.rel = 1;
+          a.tol = L.tol;
+          a.max_iter = (long long)V + 1;
+          a.partials = nullptr;
+          a.bar = nullptr;
+          a.err = t.err;
+          a.abort_flag = nullptr;
+          a.state = L.cg_state + size_t(blockIdx.x) * kMaxRhs;
         }
-        a.nrhs = nrhs;
-        a.variant = 1;
-        a.rel = 1;
-        a.tol = L.tol;
-        a.max_iter = (long long)V + 1;
-        a.partials = nullptr;
-        a.bar = nullptr;
-        a.err = t.err;
-        a.abort_flag = nullptr;
-        a.state = L.cg_state + size_t(blockIdx.x) * kMaxRhs;
+        __syncthreads();
         if (ch.w >= 2) ens_solve64<2>(a, t, sh, cs);
         else ens_solve64<1>(a, t, sh, cs);
         status = cs.status;
         iters = cs.iters;
       } else {
-        MixedArgs a;
-        a.g = g;
-        a.sm = ch.sm;
-        a.sm32 = ch.sm32;
-        for (int k = 0; k < kMaxRhs; k++) {
-          const size_t off = size_t(k < 2 ? k : 1) * V;
-          a.b[k] = ch.phi + off;
-          a.x[k] = ch.X + off;
-          a.t64[k] = ch.t64 + off;
-          a.rh[k] = ch.rh + off;
-          a.ph[k] = ch.ph + off;
-          a.uh[k] = ch.uh + off;
-          a.ah[k] = ch.ah + off;
-          a.xh[k] = ch.xh + off;
-        }
-        a.nrhs = nrhs;
-        a.variant = 1;
-        a.rel = 1;
-        a.scheme = mixed_scheme(g.V, nrhs, 1);
-        a.sm32_ready = 0;
-        a.tol = L.tol;
-        a.max_iter = (long long)V + 1;
-        a.delta = L.delta;
-        a.n_ru = L.n_ru;
-        a.partials = nullptr;
-        a.bar = nullptr;
-        a.err = t.err;
-        a.abort_flag = nullptr;
-        a.state = L.cg_state + size_t(blockIdx.x) * kMaxRhs;
-        if (L.duo && nrhs == 2) {
-          // sm32 by the whole team, then one flavour per half of every block
+        if (two) {  // sm32 by the whole team, then one flavour per half of every block
           for (uint32_t i = t.tid; i < V; i += t.nthreads) ch.sm32[i] = float(ch.sm[i]);
           ok = end_phase<0>(acc, sh, t);
-          a.sm32_ready = 1;
-          if (ok) ens_duo_solve(a, ch.w, t, duo, ds);
+        }
+        if (threadIdx.x == 0) {
+          MixedArgs &a = ds.args[0];
+          a.g = g;
+          a.sm = ch.sm;
+          a.sm32 = ch.sm32;
+          a.pm = nullptr;
+          a.pm32 = nullptr;
+          for (int k = 0; k < kMaxRhs; k++) {
+            const size_t off = size_t(k < 2 ? k : 1) * V;
+            a.b[k] = ch.phi + off;
+            a.x[k] = ch.X + off;
+            a.t64[k] = ch.t64 + off;
+            a.rh[k] = ch.rh + off;
+            a.ph[k] = ch.ph + off;
+            a.uh[k] = ch.uh + off;
+            a.ah[k] = ch.ah + off;
+            a.xh[k] = ch.xh + off;
+          }
+          a.nrhs = nrhs;
+          a.variant = 1;
+          a.rel = 1;
+          a.scheme = mixed_scheme(g.V, nrhs, 1);
+          a.sm32_ready = two ? 1 : 0;
+          a.lead = nullptr;
+          a.lead_count = 0;
+          a.tol = L.tol;
+          a.max_iter = (long long)V + 1;
+          a.delta = L.delta;
+          a.n_ru = L.n_ru;
+          a.partials = nullptr;
+          a.bar = nullptr;
+          a.err = t.err;
+          a.abort_flag = nullptr;
+          a.state = L.cg_state + size_t(blockIdx.x) * kMaxRhs;
+          if (two) {  // flavour 1 in args[1], flavour 0 alone in args[0]
+            MixedArgs &a1 = ds.args[1];
+            a1 = a;
+            a1.b[0] = a.b[1];
+            a1.x[0] = a.x[1];
+            a1.t64[0] = a.t64[1];
+            a1.rh[0] = a.rh[1];
+            a1.ph[0] = a.ph[1];
+            a1.uh[0] = a.uh[1];
+            a1.ah[0] = a.ah[1];
+            a1.xh[0] = a.xh[1];
+            a1.state = a.state + 1;
+            a.nrhs = a1.nrhs = 1;
+          }
+        }
+        __syncthreads();
+        if (two) {
+          if (ok) ens_duo_solve(ch.w, t, duo, ds);
         } else {
-          if (ch.w == 4) ens_solve<4>(a, t, sh, ms);
-          else if (ch.w == 2) ens_solve<2>(a, t, sh, ms);
-          else ens_solve<1>(a, t, sh, ms);
+          if (ch.w == 4) ens_solve<4>(ds.args[0], t, sh, ms);
+          else if (ch.w == 2) ens_solve<2>(ds.args[0], t, sh, ms);
+          else ens_solve<1>(ds.args[0], t, sh, ms);
         }
         status = ms.status;
         iters = ms.iters;
       }
       if (leader) {
-        const bool two = ch.precision != GN_PREC_FP64 && L.duo && nrhs == 2;
         for (int k = 0; k < nrhs; k++) {
           const int s = two ? ds.ms[k].status[0] : status[k];
           if (s != kCgConverged && s != kCgConvergedStart) st->failed = 1;

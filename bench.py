@@ -57,7 +57,7 @@ BETA_S = 0.85
 NFLAV = 4
 # DRAM bytes per launch measured with ncu (one capture each; summaries under
 # profiles/): the dominant solver kernel at L = 64 and the Dirac apply at L = 256.
-CG_MIXED_DRAM_BYTES = 6_683_904      # 6.390 MB read + 0.294 MB written
+CG_MIXED_DRAM_BYTES = 7_031_296      # 6.450 MB read + 0.581 MB written (cg_mixed_duo_kernel)
 DIRAC256_DRAM_BYTES = 379_232_256    # 269.540 MB read + 109.692 MB written
 METRIC = "HMC trajectories/s at L=64 (LFMN2VF, 10 x eps 0.05, CG to 1e-10 true relative residual)"
 UNIT = "traj/s"
@@ -539,7 +539,7 @@ def kernel_roofline(lat, stream, a, G):
                                       x, x^, r^ out; sm shared)
       start            12 + 28 nrhs (b in; x, x^, r^, p^ out; sm in, sm32 out)
     DRAM traffic per launch from ncu (--case cg64, dram__bytes_read.sum +
-    dram__bytes_write.sum of cg_mixed_kernel): the working set stays in L2."""
+    dram__bytes_write.sum of cg_mixed_duo_kernel): the working set stays in L2."""
     V = lat.V
     sm = lat.field_ptr(G.GN_F_SM)
     phi = lat.field_ptr(G.GN_F_PHI)
@@ -558,7 +558,8 @@ def kernel_roofline(lat, stream, a, G):
     inner = max(i["inner_iterations"] for i in infos)
     ru = sum(i["reliable_updates"] for i in infos)
     nbytes = V * ((8 + 44 * 2) * inner + 72 * ru + 12 + 28 * 2)
-    return {"gbs": nbytes / (ms * 1e-3) / 1e9, "kernel": "cg_mixed_kernel<1, 2, 1024, 4, 0> (2 flavours, L=%d)" % lat.L,
+    return {"gbs": nbytes / (ms * 1e-3) / 1e9,
+            "kernel": "cg_mixed_duo_kernel<1, 1024, 4> (2 flavours as two teams, L=%d)" % lat.L,
             "ms": ms, "bytes": nbytes, "traffic": CG_MIXED_DRAM_BYTES if lat.L == 64 else None,
             "note": f"{inner} inner iterations, {ru} reliable updates, {ms:.3f} ms per launch; working set "
                     f"{(2 * 5 * 4 + 8 * 3) * V / 1e6:.0f} MB is L2-resident within the solve"}
@@ -611,7 +612,7 @@ def batched_bench(G, dev, nchains=256, ntraj=2, warmup=1, tune=True, precision=N
             "graph": info["graph"], "launches_per_trajectory": info["launches_per_trajectory"] + 2}
 
 
-def serve_bench(G, nreq=600, rate=200.0, warm=24, seed=5, precision=None):
+def serve_bench(G, nreq=600, rate=200.0, warm=24, seed=5, precision=None, tiers=None):
     """The serving loop: Poisson arrivals at `rate`/s of requests -- one HMC
     trajectory (70 %), one solve with an N(0, 1) right-hand side (20 %), a
     condensate estimate from 16 Z2 vectors (10 %) -- on 256 resident chains,
@@ -624,7 +625,8 @@ def serve_bench(G, nreq=600, rate=200.0, warm=24, seed=5, precision=None):
     Ls = [L for L in range(8, 65, 8) for _ in range(32)]
     betas = rng.uniform(0.6, 1.1, len(Ls))
     types = (G.GN_REQ_TRAJECTORY, G.GN_REQ_SOLVE, G.GN_REQ_CONDENSATE)
-    with G.Server(G.Ensemble.params(0.08, 8, precision=prec), mem_budget_bytes=32e9, seed=seed) as srv:
+    kw = {} if tiers is None else {"tiers": tiers}
+    with G.Server(G.Ensemble.params(0.08, 8, precision=prec), mem_budget_bytes=32e9, seed=seed, **kw) as srv:
         for c, (L, b) in enumerate(zip(Ls, betas)):
             srv.add_chain(L, b, rng.normal(0.0, np.sqrt(2.0 / (NFLAV * b)), L ** 3), stream_id=c)
         for k in range(warm):
@@ -665,6 +667,42 @@ def serve_bench(G, nreq=600, rate=200.0, warm=24, seed=5, precision=None):
         if len(lt):
             out[name] = {"n": int(len(lt)), "p50_ms": float(np.percentile(lt, 50) * 1e3),
                          "p99_ms": float(np.percentile(lt, 99) * 1e3)}
+    # trajectories by lattice size: median and worst latency
+    by_L = {}
+    for r in info:
+        if r["type"] == 0:
+            by_L.setdefault(Ls[r["chain"]], []).append(r["t_done"] - r["t_arrival"])
+    out["trajectory_by_L_ms"] = {str(L): [round(float(np.median(v)) * 1e3, 1), round(float(max(v)) * 1e3, 1)]
+                                 for L, v in sorted(by_L.items())}
+    # the slowest requests: L, type, queueing (arrival to admission), run (admission to completion), ms
+    slow = sorted(info, key=lambda r: r["t_done"] - r["t_arrival"])[-5:]
+    out["slowest"] = [[Ls[r["chain"]], int(r["type"]), round((r["t_admit"] - r["t_arrival"]) * 1e3, 1),
+                       round((r["t_done"] - r["t_admit"]) * 1e3, 1)] for r in slow]
+    return out
+
+
+def serve_standalone(G, precision=None, seed=5):
+    """Latency of one request alone on the server (nothing else queued or
+    running): a trajectory on a chain of each L in 8..64, a solve and a
+    16-vector condensate at L = 64."""
+    prec = G.GN_PREC_MIXED if precision is None else precision
+    rng = np.random.default_rng(seed)
+    Ls = list(range(8, 65, 8))
+    out = {}
+    with G.Server(G.Ensemble.params(0.08, 8, precision=prec), mem_budget_bytes=32e9, seed=seed) as srv:
+        for c, L in enumerate(Ls):
+            srv.add_chain(L, 0.85, rng.normal(0.0, np.sqrt(2.0 / (NFLAV * 0.85)), L ** 3), stream_id=c)
+        for c in range(len(Ls)):  # warm-up
+            srv.submit(c, G.GN_REQ_TRAJECTORY, 0)
+        srv.drain()
+        for name, t, chains in (("trajectory", G.GN_REQ_TRAJECTORY, range(len(Ls))),
+                                ("solve", G.GN_REQ_SOLVE, [len(Ls) - 1]),
+                                ("condensate", G.GN_REQ_CONDENSATE, [len(Ls) - 1])):
+            for c in chains:
+                rid = srv.submit(c, t, 16 if t == G.GN_REQ_CONDENSATE else 0)
+                srv.drain()
+                r = srv.request(rid)
+                out[f"{name}_L{Ls[c]}_ms"] = round((r["t_done"] - r["t_arrival"]) * 1e3, 2)
     return out
 
 
@@ -676,7 +714,8 @@ def serve_sweep(G, rates=(25.0, 50.0, 100.0, 150.0, 200.0), nreq=300):
     mixed = [serve_bench(G, nreq=nreq, rate=r) for r in rates]
     fp64 = [serve_bench(G, nreq=nreq, rate=r, precision=G.GN_PREC_FP64) for r in (50.0, 200.0)]
     sus = [r["offered_req_per_s"] for r in mixed if r["throughput_req_per_s"] >= 0.95 * r["offered_req_per_s"]]
-    return {"mixed": mixed, "fp64": fp64, "max_sustained_req_s": max(sus) if sus else None}
+    return {"mixed": mixed, "fp64": fp64, "max_sustained_req_s": max(sus) if sus else None,
+            "standalone_mixed": serve_standalone(G)}
 
 
 def u1_case(G, dev, L=64, md_steps=10, eps=0.05, pi_steps=10, tol=1e-10, reps=2):
