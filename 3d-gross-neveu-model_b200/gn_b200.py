@@ -740,7 +740,17 @@ class Ensemble:
 class Server:
     """Requests on resident chains with continuous batching (gn_server_* of gn_b200.h)."""
 
-    def __init__(self, traj_params, mem_budget_bytes=8e9, seed=1231, tiers=((16, 48 ** 3), (4, 16 ** 3)), device=0):
+    # Team tiers: L >= 32 shares the whole GPU (teams of at least 32 blocks),
+    # L = 16..24 runs on 8 blocks, L = 12 on 2, the rest on single blocks.
+    # Measured with bench.py's serving mix at 50 requests/s: p50 54 ms, p99
+    # 454 ms, against 154 ms and 1.3 s for the older ((16, 48^3), (4, 16^3)),
+    # which left L = 32 and 40 on teams of 4 blocks (80 and 148 ms for one
+    # trajectory alone, against 55-68 ms for L = 48-64 on the whole GPU); a
+    # step lasts as long as its costliest slice, so those slices held up every
+    # request beside them.
+    DEFAULT_TIERS = ((32, 32 ** 3), (8, 16 ** 3), (2, 12 ** 3))
+
+    def __init__(self, traj_params, mem_budget_bytes=8e9, seed=1231, tiers=DEFAULT_TIERS, device=0):
         """tiers: (blocks per team, minimum volume) pairs, team sizes dividing each other."""
         self.lib = load_library()
         self.srv = C.c_void_p()

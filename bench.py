@@ -500,6 +500,7 @@ def summaries(d, peaks):
     if "serving" in d:
         s = d["serving"]
         out["serving"] = {"max_sustained_req_s": s["max_sustained_req_s"],
+                          "alone_L64_traj_ms": s.get("standalone_mixed", {}).get("trajectory_L64_ms"),
                           "mixed": [[r["offered_req_per_s"], round(r["throughput_req_per_s"], 1), round(r["p50_ms"]),
                                      round(r["p99_ms"])] for r in s["mixed"]],
                           "cols": "offered/s, done/s, p50 ms, p99 ms"}
@@ -706,7 +707,7 @@ def serve_standalone(G, precision=None, seed=5):
     return out
 
 
-def serve_sweep(G, rates=(25.0, 50.0, 100.0, 150.0, 200.0), nreq=300):
+def serve_sweep(G, rates=(25.0, 50.0, 100.0, 150.0, 200.0), nreq=600):
     """serve_bench at a ladder of offered rates in mixed precision, and at 50/s
     and 200/s in FP64.  max_sustained_req_s: the highest offered rate whose
     completion rate (requests over first arrival to last completion) stays
