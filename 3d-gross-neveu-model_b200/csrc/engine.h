@@ -180,6 +180,7 @@ class Engine {
   // arrival counter and its FP32 copy of sm (each team writes its own)
   PhaseBar *bar2_ = nullptr;
   float *sm32b_ = nullptr;
+  float *pm32b_ = nullptr;  // ... and of the pi mass (the U(1) model)
   bool mixed_duo_ = true;
   double *partials_ = nullptr;
   double *h_partials_ = nullptr;

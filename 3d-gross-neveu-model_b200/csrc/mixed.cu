@@ -20,18 +20,22 @@ void Engine::mixed_init() {
   sm32_ = (float *)alloc(V * sizeof(float));
   pm32_ = (float *)alloc(V * sizeof(float));
   sm32b_ = (float *)alloc(V * sizeof(float));
+  pm32b_ = (float *)alloc(V * sizeof(float));
   bar2_ = (PhaseBar *)alloc(sizeof(PhaseBar));
   const char *duo = getenv("GN_MIXED_DUO");
   mixed_duo_ = !(duo != nullptr && duo[0] == '0');
 }
 
-// Two real systems as two teams of half blocks (cg_mixed_duo_kernel).
+// Two systems as two teams of half blocks (cg_mixed_duo_kernel): two real
+// systems in 1024-thread blocks, or the U(1) model's two complex systems in
+// 512-thread blocks (the block shapes of the lock-step kernels).
 template <int W>
-static const void *mixed_duo_kernel() {
-  return (const void *)cg_mixed_duo_kernel<1, kWideThreads, W>;
+static const void *mixed_duo_kernel(bool cm) {
+  return cm ? (const void *)cg_mixed_duo_kernel<2, kSolverThreads, W, true>
+            : (const void *)cg_mixed_duo_kernel<1, kWideThreads, W>;
 }
-static const void *mixed_duo_kernel_ptr(int w) {
-  return w == 4 ? mixed_duo_kernel<4>() : w == 2 ? mixed_duo_kernel<2>() : mixed_duo_kernel<1>();
+static const void *mixed_duo_kernel_ptr(int w, bool cm) {
+  return w == 4 ? mixed_duo_kernel<4>(cm) : w == 2 ? mixed_duo_kernel<2>(cm) : mixed_duo_kernel<1>(cm);
 }
 
 template <int W>
@@ -108,12 +112,14 @@ int Engine::solve_mixed(const double *sm, const double *const *b, double *const 
   }
   const int w = fp64_width(L_, ptrs, 2 + 2 * nrhs) == 2 ? row_width(L_, 4) : 1;
   const int nb = cg_blocks(ncomp, nrhs, true, w);
-  if (mixed_duo_ && pm == nullptr && ncomp == 1 && nrhs == 2) {
+  const bool cm = pm != nullptr;
+  if (mixed_duo_ && nrhs == 2 && (cm ? ncomp == 2 : ncomp == 1)) {
     // the two systems as two teams of half blocks: the same units per thread,
     // each team with its own counter, partials (after the first team's
     // 2 (kSyncQ + 1) nb slots), sm32 copy and state slot
-    const void *fn = mixed_duo_kernel_ptr(w);
-    const int cap = coop_capacity(fn, kWideThreads);
+    const void *fn = mixed_duo_kernel_ptr(w, cm);
+    const int bs = cm ? kSolverThreads : kWideThreads;
+    const int cap = coop_capacity(fn, bs);
     if (cap < 1) throw GnError(GN_ERR_CUDA, "CG kernel cannot be resident as a cooperative grid");
     const int nbd = nb < cap ? nb : cap;
     MixedArgs a1 = a;
@@ -131,6 +137,7 @@ int Engine::solve_mixed(const double *sm, const double *const *b, double *const 
       a.x[k] = a1.x[k] = nullptr;
     }
     a1.sm32 = sm32b_;
+    a1.pm32 = pm32b_;
     a1.bar = bar2_;
     a1.partials = partials_ + size_t(2) * (kSyncQ + 1) * nbd;
     a1.state = state_ + 1;
@@ -139,7 +146,7 @@ int Engine::solve_mixed(const double *sm, const double *const *b, double *const 
     a1.lead_count = (unsigned long long)nbd;
     check(cudaMemsetAsync(bar2_, 0, sizeof(PhaseBar), stream_), "memset");
     void *args[] = {(void *)&a, (void *)&a1};
-    check(cudaLaunchCooperativeKernel(fn, dim3(nbd), dim3(kWideThreads), args, 0, stream_),
+    check(cudaLaunchCooperativeKernel(fn, dim3(nbd), dim3(bs), args, 0, stream_),
           "cg_mixed_duo_kernel launch");
     launches++;
     return finish_solve(nrhs, info);

@@ -803,7 +803,7 @@ __global__ void __launch_bounds__(BS, 1) cg_mixed_kernel(MixedArgs a) {
 // runs its own inlined copy of the solver, which reads its argument struct
 // from the kernel's parameters at fixed offsets, as the single-team kernel
 // does.
-template <int NC, int BS, int W, int H>
+template <int NC, int BS, int W, int H, bool CM>
 __device__ __forceinline__ void duo_half(const MixedArgs &a, SyncShared &sh, MixedShared &ms) {
   Team team;
   team.tid = blockIdx.x * (BS / 2) + (threadIdx.x - H * (BS / 2));
@@ -823,16 +823,17 @@ __device__ __forceinline__ void duo_half(const MixedArgs &a, SyncShared &sh, Mix
     }
     team_sync(team);
   }
-  mixed_solve<NC, 1, W>(a, team, sh, ms);
+  mixed_solve<NC, 1, W, CM>(a, team, sh, ms);
 }
 
-template <int NC, int BS, int W>
+// CM: the U(1) model's two complex systems (NC = 2), as cg_mixed_kernel's CM.
+template <int NC, int BS, int W, bool CM = false>
 __global__ void __launch_bounds__(BS, 1) cg_mixed_duo_kernel(MixedArgs a0, MixedArgs a1) {
   static_assert(BS % 64 == 0, "each half holds whole warps");
   __shared__ SyncShared sh[2];
   __shared__ MixedShared ms[2];
-  if (threadIdx.x < BS / 2) duo_half<NC, BS, W, 0>(a0, sh[0], ms[0]);
-  else duo_half<NC, BS, W, 1>(a1, sh[1], ms[1]);
+  if (threadIdx.x < BS / 2) duo_half<NC, BS, W, 0, CM>(a0, sh[0], ms[0]);
+  else duo_half<NC, BS, W, 1, CM>(a1, sh[1], ms[1]);
 }
 
 }  // namespace gn
