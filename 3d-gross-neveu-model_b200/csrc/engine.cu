@@ -3,6 +3,7 @@
 // (mul then add) wherever the reference's result is reproducible bit for bit.
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <stdexcept>
 
@@ -66,6 +67,13 @@ Engine::Engine(int L, int device) : L_(L), device_(device) {
   bar_ = (PhaseBar *)alloc(sizeof(PhaseBar));
   err_ = (int *)alloc(sizeof(int));
   state_ = (CgState *)alloc(sizeof(CgState) * kMaxRhs);
+  state_base_ = state_;
+  traj_states_ = (CgState *)alloc(sizeof(CgState) * 2 * kTrajSolves);
+  traj_partials_ = (double *)alloc(sizeof(double) * 12 * op_blocks(V_, num_sms_));
+  check(cudaHostAlloc((void **)&h_traj_states_, sizeof(CgState) * 2 * kTrajSolves, cudaHostAllocDefault),
+        "cudaHostAlloc");
+  check(cudaHostAlloc((void **)&h_traj_partials_, sizeof(double) * 12 * op_blocks(V_, num_sms_),
+                      cudaHostAllocDefault), "cudaHostAlloc");
   check(cudaHostAlloc((void **)&h_partials_, size_t(32) * max_blocks_ * d, cudaHostAllocDefault), "cudaHostAlloc");
   check(cudaHostAlloc((void **)&h_state_, sizeof(CgState) * kMaxRhs, cudaHostAllocDefault), "cudaHostAlloc");
   check(cudaHostAlloc((void **)&h_abort_, sizeof(int), cudaHostAllocMapped), "cudaHostAlloc");
@@ -82,6 +90,8 @@ Engine::~Engine() {
   for (void *p : allocs_) cudaFree(p);
   if (h_partials_) cudaFreeHost(h_partials_);
   if (h_state_) cudaFreeHost(h_state_);
+  if (h_traj_states_) cudaFreeHost(h_traj_states_);
+  if (h_traj_partials_) cudaFreeHost(h_traj_partials_);
   if (h_abort_) cudaFreeHost(h_abort_);
   if (h_stage_) cudaFreeHost(h_stage_);
   if (stream_) cudaStreamDestroy(stream_);
@@ -163,6 +173,14 @@ void Engine::energy_terms(const double *P, const double *phi, const double *X, c
   check(cudaMemcpyAsync(h_partials_, partials_, sizeof(double) * 6 * nb, cudaMemcpyDeviceToHost, stream_), "copy");
   check(cudaStreamSynchronize(stream_), "energy sync");
   for (int q = 0; q < 3; q++) out[q] = sum_partials(h_partials_, nb, q);
+}
+
+// The energy kernel's partial sums (6 per block) into dst, without a host copy.
+void Engine::energy_launch(const double *P, const double *phi, const double *X, const double *sigma, double *dst) {
+  const int nb = op_blocks(V_, num_sms_);
+  energy_kernel<double><<<nb, kOpThreads, 0, stream_>>>(uint32_t(V_), P, phi, X, sigma, dst);
+  check(cudaGetLastError(), "energy_kernel");
+  launches++;
 }
 
 void Engine::cond_dots(const double *v, const double *D, double out[3]) {
@@ -259,7 +277,7 @@ int Engine::solve(const double *sm, const double *const *b, double *const *x, in
   a.abort_flag = d_abort_;
   a.state = state_;
   check(cudaMemsetAsync(bar_, 0, sizeof(PhaseBar), stream_), "memset");
-  check(cudaMemsetAsync(err_, 0, sizeof(int), stream_), "memset");
+  if (!defer_) check(cudaMemsetAsync(err_, 0, sizeof(int), stream_), "memset");
   const void *ptrs[2 * kMaxRhs + 1] = {sm};
   for (int k = 0; k < nrhs; k++) {
     ptrs[1 + 2 * k] = b[k];
@@ -274,6 +292,7 @@ int Engine::solve(const double *sm, const double *const *b, double *const *x, in
 }
 
 int Engine::finish_solve(int nrhs, SolveInfo *info) {
+  if (defer_) return GN_OK;  // the caller reads the states when its queue is done
   int h_err = 0;
   check(cudaMemcpyAsync(h_state_, state_, sizeof(CgState) * nrhs, cudaMemcpyDeviceToHost, stream_), "copy");
   check(cudaMemcpyAsync(&h_err, err_, sizeof(int), cudaMemcpyDeviceToHost, stream_), "copy");
@@ -352,31 +371,66 @@ int Engine::trajectory(const gn_hmc_params &hp, double (*gauss)(void), double (*
     res->inner_iterations = inner;
     res->reliable_updates = rel;
   };
-  int st = solve(sm_, phis, Xs, 2, 1, hp.tol_high, 1, hp.relative, 0, hp.precision, info);
-  count_flavours(info, 2, iters, calls, inner, rel);
-  if (st != GN_OK) {
-    restore();
-    check(cudaStreamSynchronize(stream_), "restore");
-    finish(0);
-    return GN_NOT_CONVERGED;
-  }
-  const double ccoef = (4 * hp.beta_s / 4.0);  // (NFLAV * beta_scalar / 4.0), moleculardynamics.c:316
-  double e[3];
-  energy_terms(P_, phi_, X_, sigma(), e);
-  const double h0 = (e[0] + e[1]) + ccoef * e[2];
   const std::vector<Op> ops = schedule(hp.integrator, hp.eps, hp.steps);
+  // Deferred mode: the whole trajectory is queued on the stream with no host
+  // round trip; every solve leaves its two states in traj_states_ and the
+  // energies their partial sums in traj_partials_, read back once at the end
+  // (a failed solve is then found in order, and sigma restored, as the
+  // reference's early return would leave it).  The exact-order mode, whose
+  // energies are serial sums on the host path, checks every solve as it goes.
+  int nsolve = 1;
+  for (const Op &o : ops) nsolve += (o.op == OP_F_MED || o.op == OP_F_HIGH || o.op == OP_S_HIGH) ? 1 : 0;
+  const bool defer = !exact && nsolve <= kTrajSolves;
+  struct DeferScope {  // finish_solve and the solvers' state slots back to normal on every exit
+    Engine &e;
+    bool on;
+    DeferScope(Engine &en, bool d) : e(en), on(d) {
+      if (on) {
+        e.defer_ = true;
+        e.check(cudaMemsetAsync(e.err_, 0, sizeof(int), e.stream_), "memset");
+      }
+    }
+    ~DeferScope() {
+      e.defer_ = false;
+      e.state_ = e.state_base_;
+    }
+  } defer_scope(*this, defer);
+  std::vector<double> dist_before;  // deferred: the sigma distance before each solve
+  int isolve = 0;
+  // one two-flavour solve; false when it failed (synchronous mode only)
+  auto run_solve = [&](double tol, int variant) {
+    if (defer) {
+      state_ = traj_states_ + 2 * isolve++;
+      dist_before.push_back(res->distance);
+      solve(sm_, phis, Xs, 2, 1, tol, variant, hp.relative, 0, hp.precision, info);
+      return true;
+    }
+    const int st = solve(sm_, phis, Xs, 2, 1, tol, variant, hp.relative, 0, hp.precision, info);
+    count_flavours(info, 2, iters, calls, inner, rel);
+    if (st != GN_OK) {
+      restore();
+      check(cudaStreamSynchronize(stream_), "restore");
+      finish(0);
+      distance += res->distance;
+      return false;
+    }
+    return true;
+  };
+  const double ccoef = (4 * hp.beta_s / 4.0);  // (NFLAV * beta_scalar / 4.0), moleculardynamics.c:316
+  const int enb = op_blocks(V_, num_sms_);
+  double e[3];
+  double h0 = 0.0;
+  if (!run_solve(hp.tol_high, 1)) return GN_NOT_CONVERGED;
+  if (defer) {
+    energy_launch(P_, phi_, X_, sigma(), traj_partials_);
+  } else {
+    energy_terms(P_, phi_, X_, sigma(), e);
+    h0 = (e[0] + e[1]) + ccoef * e[2];
+  }
   for (size_t k = 0; k < ops.size(); k++) {
     const Op &o = ops[k];
     if (o.op == OP_F_MED || o.op == OP_F_HIGH) {
-      const double tol = o.op == OP_F_MED ? hp.tol_medium : hp.tol_high;
-      st = solve(sm_, phis, Xs, 2, 1, tol, 0, hp.relative, 0, hp.precision, info);
-      count_flavours(info, 2, iters, calls, inner, rel);
-      if (st != GN_OK) {
-        restore();
-        check(cudaStreamSynchronize(stream_), "restore");
-        finish(0);
-        return GN_NOT_CONVERGED;
-      }
+      if (!run_solve(o.op == OP_F_MED ? hp.tol_medium : hp.tol_high, 0)) return GN_NOT_CONVERGED;
       dirac(sm_, X_, Y_, 2, GN_OP_MT);
       if (k + 1 < ops.size() && ops[k + 1].op == OP_P) {
         force(X_, Y_, sigma(), hp.beta_s, F_, P_, ops[k + 1].c);
@@ -389,21 +443,54 @@ int Engine::trajectory(const gn_hmc_params &hp, double (*gauss)(void), double (*
     } else if (o.op == OP_Q) {
       sigma_mass(sigma(), P_, o.c, sigma_alt(), sm_);
       swap_sigma();
-      distance += o.c;
       res->distance += o.c;
     } else {
-      st = solve(sm_, phis, Xs, 2, 1, hp.tol_high, 1, hp.relative, 0, hp.precision, info);
+      if (!run_solve(hp.tol_high, 1)) return GN_NOT_CONVERGED;
+    }
+  }
+  double h1 = 0.0;
+  if (defer) {
+    energy_launch(P_, phi_, X_, sigma(), traj_partials_ + 6 * enb);
+    int h_err = 0;
+    check(cudaMemcpyAsync(h_traj_states_, traj_states_, sizeof(CgState) * 2 * isolve, cudaMemcpyDeviceToHost,
+                          stream_), "copy states");
+    check(cudaMemcpyAsync(h_traj_partials_, traj_partials_, sizeof(double) * 12 * enb, cudaMemcpyDeviceToHost,
+                          stream_), "copy partials");
+    check(cudaMemcpyAsync(&h_err, err_, sizeof(int), cudaMemcpyDeviceToHost, stream_), "copy err");
+    check(cudaStreamSynchronize(stream_), "trajectory");
+    if (h_err == 1) throw GnError(GN_ERR_TIMEOUT, "CG grid barrier timed out");
+    if (h_err == 2) throw GnError(GN_ERR_ABORTED, "CG aborted on request");
+    for (int j = 0; j < isolve; j++) {
+      bool ok = true;
+      for (int f = 0; f < 2; f++) {
+        const CgState &c = h_traj_states_[2 * j + f];
+        info[f].status = c.status;
+        info[f].iters = c.iters;
+        info[f].r2 = c.r2;
+        info[f].b2 = c.b2;
+        info[f].inner = c.iters;
+        info[f].reliable = c.reliable;
+        if (c.status != kCgConverged && c.status != kCgConvergedStart) ok = false;
+      }
       count_flavours(info, 2, iters, calls, inner, rel);
-      if (st != GN_OK) {
+      if (!ok) {  // the reference returns here: sigma restored, its later steps undone
+        res->distance = dist_before[j];
         restore();
         check(cudaStreamSynchronize(stream_), "restore");
         finish(0);
+        distance += res->distance;
         return GN_NOT_CONVERGED;
       }
     }
+    for (int q = 0; q < 3; q++) e[q] = sum_partials(h_traj_partials_, enb, q);
+    h0 = (e[0] + e[1]) + ccoef * e[2];
+    for (int q = 0; q < 3; q++) e[q] = sum_partials(h_traj_partials_ + 6 * enb, enb, q);
+    h1 = (e[0] + e[1]) + ccoef * e[2];
+  } else {
+    energy_terms(P_, phi_, X_, sigma(), e);
+    h1 = (e[0] + e[1]) + ccoef * e[2];
   }
-  energy_terms(P_, phi_, X_, sigma(), e);
-  const double h1 = (e[0] + e[1]) + ccoef * e[2];
+  distance += res->distance;
   res->H0 = h0;
   res->H1 = h1;
   res->dH = h1 - h0;

@@ -146,6 +146,7 @@ class Engine {
                   int variant, int rel, long long max_iter, SolveInfo *info);
   void mt_exact(const double *sm, const double *in, double *out, int ncomp);
   void energy_exact(const double *P, const double *phi, const double *X, const double *sigma, double out[3]);
+  void energy_launch(const double *P, const double *phi, const double *X, const double *sigma, double *dst);
   void cond_dots_exact(const double *v, const double *D, double out[4]);
   void mixed_init();
   const void *mixed_kernel_ptr(int ncomp, int nrhs, int w);
@@ -186,8 +187,16 @@ class Engine {
   double *h_partials_ = nullptr;
   PhaseBar *bar_ = nullptr;
   int *err_ = nullptr;
-  CgState *state_ = nullptr;
+  CgState *state_ = nullptr;  // the solvers' state slots (traj_states_ slots in a deferred trajectory)
   CgState *h_state_ = nullptr;
+  CgState *state_base_ = nullptr;
+  // a trajectory queued without a host round trip per solve (trajectory()):
+  // finish_solve then returns at once, and the states and energies are read
+  // back together at the end
+  bool defer_ = false;
+  static constexpr int kTrajSolves = 256;  // two-flavour solves of one deferred trajectory, at most
+  CgState *traj_states_ = nullptr, *h_traj_states_ = nullptr;
+  double *traj_partials_ = nullptr, *h_traj_partials_ = nullptr;
   int *h_abort_ = nullptr;
   int *d_abort_ = nullptr;
   double *h_stage_ = nullptr;

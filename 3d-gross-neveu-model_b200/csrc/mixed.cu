@@ -102,7 +102,7 @@ int Engine::solve_mixed(const double *sm, const double *const *b, double *const 
   a.abort_flag = d_abort_;
   a.state = state_;
   check(cudaMemsetAsync(bar_, 0, sizeof(PhaseBar), stream_), "memset");
-  check(cudaMemsetAsync(err_, 0, sizeof(int), stream_), "memset");
+  if (!defer_) check(cudaMemsetAsync(err_, 0, sizeof(int), stream_), "memset");
   // FP32 sweeps in items of up to 4 sites (float4) when the caller's FP64
   // arrays allow the 2-site FP64 sweeps, else one site per item throughout
   const void *ptrs[2 * kMaxRhs + 2] = {sm, pm != nullptr ? pm : sm};

@@ -378,10 +378,8 @@ __device__ __forceinline__ void mixed_solve(const MixedArgs &a, Team &team, Sync
           }
         }
       });
-      ok = end_phase<2 * NR>(acc, sh, team, abort_req);
-      if (!ok) break;
-      if (team.btid < kMaxRhs) {
-        const int k = team.btid;
+      // the step parameters of system k from the pass's totals
+      auto book = [&](int k) {
         s_ru[k] = 0;
         s_step[k] = 0;
         if (k < a.nrhs && s_active[k]) {
@@ -416,7 +414,14 @@ __device__ __forceinline__ void mixed_solve(const MixedArgs &a, Team &team, Sync
             if (rn < a.delta * s_rmax[k] || s_since[k] >= a.n_ru) s_ru[k] = 1;
           }
         }
-      }
+        if (NR == 1 && k == 0) {  // one system: its lists too, saving a barrier below
+          sys_list_from(s_upd, s_ru, a.nrhs);
+          sys_list_from(s_stp, s_step, a.nrhs);
+        }
+      };
+      ok = end_phase<2 * NR>(acc, sh, team, abort_req);
+      if (ok && team.btid < kMaxRhs) book(int(team.btid));
+      if (!ok) break;
     } else {
       // A: p^ = r^ + beta p^, t^ = M^T p^ = M^T r^ + beta t^ (linearity: only r^
       // is gathered; p^ and t^ are updated in place at the unit's own sites)
@@ -519,11 +524,13 @@ __device__ __forceinline__ void mixed_solve(const MixedArgs &a, Team &team, Sync
     }
     const int abort_seen = sh.flag;  // block 0's abort flag (the next phase ends overwrite sh.flag)
     team_sync(team);
-    if (team.btid == 0) {
-      sys_list_from(s_upd, s_ru, a.nrhs);
-      if (split) sys_list_from(s_stp, s_step, a.nrhs);
+    if (!(NR == 1 && split)) {
+      if (team.btid == 0) {
+        sys_list_from(s_upd, s_ru, a.nrhs);
+        if (split) sys_list_from(s_stp, s_step, a.nrhs);
+      }
+      team_sync(team);
     }
-    team_sync(team);
     if (abort_seen != 0) {  // block 0 saw the host's abort request
       if (team.btid == 0 && team.brank == 0) atomicExch(team.err, 2);
       ok = false;

@@ -440,8 +440,8 @@ def run_ours(a, world, rank, local):
     dirac = dirac_roofline(G, stream, dev)
     peaks = load_peaks()
     detail = {}
+    detail["batched"] = batched_bench(G, dev, world=world)
     if world == 1:
-        detail["batched"] = batched_bench(G, dev)
         lay = (detail["batched"]["layout"]["group_blocks"], detail["batched"]["layout"]["big_min_volume"])
         detail["batched_fp64"] = batched_bench(G, dev, precision=G.GN_PREC_FP64, layout=lay)
         if l128_job is not None:
@@ -494,8 +494,9 @@ def summaries(d, peaks):
     """Short forms of the side measurements for the bench line."""
     out = {}
     if "batched" in d:
-        b, b64 = d["batched"], d["batched_fp64"]
-        out["batched"] = {"mixed_traj_s": round(b["value"], 1), "fp64_traj_s": round(b64["value"], 1),
+        b, b64 = d["batched"], d.get("batched_fp64")
+        out["batched"] = {"mixed_traj_s": round(b["value"], 1),
+                          "fp64_traj_s": None if b64 is None else round(b64["value"], 1),
                           "solver_frac": round(b["solver_gbs"] / peaks["hbm_gbs"], 3)}
     if "serving" in d:
         s = d["serving"]
@@ -566,49 +567,59 @@ def kernel_roofline(lat, stream, a, G):
                     f"{(2 * 5 * 4 + 8 * 3) * V / 1e6:.0f} MB is L2-resident within the solve"}
 
 
-def batched_bench(G, dev, nchains=256, ntraj=2, warmup=1, tune=True, precision=None, layout=None):
-    """The batched ensemble: nchains chains with L uniform in {8, 12, 16, 24, 32,
-    48} (seeded), beta_s on a uniform grid over [0.5, 1.2], LFMN2VF 8 x eps 0.08,
-    every solve mixed precision to 1e-10 (true relative residual), device
-    Philox draws, one persistent kernel per MD step replayed as a CUDA graph.
-    Timed with CUDA events on the ensemble's stream over `ntraj` trajectories
-    of every chain after `warmup`.  Algorithmic bytes: 96 per site per pair of
-    solver iterations (the two flavours' FP32 sweeps, 8 + 2 x 44 B)."""
+def batched_bench(G, dev, nchains=256, ntraj=2, warmup=1, tune=True, precision=None, layout=None, world=1):
+    """The batched ensemble: nchains chains per GPU with L uniform in {8, 12, 16,
+    24, 32, 48} (seeded), beta_s on a uniform grid over [0.5, 1.2], LFMN2VF 8 x
+    eps 0.08, every solve mixed precision to 1e-10 (true relative residual),
+    device Philox draws, one persistent kernel per MD step replayed as a CUDA
+    graph.  On N GPUs the N x nchains chains are spread over the ranks by
+    gn_shard (each rank its own ensemble; no exchange), so the work per GPU
+    stays fixed.  Timed with CUDA events on each rank's ensemble stream over
+    `ntraj` trajectories of every chain after `warmup`, the slowest rank's
+    time.  Algorithmic bytes: 96 per site per pair of solver iterations (the
+    two flavours' FP32 sweeps, 8 + 2 x 44 B)."""
     import torch
+
+    import gn_shard
     prec = G.GN_PREC_MIXED if precision is None else precision
+    ntot = nchains * world
     rng = np.random.default_rng(4242)
-    Ls = [int(x) for x in rng.choice([8, 12, 16, 24, 32, 48], size=nchains)]
-    betas = list(np.linspace(0.5, 1.2, nchains))
+    Ls = [int(x) for x in rng.choice([8, 12, 16, 24, 32, 48], size=ntot)]
+    betas = list(np.linspace(0.5, 1.2, ntot))
     p = G.Ensemble.params(0.08, 8, precision=prec)
-    with G.Ensemble(Ls, betas, seed=1231) as e:
-        for c, (L, b) in enumerate(zip(Ls, betas)):
-            e.load_sigma(c, rng.normal(0.0, np.sqrt(2.0 / (NFLAV * b)), L ** 3))
+    with gn_shard.ShardedEnsemble(Ls, betas, seed=1231, device=dev.index) as e:
+        for c in e.mine:
+            e.load_sigma(c, np.random.default_rng([4242, c]).normal(0.0, np.sqrt(2.0 / (NFLAV * betas[c])),
+                                                                    Ls[c] ** 3))
         if layout is not None:
             e.set_layout(*layout)
         else:
             layout = e.tune(p) if tune else (1, 0)
         e.run(p, warmup)
         e.stats(reset=True)
-        st = torch.cuda.ExternalStream(e.stream, device=dev)
+        st = torch.cuda.ExternalStream(e.ens.stream, device=dev)
         e0, e1 = cuda_events()
+        torch.cuda.synchronize(dev)
+        dist_barrier(world)
         e0.record(st)
         e.run(p, ntraj)
         e1.record(st)
         e1.synchronize()
-        ms = e0.elapsed_time(e1)
+        ms = dist_max(e0.elapsed_time(e1), world, dev)
         stats = e.stats()
-        info = e.info()
+        info = e.ens.info()
     sites = sum(L ** 3 for L in Ls)
     iters = sum(s["cg_iterations"] for s in stats)
-    acc = sum(s["accepted"] for s in stats) / (nchains * ntraj)
+    acc = sum(s["accepted"] for s in stats) / (ntot * ntraj)
     nbytes = sum(L ** 3 * s["cg_iterations"] / 2 * 96 for L, s in zip(Ls, stats))
-    return {"metric": "chain trajectories/s, 256 chains L in {8..48}, LFMN2VF 8 x eps 0.08, CG to 1e-10",
-            "precision": "mixed" if prec == G.GN_PREC_MIXED else "fp64",
-            "value": nchains * ntraj / (ms / 1e3), "unit": "traj/s",
+    return {"metric": f"chain trajectories/s, {nchains} chains per GPU L in {{8..48}}, LFMN2VF 8 x eps 0.08, "
+                      "CG to 1e-10",
+            "precision": "mixed" if prec == G.GN_PREC_MIXED else "fp64", "n_gpus": world,
+            "value": ntot * ntraj / (ms / 1e3), "unit": "traj/s",
             "site_trajectories_per_s": sites * ntraj / (ms / 1e3), "ms_per_ensemble_trajectory": ms / ntraj,
-            "chains": nchains, "sites": sites, "acceptance": acc,
-            "cg_iterations_per_chain_trajectory": iters / (nchains * ntraj),
-            "solver_gbs": nbytes / (ms / 1e3) / 1e9,
+            "chains": ntot, "sites": sites, "acceptance": acc,
+            "cg_iterations_per_chain_trajectory": iters / (ntot * ntraj),
+            "solver_gbs": nbytes / (ms / 1e3) / 1e9 / world,
             "layout": {"group_blocks": layout[0], "big_min_volume": layout[1]},
             "graph": info["graph"], "launches_per_trajectory": info["launches_per_trajectory"] + 2}
 

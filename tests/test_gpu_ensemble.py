@@ -13,6 +13,8 @@ with device Philox random numbers.
 - A chain's trajectory does not depend on the chains beside it: the same chain
   alone and in a mixed ensemble ends bit for bit the same, with and without
   the CUDA graph.
+- Chains spread over shards (gn_shard, one rank's chains per shard) end bit
+  for bit as they do in one ensemble.
 - The autotuner returns a layout and the benchmark's mix of sizes runs.
 """
 import json
@@ -54,6 +56,35 @@ def test_chain_alone_equals_chain_in_mix():
                 assert e.info()["graph"] == 1
         assert np.array_equal(mixed, alone)
         assert st["accepted"] == st_alone["accepted"] and st["sum_dH"] == st_alone["sum_dH"]
+
+
+def test_shards_equal_the_whole_ensemble():
+    """The chains split over two shards, run one after the other on this GPU
+    as two ranks would run them on two, end as the same chains do in one
+    ensemble: each shard keys its chains by their global indices."""
+    import gn_b200 as G
+    import gn_shard as S
+    p = G.Ensemble.params(0.08, 8)
+    Ls = [8, 16, 12, 24, 8, 12, 16]
+    betas = [0.6, 1.0, 0.85, 0.7, 1.1, 0.9, 0.75]
+    sig = [_sigma0(L, b, 20 + c) for c, (L, b) in enumerate(zip(Ls, betas))]
+
+    def run(rank, world):
+        with S.ShardedEnsemble(Ls, betas, seed=99, rank=rank, world=world) as e:
+            for c in range(len(Ls)):
+                e.load_sigma(c, sig[c])
+            e.run(p, 3)
+            return e.mine, {c: e.store_sigma(c)[0] for c in e.mine}, e.stats()
+
+    _, whole, st_whole = run(0, 1)
+    seen = []
+    for r in range(2):
+        mine, part, st = run(r, 2)
+        seen += mine
+        for c in mine:
+            assert np.array_equal(part[c], whole[c]), c
+            assert st[c]["accepted"] == st_whole[c]["accepted"] and st[c]["sum_dH"] == st_whole[c]["sum_dH"]
+    assert sorted(seen) == list(range(len(Ls)))
 
 
 @pytest.mark.parametrize("L0", [8, 12, 16])
@@ -147,6 +178,32 @@ def test_fp64_and_mixed_chains_agree(Ls):
     for a, b in zip(out[G.GN_PREC_FP64][0], out[G.GN_PREC_MIXED][0]):
         assert np.max(np.abs(a - b)) / np.max(np.abs(a)) < 1e-7
     assert np.allclose(out[G.GN_PREC_FP64][1], out[G.GN_PREC_MIXED][1], rtol=0, atol=1e-6)
+
+
+def test_two_teams_and_lock_step_chains_agree(monkeypatch):
+    """A chain's two flavours solved as two teams of half blocks (the
+    default) and in lock step on the whole team (GN_ENS_DUO=0): the same
+    trajectories to the solver tolerance, on single-block teams (L = 8, 12)
+    and on a team of several blocks (L = 24)."""
+    import gn_b200 as G
+    Ls, betas = [8, 12, 24], [0.7, 0.9, 1.1]
+    p = G.Ensemble.params(0.08, 8)
+    out = {}
+    for duo in ("1", "0"):
+        monkeypatch.setenv("GN_ENS_DUO", duo)
+        with G.Ensemble(Ls, betas, seed=4) as e:
+            e.set_layout(4, 16 ** 3)
+            for c, (L, b) in enumerate(zip(Ls, betas)):
+                e.load_sigma(c, _sigma0(L, b, 80 + c))
+            e.run(p, 2)
+            st = e.stats()
+            assert all(s["failed"] == 0 for s in st)
+            out[duo] = ([e.store_sigma(c)[0] for c in range(3)], [s["sum_dH"] for s in st],
+                        [s["accepted"] for s in st])
+    for a, b in zip(out["1"][0], out["0"][0]):
+        assert np.max(np.abs(a - b)) / np.max(np.abs(a)) < 1e-7
+    assert np.allclose(out["1"][1], out["0"][1], rtol=0, atol=1e-6)
+    assert out["1"][2] == out["0"][2]
 
 
 def test_checkpoint_resume_is_exact(tmp_path):

@@ -232,3 +232,30 @@ def test_odd_half_rows_force_trajectory_mixed(lattices, port, L):
     for k in range(2):
         r2 = b[k] - port.dirac(L, sm, port.dirac(L, sm, xm[k], 1), 0)
         assert np.linalg.norm(r2) < 1e-10 * np.linalg.norm(b[k]) * 1.01
+
+
+@pytest.mark.parametrize("L", [16, 64])
+def test_two_teams_and_lock_step_agree(port, monkeypatch, L):
+    """The mixed solver's two flavours as two teams of half blocks (the
+    default) and in lock step on all threads (GN_MIXED_DUO=0, read when a
+    context is created): each system is the same CG, only the grouping of the
+    partial sums differs, so both meet the FP64 stopping rule on the true
+    residual with iteration counts within two of each other."""
+    import gn_b200 as G
+    rng = np.random.default_rng(600 + L)
+    V = L ** 3
+    sm = port.sigma_mass(L, rng.normal(0, 0.77, V))
+    b = np.stack([port.dirac(L, sm, rng.normal(size=V), 0) for _ in range(2)])
+    out = {}
+    for duo in ("1", "0"):
+        monkeypatch.setenv("GN_MIXED_DUO", duo)
+        with G.Lattice(L) as lat:
+            out[duo] = lat.cg(sm, b, None, 1e-10, variant=1, relative=True, precision=G.GN_PREC_MIXED)
+    for duo, (x, info, st) in out.items():
+        assert st == 0, duo
+        for k in range(2):
+            r = b[k] - port.dirac(L, sm, port.dirac(L, sm, x[k], 1), 0)
+            assert np.linalg.norm(r) < 1e-10 * np.linalg.norm(b[k]) * 1.01, (duo, k)
+    for k in range(2):
+        assert abs(out["1"][1][k]["iterations"] - out["0"][1][k]["iterations"]) <= 2
+        assert rel(out["1"][0][k], out["0"][0][k]) < 1e-8

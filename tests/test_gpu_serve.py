@@ -2,7 +2,8 @@
 and condensate requests on resident chains.
 
 - A request's result does not depend on the requests beside it: the same
-  chain's requests give the same bits alone and inside a mixed load.
+  chain's requests give the same bits alone and inside a mixed load, and on
+  one server or on the shard (gn_shard) that owns its chain.
 - A solve request solves (M M^T) x = b for its b ~ N(0, 1): b regenerated on
   the host from the same Philox counters gives a true relative residual
   below 1e-9 with the CPU restatement's operator.
@@ -96,6 +97,50 @@ def test_request_alone_equals_request_in_mix():
     assert np.array_equal(mixed["x"], alone["x"])
     assert mixed["cond"] == alone["cond"]
     assert np.array_equal(mixed["sigma"], alone["sigma"])
+
+
+def test_sharded_server_equals_one_server():
+    """The same request stream on one server and on two shards (run one after
+    the other on this GPU, as two ranks would on two): every request ends
+    with the same bits on the shard that owns its chain."""
+    import gn_b200 as G
+    import gn_shard as S
+    Ls = [8, 24, 16, 12, 32, 16]
+    rng = np.random.default_rng(13)
+    betas = [float(b) for b in rng.uniform(0.6, 1.1, len(Ls))]
+    kinds = [(G.GN_REQ_TRAJECTORY, 0), (G.GN_REQ_SOLVE, 0), (G.GN_REQ_CONDENSATE, 8)]
+    stream = [(int(c), kinds[int(k)]) for c, k in zip(rng.integers(0, len(Ls), 18), rng.integers(0, 3, 18))]
+
+    def serve(rank, world):
+        with S.ShardedServer(G.Ensemble.params(0.08, 8), seed=SEED, rank=rank, world=world) as s:
+            for c, (L, b) in enumerate(zip(Ls, betas)):
+                s.add_chain(L, b, _sigma0(L, b, 200 + c))
+            rids = []
+            for k, (c, (t, nv)) in enumerate(stream):
+                rids.append(s.submit(c, t, nv))
+                if k % 4 == 3:
+                    s.step()
+            s.drain()
+            recs = s.gather_requests(rids)
+            sol = {r: s.solution(r) for r in recs if recs[r]["type"] == G.GN_REQ_SOLVE}
+            sig = {c: s.chain_sigma(c) for c in range(len(Ls)) if c in s.chain_local}
+            return recs, sol, sig
+
+    whole, wsol, wsig = serve(0, 1)
+    assert len(whole) == len(stream) and all(r["status"] == 2 and r["failed"] == 0 for r in whole.values())
+    got = {}
+    for r in range(2):
+        recs, sol, sig = serve(r, 2)
+        got.update(recs)
+        for rid, rec in recs.items():
+            w = whole[rid]
+            assert rec["chain"] == w["chain"] and rec["type"] == w["type"]
+            assert (rec["dH"], rec["accepted"], rec["value"]) == (w["dH"], w["accepted"], w["value"]), rid
+        for rid, x in sol.items():
+            assert np.array_equal(x, wsol[rid])
+        for c, sg in sig.items():
+            assert np.array_equal(sg, wsig[c])
+    assert sorted(got) == sorted(whole)
 
 
 def test_solve_request_residual(port):
