@@ -102,6 +102,11 @@ class Server {
   double tol_ = 1e-10;
   int precision_ = GN_PREC_MIXED;
   cudaStream_t stream_ = nullptr;
+  // the requests' work arrays come from a pool of the server's own that keeps
+  // its memory mapped up to the budget: the device's default pool returns
+  // freed memory at every synchronisation, and mapping it again on the next
+  // admission took up to 0.8 s on B200, stalling every request behind it
+  cudaMemPool_t pool_ = nullptr;
   std::chrono::steady_clock::time_point t0_;
   std::vector<Chain> chains_;
   EnsState *d_states_ = nullptr;  // [kMaxChains]
@@ -147,6 +152,15 @@ Server::Server(const gn_ens_params &traj, size_t budget, unsigned long long seed
   check(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
   if (prop.major != 10) throw GnError(GN_ERR_NO_DEVICE, "this library is built for sm_100a (B200) only");
   check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  cudaMemPoolProps props;
+  memset(&props, 0, sizeof props);
+  props.allocType = cudaMemAllocationTypePinned;
+  props.handleTypes = cudaMemHandleTypeNone;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  check(cudaMemPoolCreate(&pool_, &props), "cudaMemPoolCreate");
+  uint64_t keep = uint64_t(budget_);
+  check(cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep), "pool release threshold");
   capacity_ = coop_capacity((const void *)ens_node_kernel, kEnsThreads);
   if (capacity_ < 1) throw GnError(GN_ERR_CUDA, "the batched kernel cannot be resident as a cooperative grid");
   // team tiers: sizes > 1, decreasing, each dividing the previous one (so a
@@ -258,6 +272,7 @@ Server::~Server() {
   cudaFree(d_partials_);
   cudaFree(d_cg_state_);
   cudaFree(d_err_);
+  if (pool_) cudaMemPoolDestroy(pool_);
   cudaStreamDestroy(stream_);
 }
 
@@ -378,7 +393,7 @@ void Server::admit() {
       ++it;
       continue;
     }
-    check(cudaMallocAsync(&r.work, r.bytes, stream_), "cudaMallocAsync work");
+    check(cudaMallocFromPoolAsync(&r.work, r.bytes, pool_, stream_), "cudaMallocFromPoolAsync work");
     in_use_ += r.bytes;
     c.busy = true;
     // the request's serial number on its chain (its Philox counter) and a zero accumulator

@@ -718,7 +718,7 @@ def serve_standalone(G, precision=None, seed=5):
     return out
 
 
-def serve_sweep(G, rates=(25.0, 50.0, 100.0, 150.0, 200.0), nreq=600):
+def serve_sweep(G, rates=(25.0, 50.0, 75.0, 100.0, 150.0, 200.0), nreq=600):
     """serve_bench at a ladder of offered rates in mixed precision, and at 50/s
     and 200/s in FP64.  max_sustained_req_s: the highest offered rate whose
     completion rate (requests over first arrival to last completion) stays
