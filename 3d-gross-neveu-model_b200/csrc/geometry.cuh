@@ -126,4 +126,22 @@ __host__ __device__ __forceinline__ uint32_t site_index(const Geom &g, int c0, i
   return par * uint32_t(g.half) + (uint32_t(c0) * L + uint32_t(c1)) * uint32_t(g.Lh) + uint32_t(c2 >> 1);
 }
 
+// Index of the corner x + S*(d0, d1, d2) of a cube, d in {0, 1}^3 and S = +1
+// or -1, for 0 <= x < L: each coordinate wraps with one compare instead of
+// site_index's three divisions (the 8-corner gathers: the sigma mass takes
+// S = -1, the sigma force S = +1).  Equal to site_index for these offsets.
+template <int S>
+__host__ __device__ __forceinline__ uint32_t corner_index(const Geom &g, uint32_t x0, uint32_t x1, uint32_t x2,
+                                                          int d0, int d1, int d2) {
+  const uint32_t L = uint32_t(g.L);
+  auto step = [L](uint32_t x, int d) -> uint32_t {
+    if (d == 0) return x;
+    if constexpr (S > 0) return x + 1u == L ? 0u : x + 1u;
+    else return x == 0u ? L - 1u : x - 1u;
+  };
+  const uint32_t c0 = step(x0, d0), c1 = step(x1, d1), c2 = step(x2, d2);
+  const uint32_t par = (c0 + c1 + c2) & 1u;
+  return par * uint32_t(g.half) + (c0 * L + c1) * uint32_t(g.Lh) + (c2 >> 1);
+}
+
 }  // namespace gn

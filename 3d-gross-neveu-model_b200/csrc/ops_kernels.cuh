@@ -69,7 +69,7 @@ __device__ __forceinline__ void sigma_mass_site(const Geom &g, uint32_t i, const
   T s = T(0);
 #pragma unroll
   for (int c = 0; c < 8; c++) {
-    const uint32_t j = site_index(g, int(x0) - off[c][0], int(x1) - off[c][1], int(x2) - off[c][2]);
+    const uint32_t j = corner_index<-1>(g, x0, x1, x2, off[c][0], off[c][1], off[c][2]);
     T v = ld_site<RO>(sigma_in + j);
     if (P != nullptr) v = v + eps * ld_site<RO>(P + j);
     s = (c == 0) ? v : s + v;
@@ -112,7 +112,7 @@ __device__ __forceinline__ void force_site(const Geom &g, uint32_t i, const T *_
   site_coords(g, i, x0, x1, x2, par, row, k);
   uint32_t cj[8];
 #pragma unroll
-  for (int c = 0; c < 8; c++) cj[c] = site_index(g, int(x0) + off[c][0], int(x1) + off[c][1], int(x2) + off[c][2]);
+  for (int c = 0; c < 8; c++) cj[c] = corner_index<1>(g, x0, x1, x2, off[c][0], off[c][1], off[c][2]);
   T f = T(0);
 #pragma unroll
   for (int fl = 0; fl < 2; fl++) {
@@ -290,7 +290,7 @@ __global__ void __launch_bounds__(kOpThreads) force_cm_kernel(Geom g, const doub
     site_coords(g, i, x0, x1, x2, par, row, k);
     uint32_t cj[8];
 #pragma unroll
-    for (int c = 0; c < 8; c++) cj[c] = site_index(g, int(x0) + off[c][0], int(x1) + off[c][1], int(x2) + off[c][2]);
+    for (int c = 0; c < 8; c++) cj[c] = corner_index<1>(g, x0, x1, x2, off[c][0], off[c][1], off[c][2]);
     double f = 0.0;
 #pragma unroll
     for (int fl = 0; fl < 2; fl++) {

@@ -57,7 +57,7 @@ BETA_S = 0.85
 NFLAV = 4
 # DRAM bytes per launch measured with ncu (one capture each; summaries under
 # profiles/): the dominant solver kernel at L = 64 and the Dirac apply at L = 256.
-CG_MIXED_DRAM_BYTES = 7_031_296      # 6.450 MB read + 0.581 MB written (cg_mixed_duo_kernel)
+CG_MIXED_DRAM_BYTES = 6_790_400      # 6.449 MB read + 0.342 MB written (cg_mixed_duo_kernel)
 DIRAC256_DRAM_BYTES = 379_232_256    # 269.540 MB read + 109.692 MB written
 METRIC = "HMC trajectories/s at L=64 (LFMN2VF, 10 x eps 0.05, CG to 1e-10 true relative residual)"
 UNIT = "traj/s"
