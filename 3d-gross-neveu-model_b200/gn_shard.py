@@ -230,10 +230,14 @@ class ShardedServer:
         return self.balancer.owner
 
     def add_chain(self, L, beta_s, sigma, stream_id=None):
-        """Global chain index; the chain's Philox stream defaults to it."""
+        """Global chain index; the chain's Philox stream defaults to it.
+        sigma may be a callable returning the field, called on the owner only
+        (the other ranks need not build it)."""
         c = len(self.balancer.owner)
         r = self.balancer.add(L)
         if r == self.rank:
+            if callable(sigma):
+                sigma = sigma()
             lc = self.srv.add_chain(L, beta_s, sigma, c if stream_id is None else stream_id)
             self.chain_local[c] = lc
             self.chain_global[lc] = c

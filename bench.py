@@ -77,8 +77,8 @@ def parse():
     ap.add_argument("--no-l128", action="store_true", help="skip the L = 128 mixed-precision case")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving sweep")
     ap.add_argument("--detail", default=None, help="write every side measurement to this JSON file")
-    ap.add_argument("--case", choices=["cg64", "dirac128", "dirac256", "traj64", "batched", "serve", "l128", "u1",
-                                       "ens", "kernels"],
+    ap.add_argument("--case", choices=["cg64", "dirac128", "dirac256", "traj64", "batched", "serve", "serve_sharded",
+                                       "l128", "u1", "ens", "kernels"],
                     default=None, help="run one small case for a profiler instead of the benchmark")
     return ap.parse_args()
 
@@ -449,6 +449,8 @@ def run_ours(a, world, rank, local):
         detail["u1"] = u1_case(G, dev)
         if not a.no_serve:
             detail["serving"] = serve_sweep(G)
+    elif not a.no_serve:
+        detail["serving_sharded"] = serve_sharded_bench(G, world, dev)
     cpu = None
     if cpu_job is not None:
         cpu = cpu_line_fields(cpu_job.result(), a)
@@ -505,6 +507,11 @@ def summaries(d, peaks):
                           "mixed": [[r["offered_req_per_s"], round(r["throughput_req_per_s"], 1), round(r["p50_ms"]),
                                      round(r["p99_ms"])] for r in s["mixed"]],
                           "cols": "offered/s, done/s, p50 ms, p99 ms"}
+    if "serving_sharded" in d:
+        s = d["serving_sharded"]
+        out["serving"] = {"n_gpus": s["n_gpus"], "offered_req_per_s": s["offered_req_per_s"],
+                          "done_req_per_s": round(s["throughput_req_per_s"], 1), "p50_ms": round(s["p50_ms"]),
+                          "p99_ms": round(s["p99_ms"])}
     if "l128" in d:
         out["l128"] = [{k: (round(v, 3) if k in ("beta_s", "solve_speedup", "trajectory_speedup") else
                             float(f"{v:.2e}")) for k, v in r.items()
@@ -691,6 +698,61 @@ def serve_bench(G, nreq=600, rate=200.0, warm=24, seed=5, precision=None, tiers=
     out["slowest"] = [[Ls[r["chain"]], int(r["type"]), round((r["t_admit"] - r["t_arrival"]) * 1e3, 1),
                        round((r["t_done"] - r["t_admit"]) * 1e3, 1)] for r in slow]
     return out
+
+
+def serve_sharded_bench(G, world, dev=None, rate_per_gpu=100.0, nreq_per_gpu=300, seed=5):
+    """Serving on N GPUs (gn_shard.ShardedServer): 256 chains per GPU (32 per
+    L in 8, 16, ..., 64, beta_s uniform in [0.6, 1.1]) spread over the ranks by
+    the online balancer, and one Poisson stream at N x rate_per_gpu requests/s
+    of serve_bench's mix, replicated on every rank; each rank serves the
+    requests on its own chains.  Latency as in serve_bench, on each rank's own
+    clock; throughput = all requests over the longest rank's span from the
+    first arrival to its last completion.  The records are gathered after the
+    run (host objects); nothing crosses between GPUs while it runs."""
+    import gn_shard
+    rng = np.random.default_rng(seed)
+    Ls = [L for L in range(8, 65, 8) for _ in range(32 * world)]
+    betas = rng.uniform(0.6, 1.1, len(Ls))
+    types = (G.GN_REQ_TRAJECTORY, G.GN_REQ_SOLVE, G.GN_REQ_CONDENSATE)
+    nreq, rate = nreq_per_gpu * world, rate_per_gpu * world
+    with gn_shard.ShardedServer(G.Ensemble.params(0.08, 8), mem_budget_bytes=32e9, seed=seed,
+                                device=int(os.environ.get("LOCAL_RANK", "0")), server_factory=G.Server) as srv:
+        for c, (L, b) in enumerate(zip(Ls, betas)):
+            srv.add_chain(L, b, lambda L=L, b=b, c=c: np.random.default_rng([seed, c]).normal(
+                0.0, np.sqrt(2.0 / (NFLAV * b)), L ** 3))
+        gaps = rng.exponential(1.0 / rate, nreq)
+        kinds = rng.choice(3, size=nreq, p=[0.7, 0.2, 0.1])
+        chains = rng.integers(len(Ls), size=nreq)
+        dist_barrier(world)
+        t0 = srv.clock() + 0.01
+        arrive = t0 + np.cumsum(gaps)
+        ids, nxt = [], 0
+        while True:
+            now = srv.clock()
+            while nxt < nreq and arrive[nxt] <= now:
+                t = types[kinds[nxt]]
+                ids.append(srv.submit(int(chains[nxt]), t, 16 if t == G.GN_REQ_CONDENSATE else 0, arrive[nxt]))
+                nxt += 1
+            ld = srv.load()
+            if ld["running"] == 0 and ld["queued"] == 0:
+                if nxt == nreq:
+                    break
+                time.sleep(max(0.0, arrive[nxt] - srv.clock()))
+                continue
+            srv.step()
+        mine = [srv.request(i) for i in ids if i in srv.req_local]
+        span = (max(r["t_done"] for r in mine) - arrive[0]) if mine else 0.0
+        recs = srv.gather_requests(ids)
+        per_rank = [0] * world
+        for r in recs.values():
+            per_rank[srv.owner[r["chain"]]] += 1
+    span = dist_max(span, world, dev)
+    lat = np.array([r["t_done"] - r["t_arrival"] for r in recs.values()])
+    return {"metric": f"serving on {world} GPU(s): Poisson {rate:g}/s, {len(Ls)} chains, serve_bench's mix",
+            "n_gpus": world, "offered_req_per_s": rate, "requests": nreq,
+            "throughput_req_per_s": nreq / span, "p50_ms": float(np.percentile(lat, 50) * 1e3),
+            "p99_ms": float(np.percentile(lat, 99) * 1e3), "failed": int(sum(r["failed"] for r in recs.values())),
+            "requests_per_rank": per_rank}
 
 
 def serve_standalone(G, precision=None, seed=5):
@@ -1075,6 +1137,9 @@ def run_case(a):
         return
     if a.case == "serve":
         print(json.dumps(serve_sweep(G)), flush=True)
+        return
+    if a.case == "serve_sharded":
+        print(json.dumps(serve_sharded_bench(G, 1)), flush=True)
         return
     L, V = 64, 64 ** 3
     lat = G.Lattice(L, 0)

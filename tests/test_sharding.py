@@ -157,3 +157,76 @@ def test_explicit_shard_without_a_group():
     assert [s is None for s in st] == [c not in mine for c in range(3)]
     obs = e.observables()
     assert np.isnan(obs[[c for c in range(3) if c not in mine]]).all()
+
+
+class ClockServer:
+    """A server stand-in with a host clock: a step completes every running
+    request and admits the queued ones."""
+
+    def __init__(self, traj_params, mem_budget_bytes, seed, device, **kw):
+        import time
+        self.t0 = time.perf_counter()
+        self.chains, self.reqs, self.queue, self.running = [], [], [], []
+
+    def clock(self):
+        import time
+        return time.perf_counter() - self.t0
+
+    def add_chain(self, L, beta_s, sigma, stream_id):
+        assert np.asarray(sigma).size == L ** 3  # built on the owner only
+        self.chains.append(L)
+        return len(self.chains) - 1
+
+    def submit(self, chain, rtype, noise_vectors, t_arrival):
+        self.reqs.append({"chain": chain, "type": rtype, "t_arrival": t_arrival, "t_done": None, "failed": 0})
+        self.queue.append(len(self.reqs) - 1)
+        return len(self.reqs) - 1
+
+    def load(self):
+        return {"running": len(self.running), "queued": len(self.queue), "bytes_in_use": 0}
+
+    def step(self):
+        for r in self.running:
+            self.reqs[r]["t_done"] = self.clock()
+        self.running, self.queue = self.queue, []
+        return 0
+
+    def request(self, rid):
+        return dict(self.reqs[rid])
+
+    def close(self):
+        pass
+
+
+def _fake_gn():
+    import types
+    G = types.SimpleNamespace(GN_REQ_TRAJECTORY=0, GN_REQ_SOLVE=1, GN_REQ_CONDENSATE=2, Server=ClockServer)
+    G.Ensemble = types.SimpleNamespace(params=lambda eps, steps: (eps, steps))
+    return G
+
+
+def _serve_rank(rank, port, out_dir):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE="2", RANK=str(rank),
+                      LOCAL_RANK="0")
+    sys.path.insert(0, str(ROOT))
+    import torch.distributed as dist
+
+    import bench
+    world, r, _ = bench.dist_setup("gloo")
+    out = bench.serve_sharded_bench(_fake_gn(), world, rate_per_gpu=400.0, nreq_per_gpu=200)
+    (Path(out_dir) / f"serve{r}.json").write_text(json.dumps(out))
+    dist.destroy_process_group()
+
+
+def test_sharded_serving_bench_gloo(tmp_path):
+    """bench.py's serving on N GPUs, as two gloo ranks with a clock-only
+    server: every request is served once, on its chain's owner, and both
+    ranks report the same gathered figures."""
+    import torch.multiprocessing as mp
+    mp.spawn(_serve_rank, args=(free_port(), str(tmp_path)), nprocs=2, join=True)
+    got = [json.loads((tmp_path / f"serve{r}.json").read_text()) for r in range(2)]
+    for g in got:
+        assert g["n_gpus"] == 2 and g["requests"] == 400 and g["failed"] == 0
+        assert sum(g["requests_per_rank"]) == 400 and min(g["requests_per_rank"]) > 0
+        assert g["throughput_req_per_s"] > 0 and g["p99_ms"] >= g["p50_ms"] >= 0
+    assert got[0] == got[1]
