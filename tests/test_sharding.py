@@ -4,7 +4,8 @@ The batched chains and the server shard with no exchange on the data path:
 every rank computes the same owner map and keeps its own chains; the ranks
 meet only to gather host-side results.  These tests check the owner maps and
 run that logic as two gloo processes, with stand-ins for the GPU ensemble
-and server that record what each rank was given.
+and server that record what each rank was given; and bench.py's serving on
+N GPUs the same way, with a server that only keeps time.
 """
 import json
 import os
