@@ -383,7 +383,8 @@ int gn_cg_u1(gn_context *ctx, const double *sigmamass, const double *pimass, con
   if (!sigmamass || !pimass || !b || !x) return fail(GN_ERR_ARG, "null pointer");
   if (nrhs < 1 || nrhs > 2) return fail(GN_ERR_ARG, "nrhs must be 1 or 2");
   if (variant < 0 || variant > 1) return fail(GN_ERR_ARG, "bad variant");
-  if (precision != GN_PREC_FP64 && precision != GN_PREC_MIXED) return fail(GN_ERR_ARG, "precision: FP64 or MIXED");
+  if (precision != GN_PREC_FP64 && precision != GN_PREC_MIXED && precision != GN_PREC_FP64_EXACT)
+    return fail(GN_ERR_ARG, "unknown precision");
   return guarded(ctx, [&](gn::Engine &E) {
     const size_t V = size_t(E.V());
     double *d_sm = ctx->io, *d_pm = d_sm + V, *d_b = d_pm + V, *d_x = d_b + 4 * V;
@@ -419,7 +420,8 @@ static int force_u1(gn_context *ctx, bool pi, double beta_s, const double *field
     const double *bs[2] = {d_phi, d_phi + 2 * V};
     double *xs[2] = {d_X, d_X + 2 * V};
     gn::SolveInfo si[2];
-    const int st = E.solve_cm(d_sm, d_pm, bs, xs, 2, tol, 0, 0, 0, si);
+    // parity mode (gn_set_parity_mode): the exact-order solver and M^dagger
+    const int st = E.solve_cm(d_sm, d_pm, bs, xs, 2, tol, 0, 0, 0, si, E.exact ? GN_PREC_FP64_EXACT : GN_PREC_FP64);
     if (st == GN_OK) {
       E.dirac_cm(d_sm, d_pm, d_X, d_Y, 2, GN_OP_MT);
       // (NFLAV * beta_scalar / 4.0) for pi (moleculardynamics.c:685), / 2.0 for sigma (:580)

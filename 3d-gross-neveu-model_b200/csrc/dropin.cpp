@@ -413,12 +413,6 @@ void GNB200_SetTolerances(double medium, double high) {
   g_tol_high = high;
 }
 void GNB200_SetPrecision(int precision) {
-#ifdef GN_DROPIN_PI
-  if (precision != GN_PREC_FP64 && precision != GN_PREC_MIXED) {
-    fprintf(stderr, "gn_dropin_pi: the U(1) model runs in GN_PREC_FP64 or GN_PREC_MIXED\n");
-    exit(2);
-  }
-#endif
   g_precision = precision;
   // the operators without a precision argument follow the exact mode too
   if (gn_set_parity_mode(ctx(), precision == GN_PREC_FP64_EXACT) != GN_OK) fatal("gn_set_parity_mode");

@@ -336,11 +336,7 @@ int Engine::trajectory(const gn_hmc_params &hp, double (*gauss)(void), double (*
   if (u1_) return trajectory_u1(hp, gauss, uniform, pre_P, pre_chi, res);
   const size_t V = size_t(V_);
   memset(res, 0, sizeof *res);
-  struct ExactScope {  // parity mode for the trajectory's operators, restored on every exit
-    bool &flag, saved;
-    ExactScope(bool &f, bool on) : flag(f), saved(f) { flag = flag || on; }
-    ~ExactScope() { flag = saved; }
-  } exact_scope(exact, hp.precision == GN_PREC_FP64_EXACT);
+  ExactScope exact_scope(exact, hp.precision == GN_PREC_FP64_EXACT);
   // draws: P, chi_0, chi_1 (moleculardynamics.c:1240-1247), uploaded in one copy
   if (gauss != nullptr) {
     double *h = h_stage_;
@@ -514,11 +510,7 @@ int Engine::evolve_in_time(const gn_hmc_params &hp, gn_traj_result *res) {
   if (u1_) throw GnError(GN_ERR_ARG, "the MD helpers are built for the Z2 model only");
   const size_t V = size_t(V_);
   memset(res, 0, sizeof *res);
-  struct ExactScope {
-    bool &flag, saved;
-    ExactScope(bool &f, bool on) : flag(f), saved(f) { flag = flag || on; }
-    ~ExactScope() { flag = saved; }
-  } exact_scope(exact, hp.precision == GN_PREC_FP64_EXACT);
+  ExactScope exact_scope(exact, hp.precision == GN_PREC_FP64_EXACT);
   const double *phis[2] = {phi_, phi_ + V};
   double *Xs[2] = {X_, X_ + V};
   SolveInfo info[2];
@@ -573,12 +565,7 @@ int Engine::condensate(const double *sm, double tol, double *target, double *D, 
                        double out[11], double *iterations, long long *calls, int precision) {
   TraceRange tr("gn condensate");
   const size_t V = size_t(V_);
-  if (u1_ && precision == GN_PREC_FP64_EXACT) throw GnError(GN_ERR_ARG, "the U(1) model has no exact-order mode");
-  struct ExactScope {
-    bool &flag, saved;
-    ExactScope(bool &f, bool on) : flag(f), saved(f) { flag = flag || on; }
-    ~ExactScope() { flag = saved; }
-  } exact_scope(exact, precision == GN_PREC_FP64_EXACT);
+  ExactScope exact_scope(exact, precision == GN_PREC_FP64_EXACT);
   // dot products: the compensated tree, or the reference's serial loop in parity mode
   auto dots = [&](const double *v, const double *Dv, double q[4]) {
     if (exact) {

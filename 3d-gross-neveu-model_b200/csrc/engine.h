@@ -32,6 +32,14 @@ struct SolveInfo {
   long long reliable;  // mixed precision: reliable updates
 };
 
+// Parity mode for one operation's operators (the engine's `exact` flag set
+// on entry when asked for, restored on every exit).
+struct ExactScope {
+  bool &flag, saved;
+  ExactScope(bool &f, bool on) : flag(f), saved(f) { flag = flag || on; }
+  ~ExactScope() { flag = saved; }
+};
+
 class Engine {
  public:
   Engine(int L, int device);
@@ -142,10 +150,13 @@ class Engine {
 
  private:
   int finish_solve(int nrhs, SolveInfo *info);
+  // pm: the U(1) model's pi mass (complex systems with the mass sm + i eps pm), else null
   int solve_exact(const double *sm, const double *const *b, double *const *x, int nrhs, int ncomp, double tol,
-                  int variant, int rel, long long max_iter, SolveInfo *info);
+                  int variant, int rel, long long max_iter, SolveInfo *info, const double *pm = nullptr);
   void mt_exact(const double *sm, const double *in, double *out, int ncomp);
+  void mt_exact_cm(const double *sm, const double *pm, const double *in, double *out, int nsys);
   void energy_exact(const double *P, const double *phi, const double *X, const double *sigma, double out[3]);
+  void energy_cm_exact(const double *P, const double *phi, const double *X, const double *field, double out[3]);
   void energy_launch(const double *P, const double *phi, const double *X, const double *sigma, double *dst);
   void cond_dots_exact(const double *v, const double *D, double out[4]);
   void mixed_init();

@@ -38,6 +38,10 @@ void Engine::set_u1(bool on) {
 }
 
 void Engine::dirac_cm(const double *sm, const double *pm, const double *in, double *out, int nsys, int op) {
+  if (exact && op == GN_OP_MT) {  // parity mode: the reference's scatter order
+    mt_exact_cm(sm, pm, in, out, nsys);
+    return;
+  }
   const void *ptrs[4] = {sm, pm, in, out};
   const int W = fp64_width(L_, ptrs, 4);
   const dim3 grid(unsigned((V_ / W + kOpThreads - 1) / kOpThreads), unsigned(nsys));
@@ -64,10 +68,11 @@ int Engine::solve_cm(const double *sm, const double *pm, const double *const *b,
                      double tol, int variant, int rel, long long max_iter, SolveInfo *info, int precision) {
   TraceRange tr(precision == GN_PREC_MIXED ? "gn cg u1 mixed" : "gn cg u1 fp64");
   if (nrhs < 1 || nrhs > 2) throw GnError(GN_ERR_ARG, "the U(1) solve takes 1 or 2 systems");
-  if (precision != GN_PREC_FP64 && precision != GN_PREC_MIXED)
-    throw GnError(GN_ERR_ARG, "the U(1) model solves in FP64 or mixed precision");
+  if (precision != GN_PREC_FP64 && precision != GN_PREC_MIXED && precision != GN_PREC_FP64_EXACT)
+    throw GnError(GN_ERR_ARG, "unknown precision");
   if (max_iter <= 0) max_iter = V_ + 1;  // MAX_CONJUGATE_GRADIENT_ITERATION, macro.h:134
   if (precision == GN_PREC_MIXED) return solve_mixed(sm, b, x, nrhs, 2, tol, variant, rel, max_iter, info, pm);
+  if (precision == GN_PREC_FP64_EXACT) return solve_exact(sm, b, x, nrhs, 2, tol, variant, rel, max_iter, info, pm);
   const size_t V = size_t(V_);
   CgArgs<double> a;
   memset(&a, 0, sizeof a);
@@ -122,6 +127,10 @@ void Engine::force_cm(bool pi, const double *X, const double *Y, const double *f
 }
 
 void Engine::energy_cm(const double *P, const double *phi, const double *X, const double *field, double out[3]) {
+  if (exact) {  // parity mode: the reference's serial sums
+    energy_cm_exact(P, phi, X, field, out);
+    return;
+  }
   const int nb = op_blocks(V_, num_sms_);
   energy_cm_kernel<<<nb, kOpThreads, 0, stream_>>>(uint32_t(V_), P, phi, X, field, partials_);
   check(cudaGetLastError(), "energy_cm_kernel");
@@ -155,8 +164,9 @@ void load_chi(Engine &E, const double *host_chi, const double *dev_chi) {
 int Engine::trajectory_u1(const gn_hmc_params &hp, double (*gauss)(void), double (*uniform)(void), const double *pre_P,
                           const double *pre_chi, gn_traj_result *res) {
   TraceRange tr("gn trajectory u1");
-  if (hp.precision != GN_PREC_FP64 && hp.precision != GN_PREC_MIXED)
-    throw GnError(GN_ERR_ARG, "the U(1) model runs in FP64 or mixed precision");
+  if (hp.precision != GN_PREC_FP64 && hp.precision != GN_PREC_MIXED && hp.precision != GN_PREC_FP64_EXACT)
+    throw GnError(GN_ERR_ARG, "unknown precision");
+  ExactScope exact_scope(exact, hp.precision == GN_PREC_FP64_EXACT);
   const size_t V = size_t(V_);
   memset(res, 0, sizeof *res);
   // draws: P, chi_0, chi_1 (moleculardynamics.c:1240-1247)
@@ -254,8 +264,9 @@ int Engine::trajectory_pi(const gn_hmc_params &hp, void (*gauss_pair)(double *, 
   TraceRange tr("gn trajectory pi");
   if (!u1_) throw GnError(GN_ERR_ARG, "the context is not in the U(1) model (load pi first)");
   if (hp.steps < 1) throw GnError(GN_ERR_ARG, "steps must be >= 1");
-  if (hp.precision != GN_PREC_FP64 && hp.precision != GN_PREC_MIXED)
-    throw GnError(GN_ERR_ARG, "the U(1) model runs in FP64 or mixed precision");
+  if (hp.precision != GN_PREC_FP64 && hp.precision != GN_PREC_MIXED && hp.precision != GN_PREC_FP64_EXACT)
+    throw GnError(GN_ERR_ARG, "unknown precision");
+  ExactScope exact_scope(exact, hp.precision == GN_PREC_FP64_EXACT);
   const size_t V = size_t(V_);
   memset(res, 0, sizeof *res);
   double *h = h_stage_;

@@ -55,8 +55,9 @@ enum gn_op { GN_OP_M = 0, GN_OP_MT = 1, GN_OP_SUB_M = 2 };
 /* GN_PREC_FP64: FP64, tree-ordered global sums (fast).  GN_PREC_MIXED: FP32
  * iterations with FP64 reliable updates.  GN_PREC_FP64_EXACT: FP64 in the
  * reference's exact order of operations -- serial sums, M^T in the order of
- * the reference's scatter -- reproducing its results bit for bit (real fields);
- * one block per solve, so meant for parity runs at small L. */
+ * the reference's scatter -- reproducing its results bit for bit (the Z2
+ * model's real fields and the U(1) model's complex ones); one block per
+ * solve, so meant for parity runs at small L. */
 enum gn_precision { GN_PREC_FP64 = 0, GN_PREC_MIXED = 1, GN_PREC_FP64_EXACT = 2 };
 enum gn_integrator { GN_LFMN2VF = 0, GN_LF2 = 1, GN_LFMN2 = 2 };
 
@@ -189,7 +190,10 @@ GN_API int gn_condensate_sigma_device(gn_context *ctx, const double *sigma, doub
  * M = D + sigmamass + i eps(x) pimass (dirac.c:65-69; eps = +1 on even, -1 on
  * odd sites), M^dagger = -D + sigmamass - i eps pimass.  Fermion fields are
  * complex: two planes (real, imaginary) per system; a field of both flavours
- * is four planes (flavour f: planes 2f, 2f + 1).  FP64 only.
+ * is four planes (flavour f: planes 2f, 2f + 1).  Precisions as for the Z2
+ * model; in parity mode (gn_set_parity_mode, or a call with
+ * GN_PREC_FP64_EXACT) M^dagger, the solves and the energies follow the
+ * reference's order of operations.
  *
  * gn_load_pi sets the resident pi (V doubles, fermion order; pimass =
  * ComputeFullPiMass, pi.c:44-60) and switches the context to the U(1) model:
@@ -203,9 +207,9 @@ GN_API int gn_set_u1(gn_context *ctx, int on);
 GN_API int gn_dirac_u1(gn_context *ctx, const double *sigmamass, const double *pimass, const double *in, double *out,
                        int nsys, int op);
 /* CG on M M^dagger for nrhs (1 or 2) complex systems (b, x: 2 nrhs V; x in/out),
- * variant / relative / max_iter as gn_cg; precision GN_PREC_FP64 or
+ * variant / relative / max_iter as gn_cg; precision GN_PREC_FP64,
  * GN_PREC_MIXED (FP32 inner iterations, FP64 reliable updates, the same
- * true-residual test).  info[nrhs] may be NULL. */
+ * true-residual test) or GN_PREC_FP64_EXACT.  info[nrhs] may be NULL. */
 GN_API int gn_cg_u1(gn_context *ctx, const double *sigmamass, const double *pimass, const double *b, double *x,
                     int nrhs, double tol, int variant, int relative, long long max_iter, int precision,
                     gn_cg_info *info);
@@ -214,7 +218,8 @@ GN_API int gn_cg_u1(gn_context *ctx, const double *sigmamass, const double *pima
  * from the incoming X_f (tolerance tol), Y_f = M^dagger X_f, then
  *   sigma: F = sum_f 1/8 sum_corners Re(conj X_f Y_f) - (N_f beta_s / 2) sigma
  *   pi:    F = sum_f 1/8 sum_corners Re(i eps conj X_f Y_f) - (N_f beta_s / 4) pi
- * phi, X, Y: 4V (X in/out); field = sigma or pi (V); force out (V). */
+ * phi, X, Y: 4V (X in/out); field = sigma or pi (V); force out (V).  FP64;
+ * the exact-order solver and M^dagger in parity mode. */
 GN_API int gn_sigma_force_u1(gn_context *ctx, double beta_s, const double *sigma, const double *sigmamass,
                              const double *pimass, const double *phi, double *X, double *Y, double tol, double *force,
                              gn_cg_info *info);

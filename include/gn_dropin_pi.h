@@ -15,8 +15,9 @@
  * LeapFrog2Pi draws the pi momenta in pairs from the host program's
  * Gauss2MeanVariance (random.c:129), found by name like Gauss1 and Casuale,
  * or from the function given to GNB200_SetRandomPair.  Precision:
- * GN_PREC_FP64 (default) or GN_PREC_MIXED for the integrators; the standalone
- * solves and forces run in FP64.
+ * GN_PREC_FP64 (default), GN_PREC_MIXED for the solves and the integrators
+ * (the standalone forces run in FP64), or GN_PREC_FP64_EXACT, the reference's
+ * order of operations throughout (bit for bit its PI_INTERACTION build).
  */
 #ifndef GN_DROPIN_PI_H
 #define GN_DROPIN_PI_H

@@ -11,7 +11,8 @@ tests/golden/make_golden_u1.py called them on the reference alone; each binds
 to the drop-in's GPU version.  Random numbers come from the reference's own
 Gauss1, Casuale and Gauss2MeanVariance, found by name.
 
-usage: python tests/dropin_driver_pi.py <golden U(1) .npz>
+usage: python tests/dropin_driver_pi.py <golden U(1) .npz> [exact]
+("exact" selects GN_PREC_FP64_EXACT, the reference's order of operations)
 """
 import ctypes as C
 import json
@@ -31,6 +32,8 @@ def main():
     V = L ** 3
     drop = C.CDLL(str(ROOT / "3d-gross-neveu-model_b200" / "lib" / "libgn_dropin_pi.so"), mode=C.RTLD_GLOBAL)
     drop.GNB200_SetLattice(L)
+    if len(sys.argv) > 2 and sys.argv[2] == "exact":
+        drop.GNB200_SetPrecision(2)  # GN_PREC_FP64_EXACT
     drop.GNB200_Context.restype = C.c_void_p
     core = C.CDLL(str(ROOT / "3d-gross-neveu-model_b200" / "lib" / "libgn_b200.so"))
     core.gn_launch_count.restype = C.c_longlong

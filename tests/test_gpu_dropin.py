@@ -93,23 +93,54 @@ def test_dropin_exact_mode_is_bit_identical():
     assert out["evolve_sigma"] == s_ref.tolist() and out["evolve_P"] == P_ref.tolist()
 
 
+def _cx(a):
+    return np.array(a[0]) + 1j * np.array(a[1])
+
+
+def _run_pi_driver(L, *mode):
+    from oracle import build_ref
+    if not build_ref.lib_path(L, 0, build_ref.PI_TAG).exists():
+        pytest.skip("reference PI build not present")
+    gold = GOLD / f"golden_L{L}_u1.npz"
+    r = subprocess.run([sys.executable, str(ROOT / "tests" / "dropin_driver_pi.py"), str(gold), *mode],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = [ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1]
+    return json.loads(line), dict(np.load(gold))
+
+
+@pytest.mark.parametrize("L", [4, 8])
+def test_dropin_pi_exact_mode_is_bit_identical(L):
+    """GNB200_SetPrecision(GN_PREC_FP64_EXACT) in libgn_dropin_pi.so: the
+    reference's PI harness, calling its own functions by name, gets every
+    result of its PI build bit for bit from the GPU."""
+    out, g = _run_pi_driver(L, "exact")
+    assert all(v > 0 for v in out["launches"].values()) and len(out["launches"]) == 6, out["launches"]
+    for key in ("M_psi", "Mt_psi", "sub_res", "cg_x", "cond_target", "cond_D"):
+        assert np.array_equal(_cx(out[key]), g[key]), key
+    for key in ("force_X", "piforce_Y"):
+        assert np.array_equal(np.stack([_cx(v) for v in out[key]]), g[key]), key
+    for key in ("force_F", "piforce_F", "cond_out"):
+        assert np.array_equal(np.array(out[key]), g[key]), key
+    assert out["energy_H"] == g["energy_H"] and out["energy_Hpi"] == g["energy_Hpi"]
+    assert tuple(out["cg_counters"]) == tuple(g["cg_counters"])
+    assert tuple(out["cond_counters"]) == tuple(g["cond_counters"])
+    for name in ("traj", "trajpi"):
+        assert out[f"{name}_ok"] and out[f"{name}_dH"] == float(g[f"{name}_dH"])
+        assert out[f"{name}_accepted"] == int(g[f"{name}_accepted"])
+        assert tuple(out[f"{name}_counters"]) == tuple(g[f"{name}_counters"])
+        assert np.array_equal(np.array(out[f"{name}_sigma"]), g[f"{name}_sigma"])
+        assert np.array_equal(np.array(out[f"{name}_pi"]), g[f"{name}_pi"])
+
+
 @pytest.mark.parametrize("L", [4, 8])
 def test_dropin_pi_under_reference_harness(L):
     """libgn_dropin_pi.so under the reference's PI_INTERACTION build: the
     reference's harness calls its own U(1) functions by name and gets the
     GPU's, with the reference's RNG.  Results against the fixtures the
     reference made alone, to the tolerances of tests/test_gpu_u1.py."""
-    from oracle import build_ref
-    if not build_ref.lib_path(L, 0, build_ref.PI_TAG).exists():
-        pytest.skip("reference PI build not present")
-    gold = GOLD / f"golden_L{L}_u1.npz"
-    r = subprocess.run([sys.executable, str(ROOT / "tests" / "dropin_driver_pi.py"), str(gold)], capture_output=True,
-                       text=True, timeout=600)
-    assert r.returncode == 0, r.stderr[-2000:]
-    line = [ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1]
-    out = json.loads(line)
-    g = dict(np.load(gold))
-    cx = lambda a: np.array(a[0]) + 1j * np.array(a[1])  # noqa: E731
+    out, g = _run_pi_driver(L)
+    cx = _cx
 
     def rel(a, b):
         return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)

@@ -10,7 +10,8 @@ Tolerances, as for the Z2 model (tests/test_gpu_ops.py):
   - CG solutions and forces: identical iteration counts, relative 1e-11 (the
     global sums run in a tree, which CG amplifies);
   - energies: relative 1e-13; trajectories: dH to 1e-10 absolute, the same
-    accept decision, the final fields to 1e-11.
+    accept decision, the final fields to 1e-11;
+  - in the exact-order mode (GN_PREC_FP64_EXACT) every one of these bit for bit.
 """
 import numpy as np
 import pytest
@@ -93,6 +94,70 @@ def test_u1_trajectories(golden, port, L):
         assert (r["cg_iterations"], r["cg_calls"]) == tuple(g["trajpi_counters"])
         assert rel(lat.store_pi()[0], g["trajpi_pi"]) < 1e-11
         assert np.array_equal(lat.store_sigma()[0], g["trajpi_sigma0"])  # LeapFrog2Pi leaves sigma alone
+
+
+@pytest.mark.parametrize("L", [4, 8])
+def test_u1_exact_order(golden, port, L):
+    """GN_PREC_FP64_EXACT with the complex mass (M^dagger in the order of the
+    reference's scatter, one-block solves with serial sums, serial energies):
+    M^dagger, the solve, both forces, both energies, both trajectories and the
+    condensate equal the reference's PI build bit for bit."""
+    import gn_b200 as G
+    g = golden(f"golden_L{L}_u1.npz")
+    beta, eps, steps = float(g["beta_s"]), float(g["traj_eps"]), int(g["traj_steps"])
+    EX = G.GN_PREC_FP64_EXACT
+    with G.Lattice(L) as lat:
+        lat.load_sigma(g["sigma"])
+        lat.load_pi(g["pi"])
+        sm, pm = g["sm"], g["pm"]
+        lat.set_parity_mode(True)
+        assert np.array_equal(lat.dirac_u1(sm, pm, g["psi"], G.GN_OP_MT), g["Mt_psi"])
+        x, info, st = lat.cg_u1(sm, pm, g["cg_b"], None, 1e-9, variant=1, precision=EX)
+        assert st == G.GN_OK and info[0]["iterations"] == g["cg_counters"][0]
+        assert np.array_equal(x, g["cg_x"])
+        zero = np.zeros((2, L ** 3), complex)
+        F, X, Y, infos, st = lat.sigma_force_u1(beta, g["sigma"], sm, pm, g["force_phi"], zero, 1e-9)
+        assert st == G.GN_OK
+        assert sum(i["iterations"] for i in infos if i["counted"]) == g["force_counters"][0]
+        assert np.array_equal(X, g["force_X"]) and np.array_equal(Y, g["force_Y"])
+        assert np.array_equal(F, g["force_F"])
+        F, X, Y, infos, st = lat.pi_force(beta, g["pi"], sm, pm, g["force_phi"], zero, 1e-9)
+        assert st == G.GN_OK
+        assert np.array_equal(X, g["piforce_X"]) and np.array_equal(Y, g["piforce_Y"])
+        assert np.array_equal(F, g["piforce_F"])
+        assert lat.energy_u1(0, beta, g["sigma"], g["energy_P"], g["force_phi"], g["piforce_X"]) == g["energy_H"]
+        assert lat.energy_u1(1, beta, g["pi"], g["energy_Ppi"], g["force_phi"], g["piforce_X"]) == g["energy_Hpi"]
+        lat.set_parity_mode(False)
+        # the trajectories with the reference's draws
+        lat.load_sigma(g["traj_sigma0"])
+        lat.load_pi(g["traj_pi0"])
+        gp, up = port.replay(g["traj_gauss"], g["traj_uniform"])
+        r = lat.trajectory(beta, eps, steps, gp, up, precision=EX)
+        # the fixture's dH is the reference's acceptance line, printed with %.16f
+        assert r["ok"] == 1 and float(f"{r['dH']:.16f}") == float(g["traj_dH"])
+        assert r["accepted"] == int(g["traj_accepted"])
+        assert (r["cg_iterations"], r["cg_calls"]) == tuple(g["traj_counters"])
+        assert np.array_equal(lat.store_sigma()[0], g["traj_sigma"])
+        lat.load_sigma(g["trajpi_sigma0"])
+        lat.load_pi(g["trajpi_pi0"])
+        gp, up = port.replay(g["trajpi_gauss"], g["trajpi_uniform"])
+        pairs = iter(g["trajpi_pairs"])
+
+        def pair(a, b):
+            a[0], b[0] = next(pairs)
+        r = lat.trajectory_pi(beta, eps, steps, pair, gp, up, precision=EX)
+        assert r["ok"] == 1 and float(f"{r['dH']:.16f}") == float(g["trajpi_dH"])
+        assert r["accepted"] == int(g["trajpi_accepted"])
+        assert (r["cg_iterations"], r["cg_calls"]) == tuple(g["trajpi_counters"])
+        assert np.array_equal(lat.store_pi()[0], g["trajpi_pi"])
+        # the condensate's ten solves and M^dagger applies
+        _, up = port.replay(np.zeros(0), g["cond_uniform"])
+        lat.load_sigma(g["cond_sigma"])
+        lat.load_pi(g["cond_pi"])
+        out, target, D, it, calls, st = lat.condensate(g["cond_sm"], 1e-9, g["cond_target0"], up, precision=EX)
+    assert st == G.GN_OK and (it, calls) == tuple(g["cond_counters"])
+    assert np.array_equal(out, g["cond_out"])
+    assert np.array_equal(target, g["cond_target"]) and np.array_equal(D, g["cond_D"])
 
 
 def test_u1_switch_back(golden):
