@@ -297,18 +297,26 @@ bool trajectory(Lattice *lattice, Info *info, Forcesigma *force, Momentasigma *m
   return true;
 }
 
-#ifndef GN_DROPIN_PI
 // The reference's EvolveSigmaInTime* helpers (moleculardynamics.c:1460-1625)
 // on the GPU: the fields they read go up, gn_evolve_sigma_in_time runs the
-// helper's steps, and the fields they write come back.
+// helper's steps, and the fields they write come back.  In the U(1) build
+// the fermion fields are complex and M carries the resident pi mass.
 void evolve_in_time(Lattice *lattice, Info *info, Forcesigma *force, Momentasigma *momenta, Fermionkit *kit,
                     double epsilon, int step, int integrator) {
   gn_context *c = ctx();
   if (gn_load_sigma(c, lattice->sigma) != GN_OK) fatal("gn_load_sigma");
+#ifdef GN_DROPIN_PI
+  if (gn_load_pi(c, lattice->pi) != GN_OK) fatal("gn_load_pi");
+  const int f_phi = GN_F_PHI_C, f_x = GN_F_X_C, f_y = GN_F_Y_C;
+  pair_to_planes(kit->phi, g_a.data());
+  pair_to_planes(kit->inverted_phi, g_b.data());
+#else
+  const int f_phi = GN_F_PHI, f_x = GN_F_X, f_y = GN_F_Y;
   pair_to_real(kit->phi, g_a.data());
   pair_to_real(kit->inverted_phi, g_b.data());
-  if (gn_write_state(c, GN_F_P, momenta->momenta) != GN_OK || gn_write_state(c, GN_F_PHI, g_a.data()) != GN_OK ||
-      gn_write_state(c, GN_F_X, g_b.data()) != GN_OK)
+#endif
+  if (gn_write_state(c, GN_F_P, momenta->momenta) != GN_OK || gn_write_state(c, f_phi, g_a.data()) != GN_OK ||
+      gn_write_state(c, f_x, g_b.data()) != GN_OK)
     fatal("gn_write_state");
   gn_hmc_params hp;
   hp.beta_s = info->beta_scalar;
@@ -323,15 +331,19 @@ void evolve_in_time(Lattice *lattice, Info *info, Forcesigma *force, Momentasigm
   if (gn_evolve_sigma_in_time(c, &hp, &r) < 0) fatal("gn_evolve_sigma_in_time");
   if (gn_store_sigma(c, lattice->sigma, lattice->sigmamass) != GN_OK) fatal("gn_store_sigma");
   if (gn_read_state(c, GN_F_P, momenta->momenta) != GN_OK || gn_read_state(c, GN_F_F, force->force) != GN_OK ||
-      gn_read_state(c, GN_F_X, g_a.data()) != GN_OK || gn_read_state(c, GN_F_Y, g_b.data()) != GN_OK)
+      gn_read_state(c, f_x, g_a.data()) != GN_OK || gn_read_state(c, f_y, g_b.data()) != GN_OK)
     fatal("gn_read_state");
+#ifdef GN_DROPIN_PI
+  planes_to_pair(g_a.data(), kit->inverted_phi);
+  planes_to_pair(g_b.data(), kit->inverted_phi_obs);
+#else
   real_to_pair(g_a.data(), kit->inverted_phi);
   real_to_pair(g_b.data(), kit->inverted_phi_obs);
+#endif
   kit->iterations += r.cg_iterations;
   kit->CG_call += int(r.cg_calls);
   lattice->distance_sigma += r.distance;
 }
-#endif
 
 #ifdef GN_DROPIN_PI
 void draw_pair(double *a, double *b) { g_gauss2(a, b, 0.0, 1.0); }  // DrawPiMomentaFromGaussianDistribution
@@ -501,7 +513,6 @@ bool LeapFrog2MinimumNormSigmaVelocityFirst(Lattice *lattice, Info *info, Forces
                                             const char *acceptance_file) {
   return trajectory(lattice, info, force, momenta, kit, epsilon, step, acceptance_file, GN_LFMN2VF);
 }
-#ifndef GN_DROPIN_PI
 void EvolveSigmaInTimeLF2(Lattice *lattice, Info *info, Forcesigma *force, Momentasigma *momenta, const Fermioncoor *,
                           Fermionkit *kit, double epsilon, const int step) {
   evolve_in_time(lattice, info, force, momenta, kit, epsilon, step, GN_LF2);
@@ -515,7 +526,6 @@ void EvolveSigmaInTimeMinimumNormSigmaVelocityFirst(Lattice *lattice, Info *info
                                                     double epsilon, const int step) {
   evolve_in_time(lattice, info, force, momenta, kit, epsilon, step, GN_LFMN2VF);
 }
-#endif
 
 void ComputeCondensateDirac(const Lattice *lat, double *tr1, double *tr1_abs, double *tr2, double *tr4, double *mu2,
                             double *mu4, double *chi, double *chi_abs, double *chip, double *c12_nosigma,

@@ -502,39 +502,56 @@ int Engine::trajectory(const gn_hmc_params &hp, double (*gauss)(void), double (*
 // The reference's MD helpers (moleculardynamics.c:1460-1625) as they behave:
 // every solve's bool is ignored; a force whose solve fails is left at zero
 // (ComputeSigmaForce zeroes it first, :634) and its flavour loop stops at the
-// failure; sigma is never restored.
+// failure; sigma is never restored.  In a context holding pi (the U(1)
+// model) the same steps run with the complex M on the complex phi and X, as
+// the PI_INTERACTION build's ComputeSigmaForce does (:590-647).
 int Engine::evolve_in_time(const gn_hmc_params &hp, gn_traj_result *res) {
   TraceRange tr("gn evolve in time");
   if (hp.steps < 1) throw GnError(GN_ERR_ARG, "steps must be >= 1");
   if (hp.integrator < 0 || hp.integrator > 2) throw GnError(GN_ERR_ARG, "unknown integrator");
-  if (u1_) throw GnError(GN_ERR_ARG, "the MD helpers are built for the Z2 model only");
   const size_t V = size_t(V_);
   memset(res, 0, sizeof *res);
   ExactScope exact_scope(exact, hp.precision == GN_PREC_FP64_EXACT);
-  const double *phis[2] = {phi_, phi_ + V};
-  double *Xs[2] = {X_, X_ + V};
+  const bool cm = u1_;
+  const size_t fl = cm ? 2 * V : V;  // one flavour's planes
+  double *phi = cm ? phi_c_ : phi_, *X = cm ? X_c_ : X_, *Y = cm ? Y_c_ : Y_;
+  const double *phis[2] = {phi, phi + fl};
+  double *Xs[2] = {X, X + fl};
   SolveInfo info[2];
   double iters = 0.0;
   long long calls = 0, inner = 0, rel = 0;
   int all_ok = 1;
+  auto solve2 = [&](double tol, int variant) {
+    return cm ? solve_cm(sm_, pm_, phis, Xs, 2, tol, variant, hp.relative, 0, info, hp.precision)
+              : solve(sm_, phis, Xs, 2, 1, tol, variant, hp.relative, 0, hp.precision, info);
+  };
+  // Y = M^dagger X, F from X, Y and sigma, then P += pcoef F when P is given
+  auto force_from_x = [&](double *P, double pcoef) {
+    if (cm) {
+      dirac_cm(sm_, pm_, X, Y, 2, GN_OP_MT);
+      force_cm(false, X, Y, sigma(), (4 * hp.beta_s / 2.0), F_, P, pcoef);  // (NFLAV * beta_scalar / 2.0), :580
+    } else {
+      dirac(sm_, X, Y, 2, GN_OP_MT);
+      force(X, Y, sigma(), hp.beta_s, F_, P, pcoef);
+    }
+  };
   const std::vector<Op> ops = evolve_schedule(hp.integrator, hp.eps, hp.steps);
   for (size_t k = 0; k < ops.size(); k++) {
     const Op &o = ops[k];
     if (o.op == OP_F_MED || o.op == OP_F_HIGH) {
       const double tol = o.op == OP_F_MED ? hp.tol_medium : hp.tol_high;
-      const int st = solve(sm_, phis, Xs, 2, 1, tol, 0, hp.relative, 0, hp.precision, info);
+      const int st = solve2(tol, 0);
       count_flavours(info, 2, iters, calls, inner, rel);
       if (st != GN_OK) {
         all_ok = 0;
         check(cudaMemsetAsync(F_, 0, V * sizeof(double), stream_), "zero force");
         continue;
       }
-      dirac(sm_, X_, Y_, 2, GN_OP_MT);
       if (k + 1 < ops.size() && ops[k + 1].op == OP_P) {
-        force(X_, Y_, sigma(), hp.beta_s, F_, P_, ops[k + 1].c);
+        force_from_x(P_, ops[k + 1].c);
         k++;
       } else {
-        force(X_, Y_, sigma(), hp.beta_s, F_, nullptr, 0.0);
+        force_from_x(nullptr, 0.0);
       }
     } else if (o.op == OP_P) {
       momenta(P_, F_, o.c);
@@ -544,8 +561,7 @@ int Engine::evolve_in_time(const gn_hmc_params &hp, gn_traj_result *res) {
       distance += o.c;
       res->distance += o.c;
     } else {  // OP_S_HIGH / OP_C_HIGH: both flavours, results not checked
-      const int st = solve(sm_, phis, Xs, 2, 1, hp.tol_high, o.op == OP_S_HIGH ? 1 : 0, hp.relative, 0,
-                           hp.precision, info);
+      const int st = solve2(hp.tol_high, o.op == OP_S_HIGH ? 1 : 0);
       count_flavours(info, 2, iters, calls, inner, rel);
       if (st != GN_OK) all_ok = 0;
     }

@@ -338,7 +338,9 @@ GN_API int gn_md_evolve(gn_context *ctx, const gn_hmc_params *params, gn_traj_re
  * EvolveSigmaInTimeMinimumNormLF2 (:1489, GN_LFMN2) and
  * EvolveSigmaInTimeMinimumNormSigmaVelocityFirst (:1551, GN_LFMN2VF), on the
  * resident sigma, P (GN_F_P), phi (GN_F_PHI) and X (GN_F_X, the start of
- * every early-exit solve); Z2 model only (GN_ERR_ARG in a U(1) context).
+ * every early-exit solve); in the U(1) model with the complex M on
+ * GN_F_PHI_C and GN_F_X_C (Y in GN_F_Y_C), as the PI_INTERACTION build's
+ * helpers run.
  * Their step sequences and tolerances are the helpers' own: the LF2 and
  * LFMN2 helpers take their first force at tol_high, the velocity-first one
  * runs an X0-imposed solve before and an early-exit solve after the

@@ -159,8 +159,8 @@ GN_API bool LeapFrog2MinimumNormSigmaVelocityFirst(struct Lattice *lattice, stru
 /* :1460, :1489, :1551 -- the MD helpers of the reference's reversibility check
  * (DEBUG_LF2_SIGMA): sigma, P and the kit's phi / inverted_phi in, sigma,
  * sigmamass, P, F, inverted_phi and inverted_phi_obs out, kit counters and
- * lat->distance_sigma updated; on the GPU through gn_evolve_sigma_in_time.
- * The Z2 model only: libgn_dropin_pi.so does not export them. */
+ * lat->distance_sigma updated; on the GPU through gn_evolve_sigma_in_time
+ * (libgn_dropin_pi.so: with the complex M, on the lattice's sigma and pi). */
 GN_API void EvolveSigmaInTimeLF2(struct Lattice *lattice, struct Info *info, struct Forcesigma *force,
                                  struct Momentasigma *momenta, const struct Fermioncoor *fermioncoor,
                                  struct Fermionkit *kit, double epsilon, const int step);

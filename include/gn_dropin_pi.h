@@ -2,10 +2,10 @@
  * gn_dropin_pi.h -- the drop-in layer for a program built with PI_INTERACTION
  * (the U(1) Gross-Neveu model): 3d-gross-neveu-model_b200/lib/libgn_dropin_pi.so.
  *
- * It exports every function of gn_dropin.h but the EvolveSigmaInTime* MD
- * helpers (built for the Z2 model only), with the PI build's meaning:
+ * It exports every function of gn_dropin.h with the PI build's meaning:
  * M = D + sigmamass + i epsilon_pi pimass on complex fermion fields
- * (dirac.c:65-69), the CG, the sigma force, the sigma integrators and
+ * (dirac.c:65-69), the CG, the sigma force, the sigma integrators and their
+ * EvolveSigmaInTime* MD helpers, and
  * ComputeCondensateDirac (condensate.c:114, unchanged by PI_INTERACTION but
  * for its M) with that M, and CondensateSigmaPi of |(sigma, pi)|
  * (observables.c:345).  It adds the pi functions below.  The struct layouts

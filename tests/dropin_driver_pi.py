@@ -7,7 +7,8 @@ compiled with -DPI_INTERACTION (oracle/_ref/libgnref_L{L}_i0_pi.so).  The
 harness then calls the reference's functions by name (DiracFermion, the CG,
 ComputeSigmaForce, ComputePiForce, the energies, CondensateSigmaPi,
 LeapFrog2MinimumNormSigmaVelocityFirst, LeapFrog2Pi, ComputeCondensateDirac) in the order
-tests/golden/make_golden_u1.py called them on the reference alone; each binds
+tests/golden/make_golden_u1.py called them on the reference alone, then
+EvolveSigmaInTimeMinimumNormSigmaVelocityFirst on seeded inputs; each binds
 to the drop-in's GPU version.  Random numbers come from the reference's own
 Gauss1, Casuale and Gauss2MeanVariance, found by name.
 
@@ -24,6 +25,29 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parent.parent
 sys.path.insert(0, str(ROOT))
+
+
+def evolve_inputs_pi(L):
+    """sigma, pi, P and chi of the MD-helper check (seeded)."""
+    rng = np.random.default_rng(12)
+    V = L ** 3
+    w = np.sqrt(2.0 / (4 * 0.85))
+    return rng.normal(0.0, w, V), rng.normal(0.0, w, V), rng.normal(size=V), rng.normal(size=(2, V))
+
+
+def evolve_setup(ref, L, beta_s):
+    """The reference's state for EvolveSigmaInTimeMinimumNormSigmaVelocityFirst:
+    sigma, pi, P, phi_f = M chi_f and X_f = 0, counters reset."""
+    sig0, pi0, P0, chi = evolve_inputs_pi(L)
+    ref.init(1231, beta_s, 0.1, 4)
+    ref.set_pi_params(0.1, 4)
+    ref.set_sigma(sig0)
+    ref.set_pi(pi0)
+    ref.set_momenta(P0)
+    for f in range(2):
+        ref.kit_set("phi", f, ref.dirac(chi[f].astype(complex), 0))
+        ref.kit_set("X", f, np.zeros(L ** 3, complex))
+    ref.lib.gnref_reset_counters()
 
 
 def main():
@@ -97,6 +121,13 @@ def main():
     counts["condensate"] = launches() - n0
     out.update(cond_counters=list(ref.counters()), cond_target=cj(ref.kit_get("Y", 0)),
                cond_D=cj(ref.kit_get("D", 0)))
+    # the MD helper of the reference's reversibility check through its call site
+    evolve_setup(ref, L, float(g["beta_s"]))
+    n0 = launches()
+    ref.evolve_in_time(0, 0.1, 4)
+    counts["evolve"] = launches() - n0
+    out.update(evolve_sigma=ref.sigma().tolist(), evolve_P=ref.momenta().tolist(),
+               evolve_counters=list(ref.counters()))
     out["launches"] = counts
     C.CDLL(None).fflush(None)  # LeapFrog2Pi's printed lines go out before the JSON line
     print(json.dumps(out))

@@ -65,13 +65,11 @@ def test_dropin_exports_every_declared_symbol(core_lib):
 
 
 def test_dropin_pi_exports_every_declared_symbol(core_lib):
-    """The PI_INTERACTION layer exports gn_dropin.h's functions, but the Z2
-    model's EvolveSigmaInTime* MD helpers, and gn_dropin_pi.h's."""
+    """The PI_INTERACTION layer exports every function of gn_dropin.h (with
+    the complex M) and gn_dropin_pi.h's."""
     lib = LIBDIR / "libgn_dropin_pi.so"
     assert lib.exists(), "build the library first (python 3d-gross-neveu-model_b200/build.py)"
-    z2_only = {"EvolveSigmaInTimeLF2", "EvolveSigmaInTimeMinimumNormLF2",
-               "EvolveSigmaInTimeMinimumNormSigmaVelocityFirst"}
-    names = (set(declared("gn_dropin.h")) - z2_only) | set(declared("gn_dropin_pi.h"))
+    names = set(declared("gn_dropin.h")) | set(declared("gn_dropin_pi.h"))
     assert len(names) >= 30
     missing = names - exported(lib)
     assert not missing, missing

@@ -93,6 +93,20 @@ def test_dropin_exact_mode_is_bit_identical():
     assert out["evolve_sigma"] == s_ref.tolist() and out["evolve_P"] == P_ref.tolist()
 
 
+def evolve_reference_pi(L, beta_s):
+    """The PI build's own EvolveSigmaInTimeMinimumNormSigmaVelocityFirst (no
+    drop-in in this process) on the PI driver's inputs: (sigma, P, counters)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from dropin_driver_pi import evolve_setup
+
+    from oracle import build_ref
+    from oracle.oracle import Ref
+    ref = Ref(L, 0, build=False, extra_defs=build_ref.PI_DEFS, tag=build_ref.PI_TAG)
+    evolve_setup(ref, L, beta_s)
+    ref.evolve_in_time(0, 0.1, 4)
+    return ref.sigma(), ref.momenta(), list(ref.counters())
+
+
 def _cx(a):
     return np.array(a[0]) + 1j * np.array(a[1])
 
@@ -115,7 +129,7 @@ def test_dropin_pi_exact_mode_is_bit_identical(L):
     reference's PI harness, calling its own functions by name, gets every
     result of its PI build bit for bit from the GPU."""
     out, g = _run_pi_driver(L, "exact")
-    assert all(v > 0 for v in out["launches"].values()) and len(out["launches"]) == 6, out["launches"]
+    assert all(v > 0 for v in out["launches"].values()) and len(out["launches"]) == 7, out["launches"]
     for key in ("M_psi", "Mt_psi", "sub_res", "cg_x", "cond_target", "cond_D"):
         assert np.array_equal(_cx(out[key]), g[key]), key
     for key in ("force_X", "piforce_Y"):
@@ -131,6 +145,9 @@ def test_dropin_pi_exact_mode_is_bit_identical(L):
         assert tuple(out[f"{name}_counters"]) == tuple(g[f"{name}_counters"])
         assert np.array_equal(np.array(out[f"{name}_sigma"]), g[f"{name}_sigma"])
         assert np.array_equal(np.array(out[f"{name}_pi"]), g[f"{name}_pi"])
+    s_ref, P_ref, cnt_ref = evolve_reference_pi(L, float(g["beta_s"]))
+    assert out["evolve_counters"] == cnt_ref
+    assert np.array_equal(np.array(out["evolve_sigma"]), s_ref) and np.array_equal(np.array(out["evolve_P"]), P_ref)
 
 
 @pytest.mark.parametrize("L", [4, 8])
@@ -145,7 +162,7 @@ def test_dropin_pi_under_reference_harness(L):
     def rel(a, b):
         return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
     # the replacement took effect: each call site launched the library's kernels
-    assert all(v > 0 for v in out["launches"].values()) and len(out["launches"]) == 6, out["launches"]
+    assert all(v > 0 for v in out["launches"].values()) and len(out["launches"]) == 7, out["launches"]
     assert np.array_equal(np.array(out["pm"]), g["pm"])
     np.testing.assert_allclose(out["sigma_obs"], g["sigma_obs"], rtol=1e-12, atol=1e-16)
     assert np.array_equal(cx(out["M_psi"]), g["M_psi"])
@@ -174,3 +191,7 @@ def test_dropin_pi_under_reference_harness(L):
         assert abs(out["cond_out"][k] - g["cond_out"][k]) <= 1e-11 * max(abs(g["cond_out"][k]), 1e-3), k
     assert rel(cx(out["cond_target"]), g["cond_target"]) < 1e-11
     assert rel(cx(out["cond_D"]), g["cond_D"]) < 1e-11
+    # the MD helper through its call site
+    s_ref, P_ref, cnt_ref = evolve_reference_pi(L, float(g["beta_s"]))
+    assert out["evolve_counters"] == cnt_ref
+    assert rel(np.array(out["evolve_sigma"]), s_ref) < 1e-11 and rel(np.array(out["evolve_P"]), P_ref) < 1e-11
