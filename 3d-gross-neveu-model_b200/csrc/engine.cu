@@ -382,8 +382,8 @@ int Engine::trajectory(const gn_hmc_params &hp, double (*gauss)(void), double (*
     bool on;
     DeferScope(Engine &en, bool d) : e(en), on(d) {
       if (on) {
+        e.check(cudaMemsetAsync(e.err_, 0, sizeof(int), e.stream_), "memset");  // may throw: before the flag
         e.defer_ = true;
-        e.check(cudaMemsetAsync(e.err_, 0, sizeof(int), e.stream_), "memset");
       }
     }
     ~DeferScope() {
