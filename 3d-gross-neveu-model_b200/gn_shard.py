@@ -1,6 +1,8 @@
 """Batched chains and served requests spread over the GPUs of one node.
 
-One process per GPU (torch.distributed, NCCL or gloo, set up by the caller).
+One process per GPU (torch.distributed, NCCL or gloo, set up by the caller;
+with NCCL the rank's device must be current, torch.cuda.set_device, since the
+gathers stage their bytes there).
 Chains shard without a collective on the data path: a chain lives on one rank
 for its whole life and keeps its global index as its Philox stream, so its
 trajectories are the same on any rank and beside any other chains (the
