@@ -455,6 +455,21 @@ def run_ours(a, world, rank, local):
     if cpu_job is not None:
         cpu = cpu_line_fields(cpu_job.result(), a)
 
+    line = bench_line(a, world, L, V, results, e2e_s, roof, dirac, peaks, cpu, detail)
+    if rank == 0:
+        if a.detail:
+            Path(a.detail).parent.mkdir(parents=True, exist_ok=True)
+            Path(a.detail).write_text(json.dumps({"line": line, "detail": detail}, indent=1, default=str))
+        print(json.dumps(line), flush=True)
+    lat.close()
+
+
+def bench_line(a, world, L, V, results, e2e_s, roof, dirac, peaks, cpu, detail):
+    """The bench's JSON line from the measurements: the contract's keys first,
+    then short summaries of the side measurements, the claims (Dirac roofline,
+    the FP64 arm, mixed over FP64) last, so that a log tail keeps them.
+    results: {"mixed"|"fp64": {"ms", "out", "clocks", "launches"}}; adds the
+    per-arm figures to detail."""
     mixed, fp64 = results["mixed"], results["fp64"]
     value = world * a.steps / (mixed["ms"] / 1000.0)
     fp64_rate = world * a.steps / (fp64["ms"] / 1000.0)
@@ -466,7 +481,6 @@ def run_ours(a, world, rank, local):
     detail["fp64"] = {"cg_iterations_per_traj": statistics.mean(o["cg_iterations"] for o in fp64["out"]),
                       "clocks": fp64["clocks"]}
     detail["roofline"], detail["dirac_roofline"] = roof, dirac
-    # the line: the contract's keys, then short summaries, the claims last
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": mixed["ms"] / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 inner CG, f64 reliable updates and dH", "data": "synthetic (seeded N(0,1) P and chi)",
@@ -484,12 +498,7 @@ def run_ours(a, world, rank, local):
                               "frac": round(dirac["gbs"] / peaks["hbm_gbs"], 3)}
     line["fp64"] = {"value": round(fp64_rate, 3), "ms_per_step": round(fp64["ms"] / a.steps, 2)}
     line["mixed_over_fp64"] = round(value / fp64_rate, 3)
-    if rank == 0:
-        if a.detail:
-            Path(a.detail).parent.mkdir(parents=True, exist_ok=True)
-            Path(a.detail).write_text(json.dumps({"line": line, "detail": detail}, indent=1, default=str))
-        print(json.dumps(line), flush=True)
-    lat.close()
+    return line
 
 
 def summaries(d, peaks):
