@@ -1,4 +1,5 @@
-"""bench.py's JSON line, assembled on the host from synthetic measurements:
+"""bench.py's JSON line, assembled on the host from synthetic measurements, and
+its clock summary from a sampled CSV:
 the contract's keys with their types and units, the whole-job value over N
 GPUs, the roofline against the given peak, and the claims (Dirac roofline,
 the FP64 arm, mixed over FP64) at the end of the line, where a log tail keeps
@@ -64,3 +65,35 @@ def test_line_over_gpus():
     assert abs(line["e2e"]["value"] - 4 * 5 / 0.315) < 1e-12
     assert line["serving"]["n_gpus"] == 4 and line["serving"]["done_req_per_s"] == 380.0
     assert line["batched"]["fp64_traj_s"] is None  # the FP64 chains run on one GPU only
+
+
+class _FakeSampler:
+    def terminate(self):
+        pass
+
+    def wait(self, timeout=None):
+        return 0
+
+
+def test_clock_summary_counts_the_timed_region_only(tmp_path):
+    """The clock sampler reports the median SM clock, the maximum and the
+    throttle reasons seen after mark() (the timed region), not before."""
+    c = bench.Clocks(0)
+    c.path = str(tmp_path / "clocks.csv")
+    c.fh = open(c.path, "w")
+    c.proc = _FakeSampler()
+    warm = "0, 1200, 1965, 300.0, 0x1, Active, Not Active, Not Active, Not Active\n"  # hw_slowdown before timing
+    c.fh.write(warm * 3)
+    c.mark()
+    rows = ["0, 1965, 1965, 900.5, 0x4, Not Active, Not Active, Not Active, Active\n",
+            "0, 1950, 1965, 990.0, 0x4, Not Active, Not Active, Not Active, Active\n",
+            "0, 1965, 1965, 950.0, 0x0, Not Active, Not Active, Not Active, Not Active\n",
+            "garbled line\n"]
+    c.fh.writelines(rows)
+    got = c.stop()
+    assert got == {"sm_mhz": 1965.0, "sm_max_mhz": 1965.0, "reasons": ["sw_power_cap"], "samples": 3,
+                   "power_w_max": 990.0}
+
+
+def test_clock_summary_without_sampler():
+    assert bench.Clocks(0).stop()["reasons"] == ["nvidia-smi unavailable"]
