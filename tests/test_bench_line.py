@@ -1,9 +1,13 @@
-"""bench.py's JSON line, assembled on the host from synthetic measurements, and
-its clock summary from a sampled CSV:
-the contract's keys with their types and units, the whole-job value over N
-GPUs, the roofline against the given peak, and the claims (Dirac roofline,
-the FP64 arm, mixed over FP64) at the end of the line, where a log tail keeps
-them.  No GPU: the measurements are stand-ins."""
+"""bench.py's host-side logic, without a GPU (the measurements are
+stand-ins):
+
+- the JSON line assembled from the measurements: the contract's keys with
+  their types and units, the whole-job value over N GPUs, the roofline against
+  the given peak, and the claims (Dirac roofline, the FP64 arm, mixed over
+  FP64) at the end of the line, where a log tail keeps them;
+- the clock summary from the sampler's CSV: only the timed region's samples,
+  and the throttle reasons seen there.
+"""
 import json
 import sys
 from pathlib import Path
